@@ -1,0 +1,379 @@
+#!/usr/bin/env python
+"""Full-step throughput of the B200 tree code (one JSON line on rank 0).
+
+Workload (the large Plummer configuration): N = 2^24 equal-mass Plummer
+sphere (seeded, the reference's plummer.h algorithm), float32, theta = 0.4,
+eps = 0.005, NLEAF = 16, NCRIT = 64, levelSplit = 5, dt = 1/128, fixed-theta
+FP32 walk.  A step is the reference's full step (treecode.cu:137-168): box +
+keys + sort + octree + multipoles + groups + walk + leapfrog move + energies,
+replayed as captured CUDA graphs; inputs stay resident in HBM (the particle
+state, 1.3 GB, is larger than the 126 MB L2, so no flush is needed).
+
+  value   : N x n_gpus / (device time per step), Mparticles/s
+  e2e     : the same through the C ABI from pinned host buffers: every step
+            copies pos+vel host->device, runs the step, scatters the
+            accelerations back to caller order and copies them device->host
+  roofline: the walk kernel (FP32 FMA bound, no tensor cores): algorithmic
+            flops = 20 per direct + 64 per quadrupole interaction
+            (treecode.cu:149-158) / walk time from CUDA events recorded on the
+            handle's stream inside the timed region; peak = this GPU's FP32
+            FMA throughput measured by bonsai_fp32_peak
+  cpu_baseline / --impl reference: the CPU restatement of the reference
+            algorithm (oracle/, OpenMP over the host cores), on a bounded
+            sample: full-N build, multipoles and groups, the walk of a sample
+            of groups extrapolated to all groups.
+
+Multi-GPU (torchrun): independent replicas, one per GPU (the single-system
+step has no exchange step); max of the device times over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "Mparticles/s per full step at N=2^24, median |δa|/|a|≤1e-3; learned-θ vs fixed-θ"
+UNIT = "Mparticles/s"
+# the walk's traffic per launch measured by ncu on this workload (see profiles/);
+# None until a capture exists
+WALK_DRAM_BYTES_PER_LAUNCH = None
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=1 << 24)
+    ap.add_argument("--theta", type=float, default=0.4)
+    ap.add_argument("--eps", type=float, default=0.005)
+    ap.add_argument("--nleaf", type=int, default=16)
+    ap.add_argument("--ncrit", type=int, default=64)
+    ap.add_argument("--level-split", type=int, default=5)
+    ap.add_argument("--dt", type=float, default=1.0 / 128)
+    ap.add_argument("--seed", type=int, default=19810614)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--error-samples", type=int, default=4096)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-group-fraction", type=float, default=1.0 / 512)
+    return ap.parse_args()
+
+
+def workload(a):
+    return ("plummer N=%d theta=%g eps=%g nleaf=%d ncrit=%d levelSplit=%d dt=1/%d seed=%d, fixed-theta FP32"
+            % (a.n, a.theta, a.eps, a.nleaf, a.ncrit, a.level_split, round(1 / a.dt), a.seed))
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas)
+# ---------------------------------------------------------------------------
+class Dist:
+    def __init__(self, backend):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+            import torch.distributed as dist
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        dev = "cuda" if self.pg.get_backend() == "nccl" else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.th.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for k, nm in enumerate(names):
+                    if r[5 + k].lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU restatement of the reference (oracle/), bounded sample
+# ---------------------------------------------------------------------------
+def cpu_reference_step(O, pos, vel, a, rng):
+    """One step of the reference algorithm on the host cores; the walk runs on
+    a random sample of groups and is extrapolated.  Returns (seconds per full
+    step (estimated), description)."""
+    t0 = time.perf_counter()
+    S = O.OracleStep(pos, theta=a.theta, eps=a.eps, nleaf=a.nleaf, ncrit=a.ncrit, level_split=a.level_split)
+    S.build()
+    t1 = time.perf_counter()
+    S.multipoles()
+    t2 = time.perf_counter()
+    S.groups()
+    t3 = time.perf_counter()
+    G = len(S.gbeg)
+    gs = max(1, int(round(G * a.cpu_group_fraction)))
+    sel = np.sort(rng.choice(G, gs, replace=False)).astype(np.int32)
+    S.forces(gsel=sel)
+    t4 = time.perf_counter()
+    acc = np.zeros_like(pos)
+    acc[S.ph_perm] = S.acc
+    p2, v2 = pos.copy(), vel.copy()
+    O.move(p2, v2, acc, a.dt, True, a.eps)
+    t5 = time.perf_counter()
+    frac = S.gnp[sel].sum() / float(pos.shape[0])
+    walk_full = (t4 - t3) / frac
+    total = (t1 - t0) + (t2 - t1) + (t3 - t2) + walk_full + (t5 - t4)
+    desc = ("full-N box+keys+sort+tree %.2fs, multipoles %.2fs, groups %.2fs; walk of %d/%d groups "
+            "(%.3f%% of particles) %.2fs extrapolated to %.1fs; move %.2fs"
+            % (t1 - t0, t2 - t1, t3 - t2, gs, G, 100 * frac, t4 - t3, walk_full, t5 - t4))
+    return total, desc
+
+
+def run_reference(a):
+    d = Dist("gloo")
+    if d.rank != 0:
+        d.close()
+        return
+    from oracle import oracle as O
+    O.build()
+    pos, vel = O.plummer_float4(a.n, a.seed)
+    rng = np.random.default_rng(1)
+    times = []
+    desc = ""
+    for s in range(a.warmup + a.steps):
+        t, desc = cpu_reference_step(O, pos, vel, a, rng)
+        if s >= a.warmup:
+            times.append(t)
+    tm = statistics.mean(times)
+    v = a.n / tm / 1e6
+    cores = O.num_threads()
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": tm * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic: seeded Plummer sphere (plummer.h algorithm)",
+            "config": {"workload": workload(a), "n": a.n}, "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": "per step: " + desc},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    d.close()
+
+
+# ---------------------------------------------------------------------------
+# the B200 path
+# ---------------------------------------------------------------------------
+def run_ours(a):
+    import ctypes
+
+    import torch
+
+    d = Dist("nccl")
+    torch.cuda.set_device(d.local)
+    import bonsai2_b200 as B
+    from bonsai2_b200.treecode import _p
+
+    L = B.load()
+    n = a.n
+    # pinned host staging (host_mem<T> of the reference, cudamem.h:64-96)
+    nbytes = n * 16
+    hp = L.bonsai_host_alloc(nbytes)
+    hv = L.bonsai_host_alloc(nbytes)
+    ha = L.bonsai_host_alloc(nbytes)
+    if not (hp and hv and ha):
+        raise RuntimeError("pinned allocation failed")
+    pos = np.ctypeslib.as_array((ctypes.c_float * (4 * n)).from_address(hp)).reshape(n, 4)
+    vel = np.ctypeslib.as_array((ctypes.c_float * (4 * n)).from_address(hv)).reshape(n, 4)
+    accb = np.ctypeslib.as_array((ctypes.c_float * (4 * n)).from_address(ha)).reshape(n, 4)
+    p0, v0 = B.plummer(n, a.seed)
+    pos[:] = p0
+    vel[:] = v0
+
+    peak = ctypes.c_double(0.0)
+    rc = L.bonsai_fp32_peak(d.local, ctypes.byref(peak))
+    if rc:
+        raise B.BonsaiError(rc, "bonsai_fp32_peak")
+
+    t = B.Treecode(eps=a.eps, theta=a.theta, ncrit=a.ncrit, nleaf=a.nleaf, level_split=a.level_split, dt=a.dt,
+                   device=d.local)
+    t.alloc(n)
+    if L.bonsai_set_particles(t.handle, _p(pos), _p(vel), n):
+        raise RuntimeError("set_particles")
+    nkern = L.bonsai_graph_kernel_count(t.handle)
+    t.step(a.warmup, graph=True)
+    assert t.synchronize() == 0
+    E0 = t.computeEnergies()
+
+    # ---- timed region: K graph steps, events on the handle's stream ----
+    phase = np.zeros(4 * a.steps + 1, np.float32)
+    d.barrier()
+    torch.cuda.synchronize()
+    clk = ClockSampler(d.local)
+    clk.start()
+    rc = L.bonsai_step_timed(t.handle, a.steps, _p(phase))
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    d.barrier()
+    if rc:
+        raise B.BonsaiError(rc, "bonsai_step_timed")
+    status = t.synchronize()
+    region_ms = d.max(float(phase[4 * a.steps]))
+    ms = region_ms / a.steps
+    ph = phase[:4 * a.steps].reshape(a.steps, 4)
+    walk_ms = float(ph[:, 1].mean())
+    E1 = t.computeEnergies()
+    st = np.zeros(4, np.uint64)
+    L.bonsai_get_stats(t.handle, _p(st))
+    n_app, n_dir = float(st[0]), float(st[1])
+    flops = 20.0 * n_dir + 64.0 * n_app
+    achieved = flops / (walk_ms * 1e-3) / 1e12
+    value = n * d.world / (ms * 1e-3) / 1e6
+
+    # ---- accuracy at the final positions: an eager force evaluation vs FP64 direct sum ----
+    t.buildTree(a.nleaf)
+    t.computeMultipoles()
+    t.makeGroups(a.level_split, a.ncrit)
+    t.computeForces(False)
+    acc = t.get_acc().astype(np.float64)
+    rng = np.random.default_rng(4096 + d.rank)
+    samp = rng.choice(n, min(a.error_samples, n), replace=False).astype(np.int32)
+    ref = t.direct_fp64(samp, include_self=True)
+    err = np.linalg.norm(acc[samp, :3] - ref[:, :3], axis=1) / np.linalg.norm(ref[:, :3], axis=1)
+
+    # ---- e2e through the C ABI with host buffers ----
+    stream = torch.cuda.ExternalStream(L.bonsai_stream(t.handle))
+    e2e_ms = []
+    for s in range(a.e2e_steps + 1):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        d.barrier()
+        e0.record(stream)
+        rc = L.bonsai_set_particles(t.handle, _p(pos), _p(vel), n)
+        rc |= L.bonsai_step(t.handle, 1, 1)
+        rc |= L.bonsai_get_particles(t.handle, None, None, _p(accb))
+        e1.record(stream)
+        e1.synchronize()
+        if rc:
+            raise B.BonsaiError(rc, "e2e step")
+        if s > 0:
+            e2e_ms.append(e0.elapsed_time(e1))
+    e2e = d.max(statistics.mean(e2e_ms))
+    e2e_value = n * d.world / (e2e * 1e-3) / 1e6
+
+    cpu = None
+    if d.rank == 0 and d.world == 1 and not a.no_cpu_baseline:
+        from oracle import oracle as O
+        O.build()
+        tcpu, desc = cpu_reference_step(O, p0, v0, a, np.random.default_rng(1))
+        cpu = {"value": n / tcpu / 1e6, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
+               "sample": "one step: " + desc}
+
+    if d.rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": d.world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: seeded Plummer sphere (plummer.h algorithm), N per GPU",
+            "config": {"workload": workload(a), "n_per_gpu": n, "parallelism": "replicas x%d" % d.world,
+                       "l2": "no flush: particle state 1.3 GB > 126 MB L2", "graph": "captured CUDA graphs"},
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": float(peak.value), "unit": "TFLOP/s",
+                         "frac": achieved / float(peak.value), "traffic": WALK_DRAM_BYTES_PER_LAUNCH,
+                         "kernel": "k_walk", "peak_source": "measured FP32 FMA probe (bonsai_fp32_peak)",
+                         "flops_per_launch": flops},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * nbytes,
+                    "d2h_bytes_per_step": nbytes, "ms_per_step": e2e},
+            "gpu_launches": int(nkern) * a.steps,
+            "clocks": clocks,
+            "accuracy": {"median_rel_force_err": float(np.median(err)), "p99_rel_force_err": float(np.percentile(err, 99)),
+                         "samples": int(samp.shape[0]), "oracle": "FP64 direct sum (bonsai_direct_fp64)"},
+            "stages_ms": {"build_multipoles_groups": float(ph[:, 0].mean()), "walk": walk_ms,
+                          "move_energies": float(ph[:, 2].mean())},
+            "interactions_per_particle": {"approx": n_app / n, "direct": n_dir / n, "max_approx": int(st[2]),
+                                          "max_direct": int(st[3])},
+            "energy": {"E_start": float(E0[3]), "E_end": float(E1[3]),
+                       "rel_drift": abs(float(E1[3]) - float(E0[3])) / abs(float(E0[3])),
+                       "steps_between": a.steps},
+            "status": int(status),
+        }
+        print(json.dumps(line), flush=True)
+    t.close()
+    for hptr in (hp, hv, ha):
+        L.bonsai_host_free(hptr)
+    d.close()
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,70 @@
+"""Build recipe of libbonsai_b200.so (in-tree, sm_100a).
+
+nvcc compiles every .cu in bonsai2_b200/csrc for sm_100a only; the tree walk
+translation unit flushes denormals (-ftz=true) like the reference's
+computeForces.o rule (code/Makefile:53-54).  Objects go to
+bonsai2_b200/_build/, the library to bonsai2_b200/libbonsai_b200.so.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OBJ = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libbonsai_b200.so")
+INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INCLUDE, "--expt-relaxed-constexpr"]
+PER_FILE = {"walk.cu": ["-ftz=true"]}
+SOURCES = ["keys.cu", "sort.cu", "tree.cu", "multipoles.cu", "groups.cu", "walk.cu", "move.cu", "treecode.cu"]
+HOST_SOURCES = ["plummer.cpp"]
+
+
+def _deps():
+    return [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(INCLUDE, "bonsai_b200.h")]
+
+
+def up_to_date() -> bool:
+    if not os.path.exists(LIB):
+        return False
+    t = os.path.getmtime(LIB)
+    return all(os.path.getmtime(d) <= t for d in _deps())
+
+
+def _compile(src: str, verbose: bool) -> str:
+    out = os.path.join(OBJ, src + ".o")
+    path = os.path.join(CSRC, src)
+    if src.endswith(".cpp"):
+        cmd = ["g++", "-O3", "-fPIC", "-std=c++17", "-c", path, "-o", out]
+    else:
+        cmd = [NVCC] + ARCH + COMMON + PER_FILE.get(src, []) + (["-Xptxas", "-v"] if verbose else []) + ["-c", path, "-o", out]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("compile failed: %s\n%s\n%s" % (" ".join(cmd), r.stdout, r.stderr))
+    if verbose:
+        sys.stderr.write(r.stderr)
+    return out
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and up_to_date():
+        return LIB
+    os.makedirs(OBJ, exist_ok=True)
+    with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+        objs = list(ex.map(lambda s: _compile(s, verbose), SOURCES + HOST_SOURCES))
+    tmp = LIB + ".tmp%d" % os.getpid()
+    cmd = [NVCC] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart"]
+    subprocess.check_call(cmd)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose="-v" in sys.argv)
+    print(LIB)

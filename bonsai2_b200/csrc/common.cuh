@@ -1,0 +1,107 @@
+// common.cuh -- shared definitions of the B200 tree-code kernels.
+//
+// Layout conventions (all device arrays are owned by one Treecode handle):
+//   positions   float4 (x, y, z, mass)        -- Particle4<float>, Particle4.h:59-83
+//   velocities  float4 (vx, vy, vz, unused)
+//   accel       float4 (ax, ay, az, potential) -- computeForces.cu:611-617
+//   CellData    uint4  (parent | level<<27, first | (n-1)<<29 or ~0 for a
+//                       leaf, pbeg, pend)      -- Treecode.h:45-89
+//   cell_open   float4 (com x,y,z, cellOp^2)   -- d_cellSize, computeMultipoles.cu:180
+//   cell_q0     float4 (M, Ixx, Iyy, Izz)      -- mass-weighted central moments
+//   cell_q1     float4 (Ixy, Ixz, Iyz, 1.5*trace I)
+//   GroupData   int2   (pbeg, np)              -- Treecode.h:29-43
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace bonsai {
+
+constexpr int kMaxLevel = 21;        // 3 bits per level in a 63-bit key
+constexpr int kLevels = 32;          // level table size (reference: 32, Treecode.h:171)
+constexpr unsigned kFull = 0xffffffffu;
+
+// Device status word bits (sticky; read by the host after a stage).
+enum : int {
+  kStatusCellCapacity = 1 << 0,   // more cells than the cell arrays hold
+  kStatusDepth = 1 << 1,          // a level-21 cell holds more than nLeaf (kept as a fat leaf)
+  kStatusWalkStack = 1 << 2,      // a walk level list outgrew its ring
+  kStatusNonFinite = 1 << 3,      // NaN/Inf coordinate seen by the box reduction
+  kStatusGroupCapacity = 1 << 4,  // more groups than the group array holds
+  kStatusBadParam = 1 << 5,
+};
+
+// Device-resident tree/group bookkeeping: written by the build kernels and
+// read by later kernels, so no stage needs a host round trip.
+struct TreeInfo {
+  int ncells;
+  int nleaves;
+  int nnodes;
+  int nlevels;
+  int ngroups;
+  int status;
+  int pad[2];
+  int level_beg[kLevels];   // half-open [beg, end) cell range of level L
+  int level_end[kLevels];
+};
+
+// Per-cell FP64 record used by the bottom-up multipole pass.
+struct MpRec {
+  double m, cx, cy, cz;
+  double ixx, iyy, izz, ixy, ixz, iyz;
+  float bmin[3], bmax[3];
+};
+
+struct Box {
+  float cx, cy, cz, hsize;
+};
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+// sm_100a: single-instruction warp min/max of f32 (redux.sync .f32).
+__device__ __forceinline__ float warp_min_f32(float v) {
+  float r;
+  asm volatile("redux.sync.min.f32 %0, %1, 0xffffffff;" : "=f"(r) : "f"(v));
+  return r;
+}
+__device__ __forceinline__ float warp_max_f32(float v) {
+  float r;
+  asm volatile("redux.sync.max.f32 %0, %1, 0xffffffff;" : "=f"(r) : "f"(v));
+  return r;
+}
+
+// inclusive warp scan of ints
+__device__ __forceinline__ int warp_incl_scan(int v) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(kFull, v, o);
+    if (lane_id() >= o) v += t;
+  }
+  return v;
+}
+
+__device__ __forceinline__ int set_status(int* status, int bit) {
+  return atomicOr(status, bit);
+}
+
+// Level (1..21) of the first octant digit where two sorted 63-bit keys
+// differ; kMaxLevel+1 when they are equal.
+__device__ __forceinline__ int diff_level(unsigned long long a, unsigned long long b) {
+  const unsigned long long x = a ^ b;
+  if (x == 0ull) return kMaxLevel + 1;
+  const int p = 63 - __clzll((long long)x);
+  return (62 - p) / 3 + 1;
+}
+
+}  // namespace bonsai
+
+#define BONSAI_CUDA_TRY(expr)                       \
+  do {                                              \
+    cudaError_t _e = (expr);                        \
+    if (_e != cudaSuccess) return -(int)_e - 1000;  \
+  } while (0)

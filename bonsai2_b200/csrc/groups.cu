@@ -1,0 +1,91 @@
+// groups.cu -- walk groups from the PH-sorted keys, and the gather of the
+// particle state into PH order.
+//
+// The reference (makeGroups.cu:137-223, :259-309) masks the sorted PH keys to
+// their top levelSplit octal digits, finds the segments of equal masked key
+// with two scan_by_key passes, and cuts every segment into chunks of nCrit
+// particles, numbering groups with an atomic counter.  The masked key of a
+// sorted key is its top 3*levelSplit bits, i.e. a bin index in
+// [0, 8^levelSplit); bins appear in increasing order along the sorted array.
+// So a histogram over bins gives every segment's size, one exclusive scan its
+// start, a second scan over ceil(size/nCrit) the group offsets, and groups are
+// written in PH order (deterministic; the reference's canonical order).
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace bonsai {
+
+__global__ void __launch_bounds__(256) k_group_hist(const unsigned long long* __restrict__ sorted, int n, int shift,
+                                                    unsigned* __restrict__ count) {
+  // 16 consecutive keys per thread; one atomic per run of equal bin
+  const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * 16;
+  if (i0 >= n) return;
+  const int i1 = min(i0 + 16, n);
+  unsigned long long cur = sorted[i0] >> shift;
+  unsigned run = 0;
+  for (int i = i0; i < i1; i++) {
+    const unsigned long long b = sorted[i] >> shift;
+    if (b != cur) {
+      atomicAdd(count + cur, run);
+      cur = b;
+      run = 0;
+    }
+    run++;
+  }
+  atomicAdd(count + cur, run);
+}
+
+__global__ void k_group_sizes(const unsigned* __restrict__ count, int nbins, int ncrit, unsigned* __restrict__ ng) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nbins; b += gridDim.x * blockDim.x)
+    ng[b] = (count[b] + (unsigned)ncrit - 1u) / (unsigned)ncrit;
+}
+
+__global__ void k_group_write(const unsigned* __restrict__ count, const unsigned* __restrict__ seg_start,
+                              const unsigned* __restrict__ goff, int nbins, int ncrit, int2* __restrict__ groups,
+                              int group_cap, TreeInfo* __restrict__ info) {
+  if (info->ngroups > group_cap) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) set_status(&info->status, kStatusGroupCapacity);
+    return;
+  }
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nbins; b += gridDim.x * blockDim.x) {
+    const int c = (int)count[b];
+    if (c == 0) continue;
+    const int s = (int)seg_start[b], g0 = (int)goff[b];
+    for (int k = 0, off = 0; off < c; k++, off += ncrit) groups[g0 + k] = make_int2(s + off, min(ncrit, c - off));
+  }
+}
+
+void make_groups(const unsigned long long* sorted_ph, int n, int level_split, int ncrit, unsigned* count,
+                 unsigned* seg_start, unsigned* ng, unsigned* bsum, int2* groups, int group_cap, TreeInfo* info,
+                 cudaStream_t s) {
+  const int nbins = 1 << (3 * level_split);
+  const int shift = 63 - 3 * level_split;
+  cudaMemsetAsync(count, 0, sizeof(unsigned) * (size_t)nbins, s);
+  const int nthr = (n + 15) / 16;
+  k_group_hist<<<(nthr + 255) / 256, 256, 0, s>>>(sorted_ph, n, shift, count);
+  exclusive_scan(count, seg_start, nbins, bsum, nullptr, s);
+  k_group_sizes<<<(nbins + 255) / 256, 256, 0, s>>>(count, nbins, ncrit, ng);
+  exclusive_scan(ng, ng, nbins, bsum, (unsigned*)&info->ngroups, s);
+  k_group_write<<<(nbins + 255) / 256, 256, 0, s>>>(count, seg_start, ng, nbins, ncrit, groups, group_cap, info);
+}
+
+// state gather: out[k] = in[perm[k]] for positions, velocities and ids
+__global__ void __launch_bounds__(256) k_gather_state(const int* __restrict__ perm, int n,
+                                                      const float4* __restrict__ pos, const float4* __restrict__ vel,
+                                                      const int* __restrict__ id, float4* __restrict__ pos_o,
+                                                      float4* __restrict__ vel_o, int* __restrict__ id_o) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int j = __ldcs(perm + k);
+    __stcs(pos_o + k, __ldg(pos + j));
+    __stcs(vel_o + k, __ldg(vel + j));
+    __stcs(id_o + k, __ldg(id + j));
+  }
+}
+
+__global__ void __launch_bounds__(256) k_gather_pos(const int* __restrict__ perm, int n,
+                                                    const float4* __restrict__ pos, float4* __restrict__ out) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    out[k] = __ldg(pos + __ldcs(perm + k));
+}
+
+}  // namespace bonsai

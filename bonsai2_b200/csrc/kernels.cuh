@@ -1,0 +1,71 @@
+// kernels.cuh -- internal declarations shared by the kernel translation units
+// and the host orchestration (treecode.cu).  Not part of the C ABI.
+#pragma once
+#include "common.cuh"
+
+namespace bonsai {
+
+constexpr int kWalkThreads = 256;
+constexpr int kWalkMinBlocks = 3;
+
+// keys.cu
+void build_ph_table(uint16_t* tab);
+__global__ void k_box(const float4* __restrict__ pos, int n, float* __restrict__ partial, unsigned* __restrict__ ticket,
+                      Box* __restrict__ box, int* __restrict__ status);
+__global__ void k_keys(const float4* __restrict__ pos, int n, const Box* __restrict__ boxp,
+                       const uint16_t* __restrict__ ph_table, unsigned long long* __restrict__ tkey,
+                       unsigned long long* __restrict__ pkey);
+
+// sort.cu
+int sort_tiles(int n);
+int scan_blocks(int m);
+void exclusive_scan(const unsigned* in, unsigned* out, int m, unsigned* bsum, unsigned* total, cudaStream_t s);
+void radix_sort_pairs(unsigned long long* keys_a, unsigned long long* keys_b, int* vals_a, int* vals_b,
+                      const int* vals_in, int n, unsigned* counts, unsigned* bsum, int passes, cudaStream_t s);
+
+// tree.cu
+int tree_tiles(int n);
+void build_tree(const unsigned long long* sorted_keys, int n, int nleaf, int cell_cap, int leaf_cap, uint8_t* dlev,
+                uint16_t* chain, unsigned* hist, TreeInfo* info, uint4* cell_data, int* cell_parent, int* leaf_list,
+                int* mp_count, cudaStream_t s);
+
+// multipoles.cu
+__global__ void k_multipoles(const int* __restrict__ leaf_list, const TreeInfo* __restrict__ info,
+                             const uint4* __restrict__ cell_data, const int* __restrict__ cell_parent,
+                             const float4* __restrict__ jpos, float inv_theta, MpRec* __restrict__ rec,
+                             float4* __restrict__ cell_open, float4* __restrict__ cell_q0,
+                             float4* __restrict__ cell_q1, int* __restrict__ mp_count, int cell_cap);
+__global__ void k_multipoles_ref_layout(const TreeInfo* __restrict__ info, const float4* __restrict__ cell_open,
+                                        const MpRec* __restrict__ rec, float4* __restrict__ size,
+                                        float4* __restrict__ mono, float4* __restrict__ quad0,
+                                        float2* __restrict__ quad1);
+
+// groups.cu
+void make_groups(const unsigned long long* sorted_ph, int n, int level_split, int ncrit, unsigned* count,
+                 unsigned* seg_start, unsigned* ng, unsigned* bsum, int2* groups, int group_cap, TreeInfo* info,
+                 cudaStream_t s);
+__global__ void k_gather_state(const int* __restrict__ perm, int n, const float4* __restrict__ pos,
+                               const float4* __restrict__ vel, const int* __restrict__ id, float4* __restrict__ pos_o,
+                               float4* __restrict__ vel_o, int* __restrict__ id_o);
+__global__ void k_gather_pos(const int* __restrict__ perm, int n, const float4* __restrict__ pos,
+                             float4* __restrict__ out);
+
+// walk.cu
+int walk_ni(int ncrit);
+int walk_blocks_per_sm(int ni);
+void launch_walk(int ni, int nblocks, const int2* groups, const TreeInfo* info, const float4* ipos, const float4* jpos,
+                 const uint4* cell_data, const float4* cell_open, const float4* cell_q0, const float4* cell_q1,
+                 float eps2, float4* acc, int* ring_pool, int ring_cap, unsigned* group_counter,
+                 unsigned long long* stats, int* status, cudaStream_t s);
+
+// move.cu
+void launch_move(float4* pos, float4* vel, const float4* acc, int n, float dt, int* closing, float eps, int write,
+                 double* partial, int nblocks, unsigned* ticket, double* energies, cudaStream_t s);
+void launch_direct_fp64(const float4* pos, int n, const int* sample, int ns, double eps2, int include_self,
+                        double* part, int nsplit, double* out, cudaStream_t s);
+__global__ void k_scatter_by_id(const int* __restrict__ id, int n, const float4* __restrict__ in,
+                                float4* __restrict__ out);
+__global__ void k_iota(int* __restrict__ a, int n);
+double fma_probe_tflops(int nsm, cudaStream_t st, float* scratch);
+
+}  // namespace bonsai

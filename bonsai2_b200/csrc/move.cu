@@ -1,0 +1,198 @@
+// move.cu -- leapfrog move with the energy sums fused in, the FP64 direct-sum
+// checker, and the scatter back to the caller's particle order.
+//
+// The reference's moveParticles and computeEnergies are stubs
+// (moveParticles.cu:3-7, computeEnergies.cu:3-7); its only energy term is the
+// potential sum made inside the walk (computeForces.cu:576-607).  Here the
+// move is a kick-drift-kick leapfrog with merged kicks, one HBM pass:
+//   closing kick  v += a dt/2   (skipped on the first step)
+//   energy sums at the synchronised point (FP64): T, W = 1/2 sum m phi,
+//     W without the i==j self term, momentum, mass
+//   opening kick  v += a dt/2,  drift x += v dt
+// Per-block FP64 partials are folded in a fixed order by the last block, so
+// the sums are deterministic.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace bonsai {
+
+constexpr int kNE = 8;
+
+// closing kick taken when *closing is set (device flag: set by every writing
+// move, cleared when particles are loaded), so the same captured graph serves
+// the first and later steps.  write == 0 computes the energies only.
+__global__ void __launch_bounds__(256) k_move(float4* __restrict__ pos, float4* __restrict__ vel,
+                                              const float4* __restrict__ acc, int n, float dt,
+                                              int* __restrict__ closing, float eps, int write,
+                                              double* __restrict__ partial, unsigned* __restrict__ ticket,
+                                              double* __restrict__ energies) {
+  const float h = 0.5f * dt;
+  const float hc = (*closing) ? h : 0.0f;
+  double T = 0, W = 0, S = 0, px = 0, py = 0, pz = 0, mt = 0;
+  const double ieps = eps > 0.f ? 1.0 / (double)eps : 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float4 p = pos[i], v = vel[i];
+    const float4 a = acc[i];
+    v.x = fmaf(a.x, hc, v.x); v.y = fmaf(a.y, hc, v.y); v.z = fmaf(a.z, hc, v.z);
+    const double m = p.w;
+    T += 0.5 * m * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
+    W += 0.5 * m * a.w;
+    S += 0.5 * m * m * ieps;
+    px += m * v.x; py += m * v.y; pz += m * v.z; mt += m;
+    if (write) {
+      v.x = fmaf(a.x, h, v.x); v.y = fmaf(a.y, h, v.y); v.z = fmaf(a.z, h, v.z);
+      p.x = fmaf(v.x, dt, p.x); p.y = fmaf(v.y, dt, p.y); p.z = fmaf(v.z, dt, p.z);
+      pos[i] = p;
+      vel[i] = v;
+    }
+  }
+  double e[kNE] = {T, W, W + S, T + W + S, px, py, pz, mt};
+  __shared__ double sh[kNE][8];
+  __shared__ bool last;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < kNE; k++) {
+    double x = e[k];
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
+    if (lane == 0) sh[k][w] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < kNE) {
+    double x = 0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); q++) x += sh[threadIdx.x][q];
+    partial[blockIdx.x * kNE + threadIdx.x] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (threadIdx.x < kNE) {
+    double x = 0;
+    for (int b = 0; b < (int)gridDim.x; b++) x += __ldcg(partial + b * kNE + threadIdx.x);
+    energies[threadIdx.x] = x;
+  }
+  if (threadIdx.x == 0) {
+    *ticket = 0u;
+    if (write) *closing = 1;
+  }
+}
+
+void launch_move(float4* pos, float4* vel, const float4* acc, int n, float dt, int* closing, float eps, int write,
+                 double* partial, int nblocks, unsigned* ticket, double* energies, cudaStream_t s) {
+  k_move<<<nblocks, 256, 0, s>>>(pos, vel, acc, n, dt, closing, eps, write, partial, ticket, energies);
+}
+
+// FP64 direct summation for sample particles (checker): grid (ceil(ns/256),
+// nsplit); thread = one sample, block = one slice of the sources.
+__global__ void __launch_bounds__(256) k_direct_fp64(const float4* __restrict__ pos, int n,
+                                                     const int* __restrict__ sample, int ns, double eps2,
+                                                     int include_self, double* __restrict__ part) {
+  __shared__ double4 sj[256];
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nsplit = gridDim.y;
+  const int jb = (int)((long long)n * blockIdx.y / nsplit), je = (int)((long long)n * (blockIdx.y + 1) / nsplit);
+  const int i = s < ns ? sample[s] : 0;
+  const float4 pi = pos[i];
+  const double xi = pi.x, yi = pi.y, zi = pi.z;
+  double ax = 0, ay = 0, az = 0, ph = 0;
+  for (int j0 = jb; j0 < je; j0 += 256) {
+    __syncthreads();
+    const int jj = j0 + threadIdx.x;
+    if (jj < je) {
+      const float4 p = pos[jj];
+      sj[threadIdx.x] = make_double4(p.x, p.y, p.z, p.w);
+    }
+    __syncthreads();
+    const int cnt = min(256, je - j0);
+    for (int t = 0; t < cnt; t++) {
+      if (j0 + t == i && !include_self) continue;
+      const double4 q = sj[t];
+      const double dx = q.x - xi, dy = q.y - yi, dz = q.z - zi;
+      const double r2 = fma(dz, dz, fma(dy, dy, fma(dx, dx, eps2)));
+      const double rinv = rsqrt(r2);
+      const double mr = q.w * rinv;
+      const double mr3 = mr * rinv * rinv;
+      ax = fma(mr3, dx, ax); ay = fma(mr3, dy, ay); az = fma(mr3, dz, az); ph -= mr;
+    }
+  }
+  if (s < ns) {
+    double* o = part + ((size_t)blockIdx.y * ns + s) * 4;
+    o[0] = ax; o[1] = ay; o[2] = az; o[3] = ph;
+  }
+}
+
+__global__ void k_direct_fold(const double* __restrict__ part, int ns, int nsplit, double* __restrict__ out) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 4 * ns; t += gridDim.x * blockDim.x) {
+    double x = 0;
+    for (int q = 0; q < nsplit; q++) x += part[(size_t)q * ns * 4 + t];
+    out[t] = x;
+  }
+}
+
+void launch_direct_fp64(const float4* pos, int n, const int* sample, int ns, double eps2, int include_self,
+                        double* part, int nsplit, double* out, cudaStream_t s) {
+  dim3 grid((ns + 255) / 256, nsplit);
+  k_direct_fp64<<<grid, 256, 0, s>>>(pos, n, sample, ns, eps2, include_self, part);
+  k_direct_fold<<<(4 * ns + 255) / 256, 256, 0, s>>>(part, ns, nsplit, out);
+}
+
+// out[id[k]] = in[k]
+__global__ void k_scatter_by_id(const int* __restrict__ id, int n, const float4* __restrict__ in,
+                                float4* __restrict__ out) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) out[id[k]] = in[k];
+}
+
+__global__ void k_iota(int* __restrict__ a, int n) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) a[k] = k;
+}
+
+}  // namespace bonsai
+
+namespace bonsai {
+
+// FP32 FMA throughput probe: 8 independent dependent-FMA chains per thread,
+// the roofline denominator of the walk (which uses no tensor cores).
+__global__ void __launch_bounds__(256) k_fma_probe(float* __restrict__ out, int iters, float b, float c) {
+  float a[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) a[k] = (float)(threadIdx.x + k) * 1e-7f;
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+#pragma unroll
+      for (int k = 0; k < 8; k++) a[k] = fmaf(a[k], b, c);
+    }
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < 8; k++) s += a[k];
+  if (s == 1234.5f) out[blockIdx.x] = s;
+}
+
+double fma_probe_tflops(int nsm, cudaStream_t st, float* scratch) {
+  const int iters = 4096, blocks = nsm * 8;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  for (int r = 0; r < 4; r++) {
+    cudaEventRecord(e0, st);
+    k_fma_probe<<<blocks, 256, 0, st>>>(scratch, iters, 0.9999999f, 1e-7f);
+    cudaEventRecord(e1, st);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (r > 0 && ms < best) best = ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  const double flops = 2.0 * 8 * 16 * (double)iters * blocks * 256;
+  return flops / (best * 1e-3) / 1e12;
+}
+
+}  // namespace bonsai

@@ -1,0 +1,344 @@
+// tree.cu -- octree from the sorted octant-path keys, in three launches and no
+// host round trip.
+//
+// The reference builds the tree by a recursive CUDA-dynamic-parallelism
+// partition (buildOctant, buildTree.cu:170-722) and then stable-sorts the
+// cells by level (buildTree.cu:725-841,932-958).  Its cell set is defined by
+// two rules: the root is always split, and a cell with more than nLeaf
+// particles is split (buildTree.cu:394-395,444,541).  With particles sorted
+// by the octant path, every cell at level L is a maximal run of equal
+// 3L-bit key prefix, so the cell set follows from d(i), the level at which
+// keys i-1 and i first differ:
+//   * with m(i) = min d(i+1..i+nLeaf) (d = 0 past the end), the level-L run
+//     starting at i holds more than nLeaf particles iff d(i) <= L < m(i);
+//     all of those runs are nodes, and the chain of cells that start at i
+//     runs from max(d(i),1) down to the first level whose run is small
+//     (a leaf), or to level 21 (a fat leaf, flagged);
+//   * a small run starting at i at level d(i) >= 2 is a leaf iff its parent
+//     run (level d(i)-1) holds more than nLeaf particles, which is decided
+//     from d inside the window i-nLeaf .. i+nLeaf.
+// Launch 1 computes the chains of a 4096-position tile (halo nLeaf) and a
+// per-level histogram; launch 2 scans the histograms (one block); launch 3
+// writes the cells level-major, key order inside a level (the canonical form
+// of the reference's cell order), with children contiguous, the leaf list,
+// parent links and the level ranges.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace bonsai {
+
+constexpr int kTreeThreads = 256;
+constexpr int kTreeItems = 16;
+constexpr int kTreeTile = kTreeThreads * kTreeItems;  // 4096
+constexpr int kHalo = 64;                              // max nLeaf
+constexpr int kNL = kMaxLevel + 1;                     // rows 0..21 (row 0 unused)
+
+int tree_tiles(int n) { return (n + kTreeTile - 1) / kTreeTile; }
+
+struct Chain {
+  int a, b;  // levels [a, b]; a == 0: no cell starts here
+};
+
+__device__ __forceinline__ Chain make_chain(const uint8_t* sd, int loc, int i, int n, int nleaf, bool* fat) {
+  // sd[loc + j] = d(i + j) for j in [-kHalo, kHalo]
+  Chain c{0, 0};
+  const int di = (i == 0) ? 0 : (int)sd[loc];
+  const int ls = max(di, 1);
+  if (ls > kMaxLevel) return c;
+  int m = kMaxLevel + 1;
+  for (int j = 1; j <= nleaf; j++) m = min(m, (i + j >= n) ? 0 : (int)sd[loc + j]);
+  if (ls < m) {
+    c.a = ls;
+    c.b = min(m, kMaxLevel);
+    *fat = (m > kMaxLevel);
+    return c;
+  }
+  if (ls == 1) {
+    c.a = c.b = 1;
+    return c;
+  }
+  // parent run at level ls-1 containing i: [p, e)
+  int p = -1, e = -1;
+  for (int j = 1; j <= nleaf; j++) {
+    const int q = i - j;
+    if (q <= 0) { p = 0; break; }
+    if ((int)sd[loc - j] <= ls - 1) { p = q; break; }
+  }
+  for (int j = 1; j <= nleaf; j++) {
+    const int q = i + j;
+    if (q >= n) { e = n; break; }
+    if ((int)sd[loc + j] <= ls - 1) { e = q; break; }
+  }
+  if (p < 0 || e < 0 || e - p > nleaf) c.a = c.b = ls;
+  return c;
+}
+
+// Loads d for positions [t0-kHalo, t0+kTreeTile+kHalo) into sd, from keys.
+__device__ void load_d_from_keys(const unsigned long long* __restrict__ keys, int n, int t0, uint8_t* sd,
+                                 unsigned long long* sk) {
+  const int nk = kTreeTile + 2 * kHalo + 1;
+  for (int j = threadIdx.x; j < nk; j += blockDim.x) {
+    const int g = t0 - kHalo - 1 + j;
+    sk[j] = (g >= 0 && g < n) ? keys[g] : 0ull;
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < kTreeTile + 2 * kHalo; j += blockDim.x) {
+    const int p = t0 - kHalo + j;
+    sd[j] = (p <= 0 || p >= n) ? (uint8_t)0 : (uint8_t)diff_level(sk[j], sk[j + 1]);
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kTreeThreads) k_tree_chains(const unsigned long long* __restrict__ keys, int n,
+                                                              int nleaf, uint8_t* __restrict__ dlev,
+                                                              uint16_t* __restrict__ chain,
+                                                              unsigned* __restrict__ hist, int nb,
+                                                              int* __restrict__ status) {
+  __shared__ unsigned long long sk[kTreeTile + 2 * kHalo + 1];
+  __shared__ uint8_t sd[kTreeTile + 2 * kHalo];
+  __shared__ unsigned hc[kNL], hl[kNL];
+  const int t0 = blockIdx.x * kTreeTile;
+  if (threadIdx.x < kNL) { hc[threadIdx.x] = 0; hl[threadIdx.x] = 0; }
+  load_d_from_keys(keys, n, t0, sd, sk);
+  for (int j = threadIdx.x; j < kTreeTile; j += blockDim.x)
+    if (t0 + j < n) dlev[t0 + j] = sd[kHalo + j];
+  bool anyfat = false;
+  const int i0 = t0 + threadIdx.x * kTreeItems;
+#pragma unroll 1
+  for (int k = 0; k < kTreeItems; k++) {
+    const int i = i0 + k;
+    if (i >= n) break;
+    bool fat = false;
+    const Chain c = make_chain(sd, kHalo + (i - t0), i, n, nleaf, &fat);
+    anyfat |= fat;
+    chain[i] = (uint16_t)(c.a | (c.b << 8));
+    if (c.a) {
+      for (int L = c.a; L <= c.b; L++) atomicAdd(&hc[L], 1u);
+      atomicAdd(&hl[c.b], 1u);
+    }
+  }
+  if (__any_sync(kFull, anyfat) && lane_id() == 0) set_status(status, kStatusDepth);
+  __syncthreads();
+  if (threadIdx.x < kNL) {
+    hist[threadIdx.x * nb + blockIdx.x] = hc[threadIdx.x];
+    hist[(kNL + threadIdx.x) * nb + blockIdx.x] = hl[threadIdx.x];
+  }
+}
+
+// One block: exclusive scan of each histogram row across tiles, rows chained
+// so that offsets are global (cells level-major; leaves ordered likewise).
+__global__ void __launch_bounds__(1024) k_tree_scan(unsigned* __restrict__ hist, int nb, int cell_cap,
+                                                    int leaf_cap, TreeInfo* __restrict__ info) {
+  __shared__ unsigned sh[32];
+  __shared__ unsigned carry;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  unsigned tot_cells = 0, tot_leaves = 0;
+  int nlevels = 0;
+  for (int row = 0; row < 2 * kNL; row++) {
+    const int L = row % kNL;
+    if (threadIdx.x == 0) {
+      carry = (row < kNL) ? tot_cells : tot_leaves;
+      if (row < kNL) info->level_beg[L] = (int)carry;
+    }
+    __syncthreads();
+    unsigned* h = hist + row * nb;
+    for (int b0 = 0; b0 < nb; b0 += 1024) {
+      const int b = b0 + threadIdx.x;
+      const unsigned v = (b < nb && L > 0) ? h[b] : 0u;
+      unsigned x = v;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned t = __shfl_up_sync(kFull, x, o);
+        if (lane >= o) x += t;
+      }
+      if (lane == 31) sh[w] = x;
+      __syncthreads();
+      if (w == 0) {
+        unsigned y = sh[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const unsigned t = __shfl_up_sync(kFull, y, o);
+          if (lane >= o) y += t;
+        }
+        sh[lane] = y;
+      }
+      __syncthreads();
+      const unsigned excl = (w ? sh[w - 1] : 0u) + x - v;
+      if (b < nb) h[b] = carry + excl;
+      __syncthreads();
+      if (threadIdx.x == 0) carry += sh[31];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      if (row < kNL) {
+        if (L > 0 && carry > tot_cells) nlevels = L;
+        tot_cells = carry;
+        info->level_end[L] = (int)carry;
+      } else {
+        tot_leaves = carry;
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    for (int L = kNL; L < kLevels; L++) info->level_beg[L] = info->level_end[L] = (int)tot_cells;
+    info->ncells = (int)tot_cells;
+    info->nleaves = (int)tot_leaves;
+    info->nnodes = (int)(tot_cells - tot_leaves);
+    info->nlevels = nlevels;
+    if ((int)tot_cells > cell_cap || (int)tot_leaves > leaf_cap) set_status(&info->status, kStatusCellCapacity);
+  }
+}
+
+__device__ __forceinline__ int lower_bound_u64(const unsigned long long* __restrict__ k, int lo, int hi,
+                                               unsigned long long t) {
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(k + mid) < t) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// first j >= lo with k[j] >= t, galloping from lo (k[lo-1] < t is known)
+__device__ __forceinline__ int gallop_u64(const unsigned long long* __restrict__ k, int lo, int n,
+                                          unsigned long long t) {
+  int step = 1, hi = lo;
+  while (hi < n && __ldg(k + hi) < t) {
+    lo = hi + 1;
+    hi += step;
+    step <<= 1;
+  }
+  return lower_bound_u64(k, lo, min(hi, n), t);
+}
+
+__global__ void __launch_bounds__(kTreeThreads) k_tree_cells(
+    const unsigned long long* __restrict__ keys, const uint8_t* __restrict__ dlev,
+    const uint16_t* __restrict__ chain, const unsigned* __restrict__ hist, int n, int nleaf, int nb, int cell_cap,
+    TreeInfo* __restrict__ info, uint4* __restrict__ cell_data, int* __restrict__ cell_parent,
+    int* __restrict__ leaf_list, int* __restrict__ mp_count) {
+  __shared__ uint8_t sd[kTreeTile + 2 * kHalo];
+  __shared__ uint16_t cpre[kNL][kTreeThreads];
+  __shared__ uint16_t lpre[kNL][kTreeThreads];
+  __shared__ unsigned boff[2][kNL];
+  if (info->ncells > cell_cap || info->nleaves > cell_cap) return;
+  const int t0 = blockIdx.x * kTreeTile;
+  for (int j = threadIdx.x; j < kTreeTile + 2 * kHalo; j += blockDim.x) {
+    const int p = t0 - kHalo + j;
+    sd[j] = (p <= 0 || p >= n) ? (uint8_t)0 : dlev[p];
+  }
+  if (threadIdx.x < kNL) {
+    boff[0][threadIdx.x] = hist[threadIdx.x * nb + blockIdx.x];
+    boff[1][threadIdx.x] = hist[(kNL + threadIdx.x) * nb + blockIdx.x];
+  }
+  const int i0 = t0 + threadIdx.x * kTreeItems;
+  int ca[kTreeItems], cb[kTreeItems];
+#pragma unroll
+  for (int k = 0; k < kTreeItems; k++) {
+    const int i = i0 + k;
+    const unsigned c = (i < n) ? (unsigned)chain[i] : 0u;
+    ca[k] = (int)(c & 255u);
+    cb[k] = (int)(c >> 8);
+  }
+  // per-thread totals per level
+  for (int L = 0; L < kNL; L++) {
+    unsigned cc = 0, lc = 0;
+#pragma unroll
+    for (int k = 0; k < kTreeItems; k++) {
+      cc += (ca[k] && ca[k] <= L && L <= cb[k]);
+      lc += (ca[k] && cb[k] == L);
+    }
+    cpre[L][threadIdx.x] = (uint16_t)cc;
+    lpre[L][threadIdx.x] = (uint16_t)lc;
+  }
+  __syncthreads();
+  // exclusive scans of the 2*kNL rows over the 256 threads (one warp per row)
+  {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int row = w; row < 2 * kNL; row += kTreeThreads / 32) {
+      uint16_t* r = (row < kNL) ? cpre[row] : lpre[row - kNL];
+      unsigned v[8], s = 0;
+#pragma unroll
+      for (int q = 0; q < 8; q++) { v[q] = r[lane * 8 + q]; s += v[q]; }
+      const unsigned incl = (unsigned)warp_incl_scan((int)s);
+      unsigned run = incl - s;
+#pragma unroll
+      for (int q = 0; q < 8; q++) { r[lane * 8 + q] = (uint16_t)run; run += v[q]; }
+    }
+  }
+  __syncthreads();
+#pragma unroll 1
+  for (int k = 0; k < kTreeItems; k++) {
+    const int i = i0 + k;
+    if (i >= n) break;
+    const int a = ca[k], b = cb[k];
+    if (!a) continue;
+    const int loc = kHalo + (i - t0);
+    const unsigned long long ki = keys[i];
+    // leaf index
+    {
+      int lk = 0;
+      for (int q = 0; q < k; q++) lk += (ca[q] && cb[q] == b);
+      const int leaf_idx = (int)(boff[1][b] + lpre[b][threadIdx.x]) + lk;
+      int lc = 0;
+      for (int q = 0; q < k; q++) lc += (ca[q] && ca[q] <= b && b <= cb[q]);
+      leaf_list[leaf_idx] = (int)(boff[0][b] + cpre[b][threadIdx.x]) + lc;
+    }
+    for (int L = a; L <= b; L++) {
+      int lc = 0;
+      for (int q = 0; q < k; q++) lc += (ca[q] && ca[q] <= L && L <= cb[q]);
+      const int cidx = (int)(boff[0][L] + cpre[L][threadIdx.x]) + lc;
+      const bool leaf = (L == b);
+      const int sh = 63 - 3 * L;
+      const unsigned long long pre = ki >> sh;
+      int pend;
+      bool small_leaf = false;
+      if (leaf) {
+        // count <= nleaf unless this is a fat level-21 leaf
+        for (int j = 1; j <= nleaf; j++) {
+          if (i + j >= n) { pend = n; small_leaf = true; break; }
+          if ((int)sd[loc + j] <= L) { pend = i + j; small_leaf = true; break; }
+        }
+      }
+      if (!small_leaf) pend = gallop_u64(keys, min(i + nleaf + 1, n), n, (pre + 1ull) << sh);
+      uint4* cd = cell_data + cidx;
+      if (L == 1) {
+        cd->x = (unsigned)(1 << 27);  // level-1 cells: parent 0, as the reference stores them
+        cell_parent[cidx] = -1;
+      }
+      unsigned ywd = 0xFFFFFFFFu;
+      if (!leaf) {
+        // children: runs of distinct level-(L+1) digit inside [i, pend)
+        int lc1 = 0;
+        for (int q = 0; q < k; q++) lc1 += (ca[q] && ca[q] <= L + 1 && L + 1 <= cb[q]);
+        const int first = (int)(boff[0][L + 1] + cpre[L + 1][threadIdx.x]) + lc1;
+        int nch = 0, lo = i;
+        for (int o = 1; o <= 8; o++) {
+          const int bnd = (o == 8) ? pend : lower_bound_u64(keys, lo, pend, ((pre << 3) | (unsigned long long)o) << (sh - 3));
+          if (bnd > lo) {
+            cell_data[first + nch].x = (unsigned)cidx | ((unsigned)(L + 1) << 27);
+            cell_parent[first + nch] = cidx;
+            nch++;
+          }
+          lo = bnd;
+        }
+        ywd = (unsigned)first | ((unsigned)(nch - 1) << 29);
+      }
+      cd->y = ywd;
+      cd->z = (unsigned)i;
+      cd->w = (unsigned)pend;
+      mp_count[cidx] = 0;
+    }
+  }
+}
+
+void build_tree(const unsigned long long* sorted_keys, int n, int nleaf, int cell_cap, int leaf_cap,
+                uint8_t* dlev, uint16_t* chain, unsigned* hist, TreeInfo* info, uint4* cell_data,
+                int* cell_parent, int* leaf_list, int* mp_count, cudaStream_t s) {
+  const int nb = tree_tiles(n);
+  k_tree_chains<<<nb, kTreeThreads, 0, s>>>(sorted_keys, n, nleaf, dlev, chain, hist, nb, &info->status);
+  k_tree_scan<<<1, 1024, 0, s>>>(hist, nb, cell_cap, leaf_cap, info);
+  k_tree_cells<<<nb, kTreeThreads, 0, s>>>(sorted_keys, dlev, chain, hist, n, nleaf, nb, cell_cap, info, cell_data,
+                                           cell_parent, leaf_list, mp_count);
+}
+
+}  // namespace bonsai

@@ -1,0 +1,827 @@
+// treecode.cu -- host side: the Treecode handle behind the C ABI
+// (include/bonsai_b200.h).  Owns every device buffer, sequences the stages on
+// the handle's stream without host round trips, and captures the whole step
+// as a CUDA graph.
+//
+// Data flow of one step (reference: treecode.cu:137-168):
+//   build     : box -> (tree key, PH key) per particle -> sort tree keys ->
+//               gather positions into tree order (jpos) -> cells
+//   multipoles: bottom-up from jpos
+//   groups    : sort PH keys -> groups -> gather the state (pos, vel, id)
+//               into PH order, so group particles are contiguous
+//   forces    : walk, acc in PH order (= state order)
+//   move      : leapfrog + energies on the state
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "../../include/bonsai_b200.h"
+#include "common.cuh"
+#include "kernels.cuh"
+
+using namespace bonsai;
+
+namespace {
+
+constexpr int kRingCap = 8192;  // per-warp level-list ring of the walk (ints)
+constexpr int kMaxLevelSplit = 7;
+
+template <class T>
+cudaError_t dalloc(T** p, size_t n) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  return cudaMalloc((void**)p, n * sizeof(T));
+}
+template <class T>
+void dfree(T** p) {
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+}
+
+struct Handle {
+  bonsai_params prm{};
+  int dev = 0, nsm = 0;
+  cudaStream_t st = nullptr;
+  int n = 0, cap_cells = 0;
+  // state, double-buffered: [par] holds the live state
+  float4* pos[2] = {nullptr, nullptr};
+  float4* vel[2] = {nullptr, nullptr};
+  int* id[2] = {nullptr, nullptr};
+  int par = 0;
+  float4* acc = nullptr;
+  float4* jpos = nullptr;
+  unsigned long long *tkey = nullptr, *pkey = nullptr, *kalt = nullptr;
+  int *tperm = nullptr, *pperm = nullptr, *valt = nullptr;
+  unsigned *sort_counts = nullptr, *bsum = nullptr;
+  uint8_t* dlev = nullptr;
+  uint16_t* chain = nullptr;
+  unsigned* hist = nullptr;
+  TreeInfo* info = nullptr;
+  uint4* cell_data = nullptr;
+  float4 *cell_open = nullptr, *cell_q0 = nullptr, *cell_q1 = nullptr;
+  int *cell_parent = nullptr, *leaf_list = nullptr, *mp_count = nullptr;
+  MpRec* rec = nullptr;
+  int2* groups = nullptr;
+  unsigned *g_count = nullptr, *g_seg = nullptr, *g_ng = nullptr;
+  int* ring = nullptr;
+  int walk_blocks[3] = {0, 0, 0};  // NI = 1, 2, 4
+  int ring_warps = 0;
+  unsigned* group_counter = nullptr;
+  unsigned long long* stats = nullptr;
+  double *move_partial = nullptr, *energies = nullptr;
+  unsigned *move_ticket = nullptr, *box_ticket = nullptr;
+  int* closing = nullptr;
+  Box* box = nullptr;
+  float* box_partial = nullptr;
+  uint16_t* ph_table = nullptr;
+  double *direct_part = nullptr, *direct_out = nullptr;
+  int* direct_sample = nullptr;
+  int direct_cap = 0;
+  int box_blocks = 0, move_blocks = 0;
+  int cur_nleaf = 16, cur_ncrit = 64, cur_ls = 5;
+  // stage bookkeeping for the eager API
+  bool built = false, mp_done = false, grouped = false, forced = false, moved_after_forces = false;
+  // graphs, one per state parity and phase (0: build+multipoles+groups, 1: walk, 2: move)
+  cudaGraphExec_t gexec[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+  int graph_kernels = 0;
+  bool graph_ok = false;
+
+  ~Handle() { release(); }
+
+  void release_graphs() {
+    for (int p = 0; p < 2; p++)
+      for (int k = 0; k < 3; k++)
+        if (gexec[p][k]) { cudaGraphExecDestroy(gexec[p][k]); gexec[p][k] = nullptr; }
+    graph_ok = false;
+  }
+
+  void release_particles() {
+    release_graphs();
+    for (int p = 0; p < 2; p++) { dfree(&pos[p]); dfree(&vel[p]); dfree(&id[p]); }
+    dfree(&acc); dfree(&jpos); dfree(&tkey); dfree(&pkey); dfree(&kalt);
+    dfree(&tperm); dfree(&pperm); dfree(&valt); dfree(&sort_counts); dfree(&bsum);
+    dfree(&dlev); dfree(&chain); dfree(&hist); dfree(&groups);
+    release_cells();
+    n = 0;
+  }
+  void release_cells() {
+    dfree(&cell_data); dfree(&cell_open); dfree(&cell_q0); dfree(&cell_q1);
+    dfree(&cell_parent); dfree(&leaf_list); dfree(&mp_count); dfree(&rec);
+    cap_cells = 0;
+  }
+  void release() {
+    if (st) cudaStreamSynchronize(st);
+    release_particles();
+    dfree(&info); dfree(&g_count); dfree(&g_seg); dfree(&g_ng); dfree(&ring);
+    dfree(&group_counter); dfree(&stats); dfree(&move_partial); dfree(&energies);
+    dfree(&move_ticket); dfree(&box_ticket); dfree(&closing); dfree(&box); dfree(&box_partial);
+    dfree(&ph_table); dfree(&direct_part); dfree(&direct_out); dfree(&direct_sample);
+    if (st) { cudaStreamDestroy(st); st = nullptr; }
+  }
+
+  int alloc_cells(int cap) {
+    release_graphs();
+    release_cells();
+    cap_cells = cap;
+    const size_t C = (size_t)cap;
+    BONSAI_CUDA_TRY(dalloc(&cell_data, C));
+    BONSAI_CUDA_TRY(dalloc(&cell_open, C));
+    BONSAI_CUDA_TRY(dalloc(&cell_q0, C));
+    BONSAI_CUDA_TRY(dalloc(&cell_q1, C));
+    BONSAI_CUDA_TRY(dalloc(&cell_parent, C));
+    BONSAI_CUDA_TRY(dalloc(&leaf_list, C));
+    BONSAI_CUDA_TRY(dalloc(&mp_count, C));
+    BONSAI_CUDA_TRY(dalloc(&rec, C));
+    return 0;
+  }
+
+  int init(const bonsai_params* p) {
+    prm = *p;
+    dev = p->device;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return BONSAI_ERR_NO_DEVICE;
+    if (dev < 0 || dev >= ndev) return BONSAI_ERR_ARG;
+    BONSAI_CUDA_TRY(cudaSetDevice(dev));
+    BONSAI_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    BONSAI_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    box_blocks = nsm * 4;
+    move_blocks = nsm * 4;
+    BONSAI_CUDA_TRY(dalloc(&info, 1));
+    BONSAI_CUDA_TRY(cudaMemset(info, 0, sizeof(TreeInfo)));
+    BONSAI_CUDA_TRY(dalloc(&g_count, (size_t)1 << (3 * kMaxLevelSplit)));
+    BONSAI_CUDA_TRY(dalloc(&g_seg, (size_t)1 << (3 * kMaxLevelSplit)));
+    BONSAI_CUDA_TRY(dalloc(&g_ng, (size_t)1 << (3 * kMaxLevelSplit)));
+    for (int k = 0; k < 3; k++) walk_blocks[k] = nsm * walk_blocks_per_sm(1 << k);
+    ring_warps = *std::max_element(walk_blocks, walk_blocks + 3) * (kWalkThreads / 32);
+    BONSAI_CUDA_TRY(dalloc(&ring, (size_t)ring_warps * kRingCap));
+    BONSAI_CUDA_TRY(dalloc(&group_counter, 1));
+    BONSAI_CUDA_TRY(dalloc(&stats, 4));
+    BONSAI_CUDA_TRY(dalloc(&move_partial, (size_t)move_blocks * 8));
+    BONSAI_CUDA_TRY(dalloc(&energies, 8));
+    BONSAI_CUDA_TRY(cudaMemset(energies, 0, 8 * sizeof(double)));
+    BONSAI_CUDA_TRY(dalloc(&move_ticket, 1));
+    BONSAI_CUDA_TRY(dalloc(&box_ticket, 1));
+    BONSAI_CUDA_TRY(cudaMemset(move_ticket, 0, sizeof(unsigned)));
+    BONSAI_CUDA_TRY(cudaMemset(box_ticket, 0, sizeof(unsigned)));
+    BONSAI_CUDA_TRY(dalloc(&closing, 1));
+    BONSAI_CUDA_TRY(cudaMemset(closing, 0, sizeof(int)));
+    BONSAI_CUDA_TRY(dalloc(&box, 1));
+    BONSAI_CUDA_TRY(dalloc(&box_partial, (size_t)box_blocks * 6));
+    std::vector<uint16_t> tab(384);
+    build_ph_table(tab.data());
+    BONSAI_CUDA_TRY(dalloc(&ph_table, 384));
+    BONSAI_CUDA_TRY(cudaMemcpy(ph_table, tab.data(), 384 * sizeof(uint16_t), cudaMemcpyHostToDevice));
+    cur_nleaf = p->nleaf;
+    cur_ncrit = p->ncrit;
+    cur_ls = p->level_split;
+    return 0;
+  }
+
+  int alloc(int nn) {
+    release_particles();
+    n = nn;
+    const size_t N = (size_t)nn;
+    for (int p = 0; p < 2; p++) {
+      BONSAI_CUDA_TRY(dalloc(&pos[p], N));
+      BONSAI_CUDA_TRY(dalloc(&vel[p], N));
+      BONSAI_CUDA_TRY(dalloc(&id[p], N));
+    }
+    BONSAI_CUDA_TRY(dalloc(&acc, N));
+    BONSAI_CUDA_TRY(cudaMemset(acc, 0, N * sizeof(float4)));
+    BONSAI_CUDA_TRY(dalloc(&jpos, N));
+    BONSAI_CUDA_TRY(dalloc(&tkey, N));
+    BONSAI_CUDA_TRY(dalloc(&pkey, N));
+    BONSAI_CUDA_TRY(dalloc(&kalt, N));
+    BONSAI_CUDA_TRY(dalloc(&tperm, N));
+    BONSAI_CUDA_TRY(dalloc(&pperm, N));
+    BONSAI_CUDA_TRY(dalloc(&valt, N));
+    BONSAI_CUDA_TRY(dalloc(&sort_counts, (size_t)256 * sort_tiles(nn)));
+    const int scan_m = std::max(256 * sort_tiles(nn), 1 << (3 * kMaxLevelSplit));
+    BONSAI_CUDA_TRY(dalloc(&bsum, (size_t)scan_blocks(scan_m) + 1));
+    BONSAI_CUDA_TRY(dalloc(&dlev, N));
+    BONSAI_CUDA_TRY(dalloc(&chain, N));
+    BONSAI_CUDA_TRY(dalloc(&hist, (size_t)2 * (kMaxLevel + 1) * tree_tiles(nn)));
+    BONSAI_CUDA_TRY(dalloc(&groups, N));
+    int rc = alloc_cells(2 * nn + 4096);
+    if (rc) return rc;
+    par = 0;
+    built = mp_done = grouped = forced = moved_after_forces = false;
+    return 0;
+  }
+
+  // ---------------- stages (enqueue only) ----------------
+  void enq_build(int nleaf) {
+    cudaMemsetAsync(box_ticket, 0, sizeof(unsigned), st);
+    k_box<<<box_blocks, 256, 0, st>>>(pos[par], n, box_partial, box_ticket, box, &info->status);
+    k_keys<<<nsm * 8, 256, 0, st>>>(pos[par], n, box, ph_table, tkey, pkey);
+    radix_sort_pairs(tkey, kalt, tperm, valt, nullptr, n, sort_counts, bsum, 8, st);
+    k_gather_pos<<<nsm * 8, 256, 0, st>>>(tperm, n, pos[par], jpos);
+    build_tree(tkey, n, nleaf, cap_cells, cap_cells, dlev, chain, hist, info, cell_data, cell_parent, leaf_list,
+               mp_count, st);
+  }
+  void enq_multipoles() {
+    k_multipoles<<<nsm * 8, 256, 0, st>>>(leaf_list, info, cell_data, cell_parent, jpos, 1.0f / prm.theta, rec,
+                                          cell_open, cell_q0, cell_q1, mp_count, cap_cells);
+  }
+  void enq_groups(int ls, int ncrit) {
+    radix_sort_pairs(pkey, kalt, pperm, valt, nullptr, n, sort_counts, bsum, 8, st);
+    make_groups(pkey, n, ls, ncrit, g_count, g_seg, g_ng, bsum, groups, n, info, st);
+    const int q = par ^ 1;
+    k_gather_state<<<nsm * 8, 256, 0, st>>>(pperm, n, pos[par], vel[par], id[par], pos[q], vel[q], id[q]);
+    par = q;
+  }
+  void enq_forces(int ncrit) {
+    const int ni = walk_ni(ncrit);
+    const int k = ni == 1 ? 0 : (ni == 2 ? 1 : 2);
+    cudaMemsetAsync(group_counter, 0, sizeof(unsigned), st);
+    cudaMemsetAsync(stats, 0, 4 * sizeof(unsigned long long), st);
+    launch_walk(ni, walk_blocks[k], groups, info, pos[par], jpos, cell_data, cell_open, cell_q0, cell_q1,
+                prm.eps * prm.eps, acc, ring, kRingCap, group_counter, stats, &info->status, st);
+  }
+  void enq_move(bool write) {
+    launch_move_wrapper(write);
+  }
+  void launch_move_wrapper(bool write);
+
+  void enq_step() {
+    enq_build(cur_nleaf);
+    enq_multipoles();
+    enq_groups(cur_ls, cur_ncrit);
+    enq_forces(cur_ncrit);
+    enq_move(true);
+  }
+
+  void enq_phase(int k) {
+    if (k == 0) {
+      enq_build(cur_nleaf);
+      enq_multipoles();
+      enq_groups(cur_ls, cur_ncrit);
+    } else if (k == 1) {
+      enq_forces(cur_ncrit);
+    } else {
+      enq_move(true);
+    }
+  }
+
+  int capture_graphs() {
+    release_graphs();
+    const int par0 = par;
+    graph_kernels = 0;
+    for (int p = 0; p < 2; p++) {
+      par = p;
+      for (int k = 0; k < 3; k++) {
+        cudaGraph_t g = nullptr;
+        BONSAI_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        enq_phase(k);
+        cudaError_t e = cudaStreamEndCapture(st, &g);
+        if (e != cudaSuccess) { par = par0; return -(int)e - 1000; }
+        if (p == 0) {
+          size_t nn = 0;
+          cudaGraphGetNodes(g, nullptr, &nn);
+          std::vector<cudaGraphNode_t> nodes(nn);
+          cudaGraphGetNodes(g, nodes.data(), &nn);
+          for (size_t q = 0; q < nn; q++) {
+            cudaGraphNodeType ty;
+            cudaGraphNodeGetType(nodes[q], &ty);
+            graph_kernels += (ty == cudaGraphNodeTypeKernel);
+          }
+        }
+        e = cudaGraphInstantiate(&gexec[p][k], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) { par = par0; return -(int)e - 1000; }
+      }
+    }
+    par = par0;
+    graph_ok = true;
+    return 0;
+  }
+
+  int launch_graph_step(cudaEvent_t* ev) {
+    for (int k = 0; k < 3; k++) {
+      if (ev) BONSAI_CUDA_TRY(cudaEventRecord(ev[k], st));
+      BONSAI_CUDA_TRY(cudaGraphLaunch(gexec[par][k], st));
+    }
+    if (ev) BONSAI_CUDA_TRY(cudaEventRecord(ev[3], st));
+    par ^= 1;
+    return 0;
+  }
+
+  int read_status(bool clear) {
+    int s = 0;
+    cudaError_t e = cudaMemcpyAsync(&s, &info->status, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return -(int)e - 1000;
+    if (clear && s) {
+      e = cudaMemsetAsync(&info->status, 0, sizeof(int), st);
+      if (e != cudaSuccess) return -(int)e - 1000;
+    }
+    return s;
+  }
+};
+
+void Handle::launch_move_wrapper(bool write) {
+  launch_move(pos[par], vel[par], acc, n, prm.dt, closing, prm.eps, write ? 1 : 0, move_partial, move_blocks,
+              move_ticket, energies, st);
+}
+
+Handle* H(bonsai_handle h) { return reinterpret_cast<Handle*>(h); }
+
+int check_params(const bonsai_params* p) {
+  if (!p) return BONSAI_ERR_ARG;
+  if (!(p->theta > 0.f) || !(p->eps >= 0.f) || !std::isfinite(p->dt)) return BONSAI_ERR_ARG;
+  if (p->nleaf < 1 || p->nleaf > 64) return BONSAI_ERR_ARG;
+  if (p->ncrit < 1 || p->ncrit > 128) return BONSAI_ERR_ARG;
+  if (p->level_split < 1 || p->level_split > kMaxLevelSplit) return BONSAI_ERR_ARG;
+  return 0;
+}
+
+int last_cuda(void) {
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : -(int)e - 1000;
+}
+
+}  // namespace
+
+// Plummer initial conditions (host): plummer.cpp
+extern "C" int bonsai_plummer_impl(long n, unsigned int seed, float* pos4, float* vel4);
+
+extern "C" {
+
+void bonsai_default_params(bonsai_params* p) {
+  if (!p) return;
+  p->theta = 0.75f;
+  p->eps = 0.01f;
+  p->nleaf = 16;
+  p->ncrit = 64;
+  p->level_split = 5;
+  p->dt = 1.0f / 64.0f;
+  p->device = 0;
+}
+
+int bonsai_create(const bonsai_params* p, bonsai_handle* out) {
+  if (!out) return BONSAI_ERR_ARG;
+  *out = nullptr;
+  int rc = check_params(p);
+  if (rc) return rc;
+  Handle* h = new Handle();
+  rc = h->init(p);
+  if (rc) { delete h; return rc; }
+  *out = reinterpret_cast<bonsai_handle>(h);
+  return 0;
+}
+
+int bonsai_destroy(bonsai_handle hh) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  cudaSetDevice(h->dev);
+  delete h;
+  return 0;
+}
+
+int bonsai_alloc(bonsai_handle hh, int n) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (n < 1) return BONSAI_ERR_ARG;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  return h->alloc(n);
+}
+
+int bonsai_set_params(bonsai_handle hh, const bonsai_params* p) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  const int rc = check_params(p);
+  if (rc) return rc;
+  if (p->device != h->dev) return BONSAI_ERR_ARG;
+  h->prm = *p;
+  h->cur_nleaf = p->nleaf;
+  h->cur_ncrit = p->ncrit;
+  h->cur_ls = p->level_split;
+  h->release_graphs();
+  return 0;
+}
+
+static int set_particles_impl(Handle* h, const float* pos4, const float* vel4, int n, cudaMemcpyKind kind) {
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (!pos4 || !vel4 || n < 1) return BONSAI_ERR_ARG;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  if (n != h->n) {
+    const int rc = h->alloc(n);
+    if (rc) return rc;
+  }
+  const size_t bytes = (size_t)n * sizeof(float4);
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(h->pos[h->par], pos4, bytes, kind, h->st));
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(h->vel[h->par], vel4, bytes, kind, h->st));
+  k_iota<<<h->nsm * 4, 256, 0, h->st>>>(h->id[h->par], n);
+  BONSAI_CUDA_TRY(cudaMemsetAsync(h->closing, 0, sizeof(int), h->st));
+  h->built = h->mp_done = h->grouped = h->forced = h->moved_after_forces = false;
+  return last_cuda();
+}
+
+int bonsai_set_particles(bonsai_handle hh, const float* pos4, const float* vel4, int n) {
+  return set_particles_impl(H(hh), pos4, vel4, n, cudaMemcpyHostToDevice);
+}
+int bonsai_set_particles_device(bonsai_handle hh, const float* pos4, const float* vel4, int n) {
+  return set_particles_impl(H(hh), pos4, vel4, n, cudaMemcpyDeviceToDevice);
+}
+
+static int get_particles_impl(Handle* h, float* pos4, float* vel4, float* acc4, cudaMemcpyKind kind) {
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (h->n == 0) return BONSAI_ERR_NOT_ALLOCATED;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  const int n = h->n;
+  const size_t bytes = (size_t)n * sizeof(float4);
+  float4* tmp = h->pos[h->par ^ 1];  // the idle state buffer
+  const float4* src[3] = {h->pos[h->par], h->vel[h->par], h->acc};
+  float* dst[3] = {pos4, vel4, acc4};
+  for (int k = 0; k < 3; k++) {
+    if (!dst[k]) continue;
+    k_scatter_by_id<<<h->nsm * 8, 256, 0, h->st>>>(h->id[h->par], n, src[k], tmp);
+    BONSAI_CUDA_TRY(cudaMemcpyAsync(dst[k], tmp, bytes, kind, h->st));
+  }
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  return last_cuda();
+}
+
+int bonsai_get_particles(bonsai_handle hh, float* pos4, float* vel4, float* acc4) {
+  return get_particles_impl(H(hh), pos4, vel4, acc4, cudaMemcpyDeviceToHost);
+}
+int bonsai_get_particles_device(bonsai_handle hh, float* pos4, float* vel4, float* acc4) {
+  return get_particles_impl(H(hh), pos4, vel4, acc4, cudaMemcpyDeviceToDevice);
+}
+
+int bonsai_build_tree(bonsai_handle hh, int nleaf) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (h->n == 0) return BONSAI_ERR_NOT_ALLOCATED;
+  if (nleaf < 1 || nleaf > 64) return BONSAI_ERR_ARG;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  h->cur_nleaf = nleaf;
+  for (int attempt = 0; attempt < 4; attempt++) {
+    h->enq_build(nleaf);
+    int nc = 0;
+    BONSAI_CUDA_TRY(cudaMemcpyAsync(&nc, &h->info->ncells, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+    BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+    if (nc <= h->cap_cells) break;
+    // grow the cell arrays and rebuild (the capacity bit is cleared)
+    const int rc = h->alloc_cells(nc + nc / 4 + 4096);
+    if (rc) return rc;
+    BONSAI_CUDA_TRY(cudaMemsetAsync(&h->info->status, 0, sizeof(int), h->st));
+  }
+  h->built = true;
+  h->mp_done = h->grouped = h->forced = h->moved_after_forces = false;
+  return last_cuda();
+}
+
+int bonsai_compute_multipoles(bonsai_handle hh) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (!h->built) return BONSAI_ERR_ORDER;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  h->enq_multipoles();
+  h->mp_done = true;
+  return last_cuda();
+}
+
+int bonsai_make_groups(bonsai_handle hh, int level_split, int ncrit) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (!h->built) return BONSAI_ERR_ORDER;
+  level_split = std::max(1, level_split);  // makeGroups.cu:259
+  if (level_split > kMaxLevelSplit || ncrit < 1 || ncrit > 128) return BONSAI_ERR_ARG;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  if (h->grouped) return BONSAI_ERR_ORDER;  // the state was already reordered for this tree
+  h->cur_ls = level_split;
+  h->cur_ncrit = ncrit;
+  h->enq_groups(level_split, ncrit);
+  h->grouped = true;
+  return last_cuda();
+}
+
+int bonsai_compute_forces(bonsai_handle hh, int intcount, double* out) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (!h->built || !h->mp_done || !h->grouped) return BONSAI_ERR_ORDER;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  h->enq_forces(h->cur_ncrit);
+  h->forced = true;
+  h->moved_after_forces = false;
+  if (intcount && out) {
+    unsigned long long s[4];
+    BONSAI_CUDA_TRY(cudaMemcpyAsync(s, h->stats, sizeof(s), cudaMemcpyDeviceToHost, h->st));
+    BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+    out[0] = (double)s[1] / h->n;  // <direct>
+    out[1] = (double)s[3];         // max direct
+    out[2] = (double)s[0] / h->n;  // <approx>
+    out[3] = (double)s[2];         // max approx
+  }
+  return last_cuda();
+}
+
+int bonsai_move_particles(bonsai_handle hh) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (!h->forced || h->moved_after_forces) return BONSAI_ERR_ORDER;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  h->enq_move(true);
+  h->moved_after_forces = true;
+  h->built = h->mp_done = h->grouped = false;
+  return last_cuda();
+}
+
+int bonsai_compute_energies(bonsai_handle hh, double* out) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (h->n == 0) return BONSAI_ERR_NOT_ALLOCATED;
+  if (!h->forced) return BONSAI_ERR_ORDER;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  if (!h->moved_after_forces) h->enq_move(false);
+  double e[8];
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(e, h->energies, sizeof(e), cudaMemcpyDeviceToHost, h->st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  if (out) std::memcpy(out, e, sizeof(e));
+  return last_cuda();
+}
+
+int bonsai_step(bonsai_handle hh, int nsteps, int use_graph) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (h->n == 0) return BONSAI_ERR_NOT_ALLOCATED;
+  if (nsteps < 0) return BONSAI_ERR_ARG;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  if (use_graph && !h->graph_ok) {
+    const int rc = h->capture_graphs();
+    if (rc) return rc;
+  }
+  for (int s = 0; s < nsteps; s++) {
+    if (use_graph) {
+      const int rc = h->launch_graph_step(nullptr);
+      if (rc) return rc;
+    } else {
+      h->enq_step();
+    }
+  }
+  if (nsteps > 0) {
+    h->built = h->mp_done = h->grouped = false;
+    h->forced = h->moved_after_forces = true;
+  }
+  return last_cuda();
+}
+
+int bonsai_step_timed(bonsai_handle hh, int nsteps, float* phase_ms) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (h->n == 0) return BONSAI_ERR_NOT_ALLOCATED;
+  if (nsteps < 1 || !phase_ms) return BONSAI_ERR_ARG;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  if (!h->graph_ok) {
+    const int rc = h->capture_graphs();
+    if (rc) return rc;
+  }
+  std::vector<cudaEvent_t> ev((size_t)4 * nsteps);
+  for (auto& e : ev) BONSAI_CUDA_TRY(cudaEventCreate(&e));
+  int rc = 0;
+  for (int s = 0; s < nsteps && !rc; s++) rc = h->launch_graph_step(&ev[(size_t)4 * s]);
+  if (!rc) {
+    BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+    for (int s = 0; s < nsteps; s++) {
+      cudaEvent_t* e = &ev[(size_t)4 * s];
+      cudaEventElapsedTime(&phase_ms[4 * s + 0], e[0], e[1]);
+      cudaEventElapsedTime(&phase_ms[4 * s + 1], e[1], e[2]);
+      cudaEventElapsedTime(&phase_ms[4 * s + 2], e[2], e[3]);
+      cudaEventElapsedTime(&phase_ms[4 * s + 3], e[0], e[3]);
+    }
+    cudaEventElapsedTime(&phase_ms[4 * nsteps], ev[0], ev[(size_t)4 * nsteps - 1]);
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  h->built = h->mp_done = h->grouped = false;
+  h->forced = h->moved_after_forces = true;
+  return rc ? rc : last_cuda();
+}
+
+int bonsai_graph_kernel_count(bonsai_handle hh) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (h->n == 0) return BONSAI_ERR_NOT_ALLOCATED;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  if (!h->graph_ok) {
+    const int rc = h->capture_graphs();
+    if (rc) return rc;
+  }
+  return h->graph_kernels;
+}
+
+int bonsai_get_stats(bonsai_handle hh, unsigned long long* out) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (!out) return BONSAI_ERR_ARG;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(out, h->stats, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  return 0;
+}
+
+int bonsai_synchronize(bonsai_handle hh) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  const int c = last_cuda();
+  if (c) return c;
+  return h->read_status(true);
+}
+
+void* bonsai_stream(bonsai_handle hh) {
+  Handle* h = H(hh);
+  return h ? (void*)h->st : nullptr;
+}
+
+const char* bonsai_error_string(int code) {
+  if (code == 0) return "ok";
+  if (code <= -1000) return cudaGetErrorString((cudaError_t)(-(code + 1000)));
+  switch (code) {
+    case BONSAI_ERR_HANDLE: return "invalid handle";
+    case BONSAI_ERR_NOT_ALLOCATED: return "particles not allocated";
+    case BONSAI_ERR_ORDER: return "stage called before the stage it depends on";
+    case BONSAI_ERR_ARG: return "invalid argument";
+    case BONSAI_ERR_NO_DEVICE: return "no CUDA device";
+    default: break;
+  }
+  if (code > 0) {
+    if (code & BONSAI_STATUS_CELL_CAPACITY) return "cell capacity exceeded";
+    if (code & BONSAI_STATUS_WALK_STACK) return "walk level list overflow";
+    if (code & BONSAI_STATUS_NONFINITE) return "non-finite particle coordinate";
+    if (code & BONSAI_STATUS_GROUP_CAPACITY) return "group capacity exceeded";
+    if (code & BONSAI_STATUS_DEPTH) return "tree deeper than 21 levels (fat leaf kept)";
+    if (code & BONSAI_STATUS_BAD_PARAM) return "bad parameter";
+  }
+  return "unknown";
+}
+
+int bonsai_get_tree_info(bonsai_handle hh, bonsai_tree_info* out) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (!out) return BONSAI_ERR_ARG;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  TreeInfo ti;
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(&ti, h->info, sizeof(ti), cudaMemcpyDeviceToHost, h->st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  out->ncells = ti.ncells;
+  out->nleaves = ti.nleaves;
+  out->nnodes = ti.nnodes;
+  out->nlevels = ti.nlevels;
+  out->ngroups = ti.ngroups;
+  out->status = ti.status;
+  for (int L = 0; L < 32; L++) { out->level_beg[L] = ti.level_beg[L]; out->level_end[L] = ti.level_end[L]; }
+  return 0;
+}
+
+int bonsai_get_box(bonsai_handle hh, float* box4) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (!box4) return BONSAI_ERR_ARG;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(box4, h->box, 4 * sizeof(float), cudaMemcpyDeviceToHost, h->st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  return 0;
+}
+
+int bonsai_get_keys(bonsai_handle hh, uint64_t* tk, int* tp, uint64_t* pk, int* pp, int* ids) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (h->n == 0) return BONSAI_ERR_NOT_ALLOCATED;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  const size_t N = (size_t)h->n;
+  if (tk) BONSAI_CUDA_TRY(cudaMemcpyAsync(tk, h->tkey, N * 8, cudaMemcpyDeviceToHost, h->st));
+  if (tp) BONSAI_CUDA_TRY(cudaMemcpyAsync(tp, h->tperm, N * 4, cudaMemcpyDeviceToHost, h->st));
+  if (pk) BONSAI_CUDA_TRY(cudaMemcpyAsync(pk, h->pkey, N * 8, cudaMemcpyDeviceToHost, h->st));
+  if (pp) BONSAI_CUDA_TRY(cudaMemcpyAsync(pp, h->pperm, N * 4, cudaMemcpyDeviceToHost, h->st));
+  // ids of the order the build saw: the state buffer before the PH gather
+  const int q = h->grouped ? (h->par ^ 1) : h->par;
+  if (ids) BONSAI_CUDA_TRY(cudaMemcpyAsync(ids, h->id[q], N * 4, cudaMemcpyDeviceToHost, h->st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  return 0;
+}
+
+int bonsai_get_cells(bonsai_handle hh, uint32_t* cell_data, float* size4, float* mono4, float* quad0, float* quad1,
+                     int* leaf_list, int* parent) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (!h->built) return BONSAI_ERR_ORDER;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  TreeInfo ti;
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(&ti, h->info, sizeof(ti), cudaMemcpyDeviceToHost, h->st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  const size_t C = (size_t)ti.ncells;
+  if (cell_data) BONSAI_CUDA_TRY(cudaMemcpyAsync(cell_data, h->cell_data, C * 16, cudaMemcpyDeviceToHost, h->st));
+  if (leaf_list)
+    BONSAI_CUDA_TRY(cudaMemcpyAsync(leaf_list, h->leaf_list, (size_t)ti.nleaves * 4, cudaMemcpyDeviceToHost, h->st));
+  if (parent) BONSAI_CUDA_TRY(cudaMemcpyAsync(parent, h->cell_parent, C * 4, cudaMemcpyDeviceToHost, h->st));
+  if ((size4 || mono4 || quad0 || quad1) && C > 0) {
+    if (!h->mp_done) return BONSAI_ERR_ORDER;
+    float4 *s = nullptr, *m = nullptr, *q0 = nullptr;
+    float2* q1 = nullptr;
+    BONSAI_CUDA_TRY(dalloc(&s, C));
+    BONSAI_CUDA_TRY(dalloc(&m, C));
+    BONSAI_CUDA_TRY(dalloc(&q0, C));
+    BONSAI_CUDA_TRY(dalloc(&q1, C));
+    k_multipoles_ref_layout<<<h->nsm * 4, 256, 0, h->st>>>(h->info, h->cell_open, h->rec, s, m, q0, q1);
+    if (size4) BONSAI_CUDA_TRY(cudaMemcpyAsync(size4, s, C * 16, cudaMemcpyDeviceToHost, h->st));
+    if (mono4) BONSAI_CUDA_TRY(cudaMemcpyAsync(mono4, m, C * 16, cudaMemcpyDeviceToHost, h->st));
+    if (quad0) BONSAI_CUDA_TRY(cudaMemcpyAsync(quad0, q0, C * 16, cudaMemcpyDeviceToHost, h->st));
+    if (quad1) BONSAI_CUDA_TRY(cudaMemcpyAsync(quad1, q1, C * 8, cudaMemcpyDeviceToHost, h->st));
+    BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+    dfree(&s); dfree(&m); dfree(&q0); dfree(&q1);
+  }
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  return last_cuda();
+}
+
+int bonsai_get_groups(bonsai_handle hh, int* groups) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (!h->grouped && !h->forced) return BONSAI_ERR_ORDER;
+  if (!groups) return BONSAI_ERR_ARG;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  int ng = 0;
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(&ng, &h->info->ngroups, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(groups, h->groups, (size_t)ng * 8, cudaMemcpyDeviceToHost, h->st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  return 0;
+}
+
+int bonsai_get_walk_arrays(bonsai_handle hh, float* ipos4, float* jpos4, float* acc4, int* ids) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (h->n == 0) return BONSAI_ERR_NOT_ALLOCATED;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  const size_t N = (size_t)h->n;
+  if (ipos4) BONSAI_CUDA_TRY(cudaMemcpyAsync(ipos4, h->pos[h->par], N * 16, cudaMemcpyDeviceToHost, h->st));
+  if (jpos4) BONSAI_CUDA_TRY(cudaMemcpyAsync(jpos4, h->jpos, N * 16, cudaMemcpyDeviceToHost, h->st));
+  if (acc4) BONSAI_CUDA_TRY(cudaMemcpyAsync(acc4, h->acc, N * 16, cudaMemcpyDeviceToHost, h->st));
+  if (ids) BONSAI_CUDA_TRY(cudaMemcpyAsync(ids, h->id[h->par], N * 4, cudaMemcpyDeviceToHost, h->st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  return 0;
+}
+
+int bonsai_direct_fp64(bonsai_handle hh, const int* sample, int ns, int include_self, double* out) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (h->n == 0) return BONSAI_ERR_NOT_ALLOCATED;
+  if (!sample || !out || ns < 1) return BONSAI_ERR_ARG;
+  for (int s = 0; s < ns; s++)
+    if (sample[s] < 0 || sample[s] >= h->n) return BONSAI_ERR_ARG;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  const int nsplit = std::max(1, std::min(512, (h->nsm * 8 * 256) / std::max(ns, 1)));
+  if (ns > h->direct_cap || !h->direct_part) {
+    dfree(&h->direct_part); dfree(&h->direct_out); dfree(&h->direct_sample);
+    BONSAI_CUDA_TRY(dalloc(&h->direct_part, (size_t)512 * ns * 4));
+    BONSAI_CUDA_TRY(dalloc(&h->direct_out, (size_t)ns * 4));
+    BONSAI_CUDA_TRY(dalloc(&h->direct_sample, (size_t)ns));
+    h->direct_cap = ns;
+  }
+  // positions in caller order into the idle state buffer
+  float4* tmp = h->pos[h->par ^ 1];
+  k_scatter_by_id<<<h->nsm * 8, 256, 0, h->st>>>(h->id[h->par], h->n, h->pos[h->par], tmp);
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(h->direct_sample, sample, (size_t)ns * 4, cudaMemcpyHostToDevice, h->st));
+  const double e2 = (double)h->prm.eps * (double)h->prm.eps;
+  launch_direct_fp64(tmp, h->n, h->direct_sample, ns, e2, include_self, h->direct_part, nsplit, h->direct_out, h->st);
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(out, h->direct_out, (size_t)ns * 4 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  return last_cuda();
+}
+
+int bonsai_plummer(long n, unsigned int seed, float* pos4, float* vel4) {
+  if (n < 1 || !pos4 || !vel4) return BONSAI_ERR_ARG;
+  return bonsai_plummer_impl(n, seed, pos4, vel4);
+}
+
+int bonsai_fp32_peak(int device, double* tflops) {
+  if (!tflops) return BONSAI_ERR_ARG;
+  BONSAI_CUDA_TRY(cudaSetDevice(device));
+  int nsm = 0;
+  BONSAI_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+  cudaStream_t st;
+  BONSAI_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  float* scratch = nullptr;
+  BONSAI_CUDA_TRY(dalloc(&scratch, (size_t)nsm * 8));
+  *tflops = fma_probe_tflops(nsm, st, scratch);
+  cudaStreamSynchronize(st);
+  dfree(&scratch);
+  cudaStreamDestroy(st);
+  return last_cuda();
+}
+
+void* bonsai_host_alloc(size_t bytes) {
+  void* p = nullptr;
+  if (cudaMallocHost(&p, bytes) != cudaSuccess) return nullptr;
+  return p;
+}
+
+void bonsai_host_free(void* p) {
+  if (p) cudaFreeHost(p);
+}
+
+}  // extern "C"

@@ -1,0 +1,312 @@
+// walk.cu -- the tree walk: one warp per group, FP32, persistent.
+//
+// Semantics follow treewalk / treewalk_warp (computeForces.cu:229-619):
+//   * a warp takes the next group from an atomic counter (:516-522) and holds
+//     NI particles per lane (NI = 1 for nCrit <= 32, 2 for <= 64, 4 for <= 128);
+//   * group box from the min/max of its particles (:531-555);
+//   * breadth-first walk from all level-1 cells (:259-263, :511-512);
+//   * a cell is opened when split_node_grav_impbh holds (:30-54) or when it
+//     holds fewer than 3 particles (:284-285);
+//   * opened nodes push their children to the next level (:291-334);
+//     cells that stay closed (leaves too) are quadrupoles (:337-367);
+//     opened leaves are evaluated particle by particle, i==j included
+//     (:370-430);
+//   * acc = (ax, ay, az, potential) in group (PH) order (:611-617), interaction
+//     counts per particle (:568-609).
+// B200 design:
+//   * explicit __shfl_sync / __ballot_sync / redux.sync cooperation, no
+//     implicit warp-synchronous shared memory;
+//   * range expansion (children, leaf particles) with a shuffle binary search
+//     over the warp's inclusive scan: 32 outputs per step;
+//   * the level lists live in a per-warp ring in global memory (L1/L2
+//     resident), bounded; overflow sets a status bit, never traps;
+//   * accepted cells and direct particles are staged by value in per-warp
+//     64-entry shared-memory rings as they are found, so the 32-wide
+//     evaluation loops read broadcast LDS.128 only;
+//   * the quadrupole kernel uses mass-weighted, pre-scaled moments
+//     (34 FP32 operations + 1 MUFU per interaction; the reference's
+//     formulation, counted as 64 flops by treecode.cu:149-158, is the same
+//     algebra).
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace bonsai {
+
+constexpr int kWalkWarps = kWalkThreads / 32;
+
+struct IPart {
+  float x, y, z;
+};
+
+// Opening test of split_node_grav_impbh (computeForces.cu:30-54), explicitly
+// rounded so that the CPU restatement reproduces it bit for bit.
+__device__ __forceinline__ bool open_cell(const float4 co, const float3 gc, const float3 gs) {
+  float dx = __fsub_rn(fabsf(__fsub_rn(gc.x, co.x)), gs.x);
+  float dy = __fsub_rn(fabsf(__fsub_rn(gc.y, co.y)), gs.y);
+  float dz = __fsub_rn(fabsf(__fsub_rn(gc.z, co.z)), gs.z);
+  dx = __fmul_rn(__fadd_rn(dx, fabsf(dx)), 0.5f);
+  dy = __fmul_rn(__fadd_rn(dy, fabsf(dy)), 0.5f);
+  dz = __fmul_rn(__fadd_rn(dz, fabsf(dz)), 0.5f);
+  const float ds2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+  return ds2 < fabsf(co.w);
+}
+
+// quadrupole: a0 = (COM, -0.5 tr I), a1 = (M, 3Ixx, 3Iyy, 3Izz), a2 = (3Ixy, 3Ixz, 3Iyz, 1.5 tr I)
+//   phi -= M/r - 0.5 tr/r^3 + 1.5 dIdr/r^5
+//   a   += [-M + u (1.5 tr - 7.5 dIdr u)] dr / r^3 + 3 I dr / r^5,   dr = x_i - COM
+__device__ __forceinline__ void quad_acc(float4& acc, const IPart& p, const float4 a0, const float4 a1,
+                                         const float4 a2, float eps2) {
+  const float dx = p.x - a0.x, dy = p.y - a0.y, dz = p.z - a0.z;
+  const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
+  const float rinv = rsqrtf(r2);
+  const float u = rinv * rinv;
+  const float qx = fmaf(a2.y, dz, fmaf(a2.x, dy, a1.y * dx));
+  const float qy = fmaf(a2.z, dz, fmaf(a1.z, dy, a2.x * dx));
+  const float qz = fmaf(a1.w, dz, fmaf(a2.z, dy, a2.y * dx));
+  const float qrr = fmaf(qz, dz, fmaf(qy, dy, qx * dx));  // 3 dIdr
+  const float r3 = rinv * u;
+  const float r5 = r3 * u;
+  const float b = qrr * u;
+  const float ca = fmaf(u, fmaf(-2.5f, b, a2.w), -a1.x) * r3;
+  acc.x = fmaf(r5, qx, fmaf(ca, dx, acc.x));
+  acc.y = fmaf(r5, qy, fmaf(ca, dy, acc.y));
+  acc.z = fmaf(r5, qz, fmaf(ca, dz, acc.z));
+  const float pp = fmaf(u, fmaf(0.5f, b, a0.w), a1.x);
+  acc.w = fmaf(-rinv, pp, acc.w);
+}
+
+// monopole (computeForces.cu:58-78): dr = x_j - x_i
+__device__ __forceinline__ void mono_acc(float4& acc, const IPart& p, const float4 j, float eps2) {
+  const float dx = j.x - p.x, dy = j.y - p.y, dz = j.z - p.z;
+  const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
+  const float rinv = rsqrtf(r2);
+  const float mr = j.w * rinv;
+  const float mr3 = mr * rinv * rinv;
+  acc.w -= mr;
+  acc.x = fmaf(mr3, dx, acc.x);
+  acc.y = fmaf(mr3, dy, acc.y);
+  acc.z = fmaf(mr3, dz, acc.z);
+}
+
+// binary search over the warp's inclusive scan: the lane whose range holds s
+__device__ __forceinline__ int find_src(int incl, int s) {
+  int src = 0;
+#pragma unroll
+  for (int step = 16; step >= 1; step >>= 1) {
+    const int v = __shfl_sync(kFull, incl, src + step - 1);
+    if (v <= s) src += step;
+  }
+  return src;
+}
+
+template <int NI>
+__global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
+    k_walk(const int2* __restrict__ groups, const TreeInfo* __restrict__ info, const float4* __restrict__ ipos,
+           const float4* __restrict__ jpos, const uint4* __restrict__ cell_data,
+           const float4* __restrict__ cell_open, const float4* __restrict__ cell_q0,
+           const float4* __restrict__ cell_q1, float eps2, float4* __restrict__ acc, int* __restrict__ ring_pool,
+           int ring_cap, unsigned* __restrict__ group_counter, unsigned long long* __restrict__ stats,
+           int* __restrict__ status) {
+  __shared__ float4 s_a0[kWalkWarps][64];
+  __shared__ float4 s_a1[kWalkWarps][64];
+  __shared__ float4 s_a2[kWalkWarps][64];
+  __shared__ float4 s_d[kWalkWarps][64];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int* ring = ring_pool + (size_t)(blockIdx.x * kWalkWarps + w) * (size_t)ring_cap;
+  const int rmask = ring_cap - 1;
+  const int ngroups = info->ngroups;
+  const int l1b = info->level_beg[1], l1e = info->level_end[1];
+  const unsigned lt = lanemask_lt();
+  unsigned long long sum_app = 0, sum_dir = 0;
+  unsigned max_app = 0, max_dir = 0;
+
+  while (true) {
+    int g = 0;
+    if (lane == 0) g = (int)atomicAdd(group_counter, 1u);
+    g = __shfl_sync(kFull, g, 0);
+    if (g >= ngroups) break;
+    const int2 gd = groups[g];
+    const int pbeg = gd.x, np = gd.y;
+    IPart pi[NI];
+    float4 ai[NI];
+    float mnx = 3.0e38f, mny = 3.0e38f, mnz = 3.0e38f, mxx = -3.0e38f, mxy = -3.0e38f, mxz = -3.0e38f;
+#pragma unroll
+    for (int k = 0; k < NI; k++) {
+      const float4 p = ipos[pbeg + min(k * 32 + lane, np - 1)];
+      pi[k].x = p.x; pi[k].y = p.y; pi[k].z = p.z;
+      ai[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+      mnx = fminf(mnx, p.x); mny = fminf(mny, p.y); mnz = fminf(mnz, p.z);
+      mxx = fmaxf(mxx, p.x); mxy = fmaxf(mxy, p.y); mxz = fmaxf(mxz, p.z);
+    }
+    mnx = warp_min_f32(mnx); mny = warp_min_f32(mny); mnz = warp_min_f32(mnz);
+    mxx = warp_max_f32(mxx); mxy = warp_max_f32(mxy); mxz = warp_max_f32(mxz);
+    const float3 gc = make_float3(__fmul_rn(0.5f, __fadd_rn(mxx, mnx)), __fmul_rn(0.5f, __fadd_rn(mxy, mny)),
+                                  __fmul_rn(0.5f, __fadd_rn(mxz, mnz)));
+    const float3 gs = make_float3(__fmul_rn(0.5f, __fsub_rn(mxx, mnx)), __fmul_rn(0.5f, __fsub_rn(mxy, mny)),
+                                  __fmul_rn(0.5f, __fsub_rn(mxz, mnz)));
+
+    int cur_off = 0, ncur = l1e - l1b, nnext = 0;
+    for (int j = lane; j < ncur; j += 32) ring[j & rmask] = l1b + j;
+    int a_head = 0, a_cnt = 0, d_head = 0, d_cnt = 0;
+    unsigned n_app = 0, n_dir = 0;
+    bool overflow = ncur > ring_cap;
+    __syncwarp();
+
+    while (ncur > 0 && !overflow) {
+      for (int blk = 0; blk < ncur; blk += 32) {
+        const int li = blk + lane;
+        const bool valid = li < ncur;
+        const int cell = valid ? ring[(cur_off + li) & rmask] : 0;
+        uint4 cd = make_uint4(0u, 0xFFFFFFFFu, 0u, 0u);
+        float4 co = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (valid) {
+          cd = __ldg(cell_data + cell);
+          co = __ldg(cell_open + cell);
+        }
+        const bool leaf = cd.y == 0xFFFFFFFFu;
+        const bool split = valid && (open_cell(co, gc, gs) || ((int)(cd.w - cd.z) < 3));
+
+        // (1) children of opened nodes -> next level
+        const int nch = (split && !leaf) ? (int)(cd.y >> 29) + 1 : 0;
+        const int incl = warp_incl_scan(nch);
+        const int tot = __shfl_sync(kFull, incl, 31);
+        if (ncur - blk + nnext + tot > ring_cap) { overflow = true; break; }
+        const int wbase = cur_off + ncur + nnext;
+        const int first = (int)(cd.y & 0x1FFFFFFFu);
+        for (int base = 0; base < tot; base += 32) {
+          const int s = base + lane;
+          const int src = find_src(incl, s);
+          const int f = __shfl_sync(kFull, first, src);
+          const int e = __shfl_sync(kFull, incl - nch, src);
+          if (s < tot) ring[(wbase + s) & rmask] = f + (s - e);
+        }
+        nnext += tot;
+
+        // (2) accepted cells -> approximate list (staged by value)
+        const bool app = valid && !split;
+        const unsigned bal = __ballot_sync(kFull, app);
+        if (app) {
+          const int slot = (a_head + a_cnt + __popc(bal & lt)) & 63;
+          const float4 q1 = __ldg(cell_q1 + cell);
+          s_a0[w][slot] = make_float4(co.x, co.y, co.z, q1.w * (-1.0f / 3.0f));
+          s_a1[w][slot] = __ldg(cell_q0 + cell);
+          s_a2[w][slot] = q1;
+        }
+        a_cnt += __popc(bal);
+        if (a_cnt >= 32) {
+          __syncwarp();
+#pragma unroll 4
+          for (int j = 0; j < 32; j++) {
+            const int sl = (a_head + j) & 63;
+            const float4 a0 = s_a0[w][sl], a1 = s_a1[w][sl], a2 = s_a2[w][sl];
+#pragma unroll
+            for (int k = 0; k < NI; k++) quad_acc(ai[k], pi[k], a0, a1, a2, eps2);
+          }
+          __syncwarp();
+          a_head = (a_head + 32) & 63;
+          a_cnt -= 32;
+          n_app += 32;
+        }
+
+        // (3) particles of opened leaves -> direct list
+        const int nb = (split && leaf) ? (int)(cd.w - cd.z) : 0;
+        const int incl2 = warp_incl_scan(nb);
+        const int tot2 = __shfl_sync(kFull, incl2, 31);
+        const int pb = (int)cd.z;
+        for (int base = 0; base < tot2; base += 32) {
+          const int s = base + lane;
+          const int src = find_src(incl2, s);
+          const int f = __shfl_sync(kFull, pb, src);
+          const int e = __shfl_sync(kFull, incl2 - nb, src);
+          const int cnt = min(32, tot2 - base);
+          if (lane < cnt) s_d[w][(d_head + d_cnt + lane) & 63] = __ldg(jpos + f + (s - e));
+          d_cnt += cnt;
+          if (d_cnt >= 32) {
+            __syncwarp();
+#pragma unroll 4
+            for (int j = 0; j < 32; j++) {
+              const float4 pj = s_d[w][(d_head + j) & 63];
+#pragma unroll
+              for (int k = 0; k < NI; k++) mono_acc(ai[k], pi[k], pj, eps2);
+            }
+            __syncwarp();
+            d_head = (d_head + 32) & 63;
+            d_cnt -= 32;
+            n_dir += 32;
+          }
+        }
+      }
+      cur_off += ncur;
+      ncur = nnext;
+      nnext = 0;
+      __syncwarp();
+    }
+
+    // flush the partial batches
+    __syncwarp();
+    for (int j = 0; j < a_cnt; j++) {
+      const int sl = (a_head + j) & 63;
+      const float4 a0 = s_a0[w][sl], a1 = s_a1[w][sl], a2 = s_a2[w][sl];
+#pragma unroll
+      for (int k = 0; k < NI; k++) quad_acc(ai[k], pi[k], a0, a1, a2, eps2);
+    }
+    n_app += a_cnt;
+    for (int j = 0; j < d_cnt; j++) {
+      const float4 pj = s_d[w][(d_head + j) & 63];
+#pragma unroll
+      for (int k = 0; k < NI; k++) mono_acc(ai[k], pi[k], pj, eps2);
+    }
+    n_dir += d_cnt;
+    __syncwarp();
+
+    if (overflow) {
+      if (lane == 0) set_status(status, kStatusWalkStack);
+#pragma unroll
+      for (int k = 0; k < NI; k++) ai[k] = make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, 0.f);
+    }
+#pragma unroll
+    for (int k = 0; k < NI; k++) {
+      const int idx = k * 32 + lane;
+      if (idx < np) acc[pbeg + idx] = ai[k];
+    }
+    sum_app += (unsigned long long)n_app * (unsigned long long)np;
+    sum_dir += (unsigned long long)n_dir * (unsigned long long)np;
+    max_app = max(max_app, n_app);
+    max_dir = max(max_dir, n_dir);
+  }
+  if (lane == 0) {
+    atomicAdd(stats + 0, sum_app);
+    atomicAdd(stats + 1, sum_dir);
+    atomicMax(stats + 2, (unsigned long long)max_app);
+    atomicMax(stats + 3, (unsigned long long)max_dir);
+  }
+}
+
+int walk_ni(int ncrit) { return ncrit <= 32 ? 1 : (ncrit <= 64 ? 2 : 4); }
+
+int walk_blocks_per_sm(int ni) {
+  int nb = 0;
+  cudaError_t e;
+  if (ni == 1) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_walk<1>, kWalkThreads, 0);
+  else if (ni == 2) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_walk<2>, kWalkThreads, 0);
+  else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_walk<4>, kWalkThreads, 0);
+  if (e != cudaSuccess || nb < 1) nb = 1;
+  return nb;
+}
+
+void launch_walk(int ni, int nblocks, const int2* groups, const TreeInfo* info, const float4* ipos,
+                 const float4* jpos, const uint4* cell_data, const float4* cell_open, const float4* cell_q0,
+                 const float4* cell_q1, float eps2, float4* acc, int* ring_pool, int ring_cap,
+                 unsigned* group_counter, unsigned long long* stats, int* status, cudaStream_t s) {
+  if (ni == 1)
+    k_walk<1><<<nblocks, kWalkThreads, 0, s>>>(groups, info, ipos, jpos, cell_data, cell_open, cell_q0, cell_q1, eps2,
+                                               acc, ring_pool, ring_cap, group_counter, stats, status);
+  else if (ni == 2)
+    k_walk<2><<<nblocks, kWalkThreads, 0, s>>>(groups, info, ipos, jpos, cell_data, cell_open, cell_q0, cell_q1, eps2,
+                                               acc, ring_pool, ring_cap, group_counter, stats, status);
+  else
+    k_walk<4><<<nblocks, kWalkThreads, 0, s>>>(groups, info, ipos, jpos, cell_data, cell_open, cell_q0, cell_q1, eps2,
+                                               acc, ring_pool, ring_cap, group_counter, stats, status);
+}
+
+}  // namespace bonsai

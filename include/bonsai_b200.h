@@ -1,0 +1,171 @@
+/*
+ * bonsai_b200.h -- C ABI of the B200 tree code (libbonsai_b200.so).
+ *
+ * Drop-in for the per-step path of Bonsai2's Treecode<float>
+ * (code/Treecode.h:123-223, instantiated for float only in
+ * code/TreecodeInstances.h:3).  Every entry point names the reference member
+ * it replaces.  Plain pointers and sizes only; all state lives in an opaque
+ * handle (one CUDA stream per handle, no globals), so handles are
+ * independent and a process may hold several.
+ *
+ * Return codes: 0 = OK; > 0 = bit set of device-detected data conditions
+ * (BONSAI_STATUS_*), reported after the stage that raised them; < 0 = API
+ * misuse (BONSAI_ERR_*) or a CUDA error (-1000 - cudaError_t).  Nothing
+ * aborts, asserts or traps (the reference aborts through CUDA_SAFE_CALL and
+ * device assert, Treecode.h:18-27, computeForces.cu:565).
+ *
+ * Particle order: positions/velocities are passed in and returned in the
+ * caller's order (index i of the arrays given to bonsai_set_particles).
+ * Internally particles are kept in Peano-Hilbert order and reordered every
+ * step; bonsai_get_particles scatters them back.
+ */
+#ifndef BONSAI_B200_H
+#define BONSAI_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* device status bits (returned as positive codes) */
+#define BONSAI_STATUS_CELL_CAPACITY 1  /* tree has more cells than allocated (retry with bonsai_alloc) */
+#define BONSAI_STATUS_DEPTH 2          /* a level-21 cell holds more than nLeaf: kept as one leaf */
+#define BONSAI_STATUS_WALK_STACK 4     /* a walk level list outgrew its ring: forces of that group are NaN */
+#define BONSAI_STATUS_NONFINITE 8      /* NaN/Inf coordinate in the input */
+#define BONSAI_STATUS_GROUP_CAPACITY 16
+#define BONSAI_STATUS_BAD_PARAM 32
+
+/* API errors */
+#define BONSAI_ERR_HANDLE (-1)
+#define BONSAI_ERR_NOT_ALLOCATED (-2)
+#define BONSAI_ERR_ORDER (-3)     /* a stage was called before the stage it needs */
+#define BONSAI_ERR_ARG (-4)
+#define BONSAI_ERR_NO_DEVICE (-5)
+
+typedef struct bonsai_handle_s *bonsai_handle;
+
+typedef struct bonsai_params {
+  float theta;      /* opening angle: Treecode::theta (Treecode.h:133,167) */
+  float eps;        /* softening: Treecode::eps2 = eps*eps (Treecode.h:133,166) */
+  int nleaf;        /* max particles per leaf, 1..64: buildTree(nLeaf) (Treecode.h:216) */
+  int ncrit;        /* max particles per group, 1..128: makeGroups(levelSplit, nCrit) (Treecode.h:218) */
+  int level_split;  /* PH octal digits per group segment, 1..7 (Treecode.h:218; treecode.cu:142 passes 5) */
+  float dt;         /* leapfrog step; the reference's moveParticles is a stub (moveParticles.cu:3-7) */
+  int device;       /* CUDA device ordinal */
+} bonsai_params;
+
+typedef struct bonsai_tree_info {
+  int ncells, nleaves, nnodes, nlevels, ngroups, status;
+  int level_beg[32]; /* cells of level L are [level_beg[L], level_end[L]);   */
+  int level_end[32]; /* the reference stores inclusive int2 ranges (buildTree.cu:748-780) */
+} bonsai_tree_info;
+
+/* Defaults of the Treecode constructor (Treecode.h:164: eps 0.01, theta 0.75,
+ * nCrit 64), buildTree's nLeaf 16 (Treecode.h:216), the driver's
+ * levelSplit 5 (treecode.cu:142), dt 1/64, device 0. */
+void bonsai_default_params(bonsai_params *p);
+
+/* Treecode(eps, theta, ncrit) -- Treecode.h:164-173 */
+int bonsai_create(const bonsai_params *p, bonsai_handle *out);
+/* ~Treecode (cuda_mem destructors, cudamem.h:13) */
+int bonsai_destroy(bonsai_handle h);
+/* Treecode::alloc(nPtcl) -- Treecode.h:175-198 */
+int bonsai_alloc(bonsai_handle h, int n);
+/* update theta / eps / dt between steps (the reference's public theta, eps2 fields, Treecode.h:133) */
+int bonsai_set_params(bonsai_handle h, const bonsai_params *p);
+
+/* Treecode::ptcl_h2d -- Treecode.h:207-214.  pos4 = (x,y,z,m), vel4 = (vx,vy,vz,*),
+ * n floats4 each, host memory (pinned memory from bonsai_host_alloc is fastest).
+ * Velocities are taken as synchronised with positions (first step: no closing kick). */
+int bonsai_set_particles(bonsai_handle h, const float *pos4, const float *vel4, int n);
+/* same, from device memory */
+int bonsai_set_particles_device(bonsai_handle h, const float *d_pos4, const float *d_vel4, int n);
+/* Treecode::ptcl_d2h -- Treecode.h:200-204, plus the accelerations (d_ptclAcc,
+ * computeForces.cu:611-617); caller order; any pointer may be NULL. */
+int bonsai_get_particles(bonsai_handle h, float *pos4, float *vel4, float *acc4);
+int bonsai_get_particles_device(bonsai_handle h, float *d_pos4, float *d_vel4, float *d_acc4);
+
+/* Treecode::buildTree(nLeaf) -- Treecode.h:216, buildTree.cu:845-1108 (box, tree, level order, leaves) */
+int bonsai_build_tree(bonsai_handle h, int nleaf);
+/* Treecode::computeMultipoles() -- Treecode.h:217, computeMultipoles.cu:194-234 */
+int bonsai_compute_multipoles(bonsai_handle h);
+/* Treecode::makeGroups(levelSplit, nCrit) -- Treecode.h:218, makeGroups.cu:236-341 */
+int bonsai_make_groups(bonsai_handle h, int level_split, int ncrit);
+/* Treecode::computeForces(INTCOUNT) -- Treecode.h:219, computeForces.cu:622-727.
+ * If intcount and stats != NULL: stats = {<direct>, max direct, <approx>, max approx}
+ * per particle (the reference's double4), and the call waits for the walk. */
+int bonsai_compute_forces(bonsai_handle h, int intcount, double *stats);
+/* Treecode::moveParticles() -- Treecode.h:220 (reference stub, moveParticles.cu:3-7):
+ * kick-drift-kick leapfrog with merged kicks; energies of the synchronised
+ * point are summed in the same pass. */
+int bonsai_move_particles(bonsai_handle h);
+/* Treecode::computeEnergies() -- Treecode.h:221 (reference stub, computeEnergies.cu:3-7;
+ * potential sum of computeForces.cu:576-607).  out (may be NULL) =
+ * {T, W, W without the i==j self term, T + W_noself, Px, Py, Pz, M}, FP64,
+ * at the time of the last force evaluation.  Waits for the device. */
+int bonsai_compute_energies(bonsai_handle h, double *out);
+
+/* The whole step of treecode.cu:137-168 (build, multipoles, groups, forces,
+ * move) nsteps times; use_graph != 0 replays it as a captured CUDA graph.
+ * Asynchronous: call bonsai_synchronize for the status. */
+int bonsai_step(bonsai_handle h, int nsteps, int use_graph);
+/* bonsai_step with use_graph = 1 and CUDA events recorded on the handle's
+ * stream between the phases of every step; waits, then writes
+ * phase_ms[4*s + k] = {build+multipoles+groups, walk, move, whole step} (ms),
+ * and phase_ms[4*nsteps] = device time from the first step's start to the
+ * last step's end (phase_ms holds 4*nsteps+1 floats). */
+int bonsai_step_timed(bonsai_handle h, int nsteps, float *phase_ms);
+/* number of kernel nodes in the captured graphs of one step */
+int bonsai_graph_kernel_count(bonsai_handle h);
+/* interaction statistics of the last walk (computeForces.cu:568-609):
+ * {sum over particles of n_approx, of n_direct, max n_approx, max n_direct} */
+int bonsai_get_stats(bonsai_handle h, unsigned long long *out4);
+/* measured FP32 FMA throughput of the device (TFLOP/s): the walk's roofline */
+int bonsai_fp32_peak(int device, double *tflops);
+/* Wait for the handle's stream; returns the sticky device status (and clears it). */
+int bonsai_synchronize(bonsai_handle h);
+/* the handle's CUDA stream (cudaStream_t) */
+void *bonsai_stream(bonsai_handle h);
+const char *bonsai_error_string(int code);
+
+/* ---- inspection (parity tests; the reference keeps these in device globals
+ * and cuda_mem members: d_domain, d_cellDataList, d_level_begIdx, d_leafList,
+ * d_key/d_value, d_groupList, d_cellSize, d_cellMonopole, d_cellQuad0/1) ---- */
+int bonsai_get_tree_info(bonsai_handle h, bonsai_tree_info *out);
+/* domain box {cx, cy, cz, hsize} (d_domain, buildTree.cu:161) */
+int bonsai_get_box(bonsai_handle h, float *box4);
+/* keys of the last build, sorted, and the sort permutations (indices into the
+ * particle order the build saw); ids_at_build maps that order to caller order.
+ * Any pointer may be NULL.  n entries each. */
+int bonsai_get_keys(bonsai_handle h, uint64_t *tree_keys, int *tree_perm, uint64_t *ph_keys, int *ph_perm,
+                    int *ids_at_build);
+/* cells in the reference layout: cell_data uint32[4C] (CellData packing,
+ * Treecode.h:45-89), size4/mono4/quad0 float[4C], quad1 float[2C],
+ * leaf_list int[nleaves], parent int[C] (-1 for level 1).  Any may be NULL. */
+int bonsai_get_cells(bonsai_handle h, uint32_t *cell_data, float *size4, float *mono4, float *quad0, float *quad1,
+                     int *leaf_list, int *parent);
+/* groups int[2G] = (pbeg, np) in PH order (GroupData, Treecode.h:29-43) */
+int bonsai_get_groups(bonsai_handle h, int *groups);
+/* walk inputs/outputs in internal order: ipos4 (PH/group order), jpos4 (tree
+ * order), acc4 (PH order), ids (caller index of each PH-order particle) */
+int bonsai_get_walk_arrays(bonsai_handle h, float *ipos4, float *jpos4, float *acc4, int *ids);
+
+/* FP64 direct summation for ns sample particles (caller indices) against all
+ * particles -- the force checker.  out double[4*ns] = (ax, ay, az, phi). */
+int bonsai_direct_fp64(bonsai_handle h, const int *sample, int ns, int include_self, double *out);
+
+/* Plummer sphere initial conditions on the host: the algorithm of
+ * code/plummer.h:9-138 (glibc rand(), same stream), converted to float4 like
+ * treecode.cu:65-87: pos4 = (x,y,z,m), vel4 = (vx,vy,vz,m).  n >= 1. */
+int bonsai_plummer(long n, unsigned int seed, float *pos4, float *vel4);
+
+/* pinned host memory (host_mem<T>, cudamem.h:64-96) */
+void *bonsai_host_alloc(size_t bytes);
+void bonsai_host_free(void *p);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BONSAI_B200_H */

@@ -1,0 +1,58 @@
+"""The C ABI library loads and exports every entry point that
+include/bonsai_b200.h declares; without a GPU, creating a handle fails with
+an error code (no CPU fallback).  No compute calls here."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    src = open(os.path.join(ROOT, "include", "bonsai_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(bonsai_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol(lib):
+    from bonsai2_b200 import _lib
+    names = declared_symbols()
+    assert len(names) >= 25
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(l.split()[-1] for l in out.splitlines() if l.strip())
+    missing = [s for s in names if s not in exported]
+    assert not missing, missing
+    for s in names:
+        assert hasattr(lib, s)
+    assert set(names) == set(_lib.SIGNATURES)
+
+
+def test_library_is_built_for_sm100a(lib):
+    from bonsai2_b200 import _lib
+    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", _lib.LIB_PATH],
+                         capture_output=True, text=True).stdout
+    assert "sm_100a" in out
+
+
+def test_create_without_gpu_fails_loudly(lib):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    import bonsai2_b200 as B
+    with pytest.raises(B.BonsaiError):
+        B.Treecode()
+
+
+def test_error_strings(lib):
+    for c in (0, -1, -2, -3, -4, -5, 1, 2, 4, 8, 16):
+        assert lib.bonsai_error_string(c)
+
+
+def test_default_params(lib):
+    import bonsai2_b200 as B
+    p = B.default_params()
+    assert abs(p.theta - 0.75) < 1e-7 and abs(p.eps - 0.01) < 1e-7   # Treecode.h:164
+    assert p.nleaf == 16 and p.ncrit == 64 and p.level_split == 5

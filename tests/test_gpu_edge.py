@@ -1,0 +1,170 @@
+"""GPU edge cases and size-independent properties at the full size.
+
+Edge cases the reference's own debug checks cover (every particle in one leaf,
+sum of group sizes = N, permutation consistency, PSHFL_SANITY_CHECK) and those
+it cannot handle (N=1, coincident particles deeper than 21 levels, NaN input:
+the reference traps or loops there; here they return a status code)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def full_tree(oracle, pos, vel, nleaf, ncrit, ls=5, theta=0.4, eps=0.01):
+    import bonsai2_b200 as B
+    t = B.Treecode(eps=eps, theta=theta, ncrit=ncrit, nleaf=nleaf, level_split=ls)
+    t.alloc(pos.shape[0])
+    t.h_ptclPos[:] = pos
+    t.h_ptclVel[:] = vel
+    t.ptcl_h2d()
+    t.buildTree(nleaf)
+    t.computeMultipoles()
+    t.makeGroups(ls, ncrit)
+    stats = t.computeForces(True)
+    return t, stats
+
+
+def check_against_oracle(oracle, t, pos, nleaf, ncrit, ls):
+    box, _ = oracle.bbox(pos)
+    assert np.array_equal(t.box(), box)
+    T = oracle.OracleTree(pos, box, nleaf)
+    c = t.cells(multipoles=False)
+    assert c["info"]["ncells"] == T.ncells
+    assert np.array_equal(c["cell_data"], T.cell_data())
+    k = t.keys()
+    leaf = T.nchild == 0
+    for ci in np.nonzero(leaf)[0]:
+        b, e = T.pbeg[ci], T.pend[ci]
+        assert np.array_equal(np.sort(k["tree_perm"][b:e]), np.sort(T.perm[b:e]))
+    pk = oracle.ph_keys(pos, box)
+    pp = oracle.argsort_u64(pk)
+    assert np.array_equal(k["ph_perm"], pp)
+    gb, gn = oracle.make_groups(pk[pp], ls, ncrit)
+    g = t.groups()
+    assert np.array_equal(g[:, 0], gb) and np.array_equal(g[:, 1], gn)
+    return T
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 16, 17, 100, 4097])
+def test_small_n(oracle, lib, n):
+    p, v = oracle.plummer_float4(max(n, 64), 5)
+    p, v = np.ascontiguousarray(p[:n]), np.ascontiguousarray(v[:n])
+    t, stats = full_tree(oracle, p, v, 16, 64)
+    check_against_oracle(oracle, t, p, 16, 64, 5)
+    acc = t.get_acc().astype(np.float64)
+    d = oracle.direct_fp64(p, np.arange(n), 0.01, include_self=True)
+    err = np.linalg.norm(acc[:, :3] - d[:, :3], axis=1) / np.maximum(np.linalg.norm(d[:, :3], axis=1), 1e-30)
+    if n > 1:
+        assert np.median(err) < 1e-3
+    else:
+        assert np.all(acc[:, :3] == 0) and abs(acc[0, 3] + p[0, 3] / 0.01) < 1e-6 * abs(acc[0, 3])
+    assert t.synchronize() == 0
+
+
+@pytest.mark.parametrize("nleaf,ncrit", [(16, 32), (24, 64), (32, 64), (48, 128), (64, 64), (1, 16), (8, 100)])
+def test_leaf_and_group_sizes(oracle, lib, nleaf, ncrit):
+    p, v = oracle.plummer_float4(30000, 11)
+    t, stats = full_tree(oracle, p, v, nleaf, ncrit)
+    check_against_oracle(oracle, t, p, nleaf, ncrit, 5)
+    acc = t.get_acc().astype(np.float64)
+    samp = np.arange(0, 30000, 97)
+    d = oracle.direct_fp64(p, samp, 0.01)
+    err = np.linalg.norm(acc[samp, :3] - d[:, :3], axis=1) / np.linalg.norm(d[:, :3], axis=1)
+    assert np.median(err) < 1e-3
+
+
+@pytest.mark.parametrize("ls", [1, 3, 7])
+def test_level_split(oracle, lib, ls):
+    p, v = oracle.plummer_float4(20000, 3)
+    t, _ = full_tree(oracle, p, v, 16, 64, ls=ls)
+    check_against_oracle(oracle, t, p, 16, 64, ls)
+
+
+def test_coincident_particles_depth_status(oracle, lib):
+    # 40 particles at one point force the partition below level 21: the
+    # reference recurses without bound; here a fat leaf is kept and flagged
+    p, v = oracle.plummer_float4(5000, 2)
+    p[100:140, :3] = p[7, :3]
+    with pytest.warns(UserWarning):
+        t, _ = full_tree(oracle, p, v, 16, 64)
+    T = check_against_oracle(oracle, t, p, 16, 64, 5)
+    assert T.overflow
+    assert t.tree_info()["status"] & 2
+    acc = t.get_acc()
+    assert np.all(np.isfinite(acc))
+
+
+def test_nonfinite_input_reports_status(oracle, lib):
+    import bonsai2_b200 as B
+    p, v = oracle.plummer_float4(4096, 2)
+    p[10, 0] = np.nan
+    t = B.Treecode(eps=0.01, theta=0.4)
+    t.alloc(p.shape[0])
+    t.h_ptclPos[:] = p
+    t.h_ptclVel[:] = v
+    t.ptcl_h2d()
+    with pytest.raises(B.BonsaiError) as ei:
+        t.buildTree(16)
+        t.synchronize()
+    assert ei.value.code & 8
+
+
+def test_stage_order_errors(oracle, lib):
+    import bonsai2_b200 as B
+    p, v = oracle.plummer_float4(1000, 2)
+    t = B.Treecode()
+    t.alloc(1000)
+    t.h_ptclPos[:] = p
+    t.h_ptclVel[:] = v
+    t.ptcl_h2d()
+    with pytest.raises(B.BonsaiError):
+        t.computeMultipoles()
+    with pytest.raises(B.BonsaiError):
+        t.computeForces()
+    with pytest.raises(B.BonsaiError):
+        t.moveParticles()
+
+
+def test_energy_drift_short_run(oracle, lib):
+    import bonsai2_b200 as B
+    p, v = oracle.plummer_float4(65536)
+    t = B.Treecode(eps=0.01, theta=0.4, dt=1.0 / 128)
+    t.alloc(p.shape[0])
+    t.h_ptclPos[:] = p
+    t.h_ptclVel[:] = v
+    t.ptcl_h2d()
+    E = []
+    for s in range(8):
+        t.step(1, graph=True)
+        E.append(t.computeEnergies()[3])
+    assert t.synchronize() == 0
+    E = np.array(E)
+    assert abs(E[-1] - E[0]) / abs(E[0]) < 1e-4
+    assert abs(t.computeEnergies()[7] - 1.0) < 1e-6
+
+
+def test_full_size_properties(lib):
+    # BASELINE's large configuration: N = 2^24 Plummer, theta 0.4, eps 0.005
+    import bonsai2_b200 as B
+    n = 1 << 24
+    pos, vel = B.plummer(n, 19810614)
+    t, stats = full_tree(None, pos, vel, 16, 64, eps=0.005)
+    assert t.synchronize() == 0
+    k = t.keys()
+    assert np.all(k["tree_keys"][1:] >= k["tree_keys"][:-1])
+    assert np.all(k["ph_keys"][1:] >= k["ph_keys"][:-1])
+    assert np.array_equal(np.sort(k["tree_perm"]), np.arange(n))
+    assert np.array_equal(np.sort(k["ph_perm"]), np.arange(n))
+    c = t.cells(multipoles=False)
+    cd = c["cell_data"]
+    leaf = cd[:, 1] == 0xFFFFFFFF
+    assert (cd[leaf, 3].astype(np.int64) - cd[leaf, 2]).sum() == n
+    assert np.all(cd[leaf, 3] - cd[leaf, 2] <= 16)
+    g = t.groups()
+    assert g[:, 1].sum() == n and np.all(g[:, 1] <= 64)
+    acc = t.get_acc().astype(np.float64)
+    rng = np.random.default_rng(11)
+    samp = rng.choice(n, 256, replace=False)
+    d = t.direct_fp64(samp, include_self=True)
+    err = np.linalg.norm(acc[samp, :3] - d[:, :3], axis=1) / np.linalg.norm(d[:, :3], axis=1)
+    assert np.median(err) < 1e-3
