@@ -307,7 +307,7 @@ def run_ours(a):
     # ---- e2e through the C ABI with host buffers ----
     stream = torch.cuda.ExternalStream(L.bonsai_stream(t.handle))
     e2e_ms = []
-    for s in range(a.e2e_steps + 1):
+    for s in range(a.e2e_steps + 1 if a.e2e_steps > 0 else 0):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         d.barrier()
@@ -321,7 +321,7 @@ def run_ours(a):
             raise B.BonsaiError(rc, "e2e step")
         if s > 0:
             e2e_ms.append(e0.elapsed_time(e1))
-    e2e = d.max(statistics.mean(e2e_ms))
+    e2e = d.max(statistics.mean(e2e_ms)) if e2e_ms else float("nan")
     e2e_value = n * d.world / (e2e * 1e-3) / 1e6
 
     cpu = None

@@ -9,7 +9,8 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libbonsai_b200.so")
+# BONSAI_B200_LIB selects an alternative build of the same library (tuning builds)
+LIB_PATH = os.environ.get("BONSAI_B200_LIB") or os.path.join(HERE, "libbonsai_b200.so")
 
 
 class bonsai_params(ctypes.Structure):

@@ -21,6 +21,8 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INCLUDE, "--expt-relaxed-constexpr"]
+# extra -D tuning flags (e.g. BONSAI_WALK_SPLIT=0) for alternative builds
+EXTRA = os.environ.get("BONSAI_NVCC_DEFINES", "").split()
 PER_FILE = {"walk.cu": ["-ftz=true"]}
 SOURCES = ["keys.cu", "sort.cu", "tree.cu", "multipoles.cu", "groups.cu", "walk.cu", "move.cu", "treecode.cu"]
 HOST_SOURCES = ["plummer.cpp"]
@@ -43,7 +45,7 @@ def _compile(src: str, verbose: bool) -> str:
     if src.endswith(".cpp"):
         cmd = ["g++", "-O3", "-fPIC", "-std=c++17", "-c", path, "-o", out]
     else:
-        cmd = [NVCC] + ARCH + COMMON + PER_FILE.get(src, []) + (["-Xptxas", "-v"] if verbose else []) + ["-c", path, "-o", out]
+        cmd = [NVCC] + ARCH + COMMON + EXTRA + PER_FILE.get(src, []) + (["-Xptxas", "-v"] if verbose else []) + ["-c", path, "-o", out]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("compile failed: %s\n%s\n%s" % (" ".join(cmd), r.stdout, r.stderr))
@@ -52,19 +54,29 @@ def _compile(src: str, verbose: bool) -> str:
     return out
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and up_to_date():
+def build(force: bool = False, verbose: bool = False, out: str = None, objdir: str = None) -> str:
+    global OBJ
+    lib = out or LIB
+    if not force and out is None and up_to_date():
         return LIB
+    if objdir:
+        OBJ = objdir
     os.makedirs(OBJ, exist_ok=True)
     with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose), SOURCES + HOST_SOURCES))
-    tmp = LIB + ".tmp%d" % os.getpid()
+    tmp = lib + ".tmp%d" % os.getpid()
     cmd = [NVCC] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart"]
     subprocess.check_call(cmd)
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, lib)
+    return lib
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose="-v" in sys.argv)
-    print(LIB)
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("-v", action="store_true")
+    ap.add_argument("--out", default=None, help="write the library here instead of the in-tree path")
+    ap.add_argument("--objdir", default=None)
+    a = ap.parse_args()
+    print(build(force=a.force, verbose=a.v, out=a.out, objdir=a.objdir))

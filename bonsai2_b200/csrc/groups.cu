@@ -40,18 +40,30 @@ __global__ void k_group_sizes(const unsigned* __restrict__ count, int nbins, int
     ng[b] = (count[b] + (unsigned)ncrit - 1u) / (unsigned)ncrit;
 }
 
-__global__ void k_group_write(const unsigned* __restrict__ count, const unsigned* __restrict__ seg_start,
-                              const unsigned* __restrict__ goff, int nbins, int ncrit, int2* __restrict__ groups,
-                              int group_cap, TreeInfo* __restrict__ info) {
-  if (info->ngroups > group_cap) {
+// one thread per group: the group's bin is found by binary search over the
+// exclusive scan of group counts (bins near a dense core hold 10^5 groups, so
+// a thread per bin would serialise them)
+__global__ void __launch_bounds__(256) k_group_write(const unsigned* __restrict__ count,
+                                                     const unsigned* __restrict__ seg_start,
+                                                     const unsigned* __restrict__ goff, int nbins, int ncrit,
+                                                     int2* __restrict__ groups, int group_cap,
+                                                     TreeInfo* __restrict__ info) {
+  const int ng = info->ngroups;
+  if (ng > group_cap) {
     if (blockIdx.x == 0 && threadIdx.x == 0) set_status(&info->status, kStatusGroupCapacity);
     return;
   }
-  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nbins; b += gridDim.x * blockDim.x) {
-    const int c = (int)count[b];
-    if (c == 0) continue;
-    const int s = (int)seg_start[b], g0 = (int)goff[b];
-    for (int k = 0, off = 0; off < c; k++, off += ncrit) groups[g0 + k] = make_int2(s + off, min(ncrit, c - off));
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
+    int lo = 0, hi = nbins;  // last bin with goff <= g
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if ((int)__ldg(goff + mid) <= g) lo = mid; else hi = mid;
+    }
+    // the last bin with goff <= g is never empty (an empty bin shares its
+    // offset with the next bin)
+    const int k = g - (int)goff[lo];
+    const int off = k * ncrit;
+    groups[g] = make_int2((int)seg_start[lo] + off, min(ncrit, (int)count[lo] - off));
   }
 }
 
@@ -66,7 +78,7 @@ void make_groups(const unsigned long long* sorted_ph, int n, int level_split, in
   exclusive_scan(count, seg_start, nbins, bsum, nullptr, s);
   k_group_sizes<<<(nbins + 255) / 256, 256, 0, s>>>(count, nbins, ncrit, ng);
   exclusive_scan(ng, ng, nbins, bsum, (unsigned*)&info->ngroups, s);
-  k_group_write<<<(nbins + 255) / 256, 256, 0, s>>>(count, seg_start, ng, nbins, ncrit, groups, group_cap, info);
+  k_group_write<<<1184, 256, 0, s>>>(count, seg_start, ng, nbins, ncrit, groups, group_cap, info);
 }
 
 // state gather: out[k] = in[perm[k]] for positions, velocities and ids

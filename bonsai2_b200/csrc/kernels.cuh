@@ -6,7 +6,10 @@
 namespace bonsai {
 
 constexpr int kWalkThreads = 256;
-constexpr int kWalkMinBlocks = 3;
+#ifndef BONSAI_WALK_MINB
+#define BONSAI_WALK_MINB 3
+#endif
+constexpr int kWalkMinBlocks = BONSAI_WALK_MINB;
 
 // keys.cu
 void build_ph_table(uint16_t* tab);
@@ -51,9 +54,9 @@ __global__ void k_gather_pos(const int* __restrict__ perm, int n, const float4* 
                              float4* __restrict__ out);
 
 // walk.cu
-int walk_ni(int ncrit);
-int walk_blocks_per_sm(int ni);
-void launch_walk(int ni, int nblocks, const int2* groups, const TreeInfo* info, const float4* ipos, const float4* jpos,
+int walk_variant(int ncrit);
+int walk_blocks_per_sm(int variant);
+void launch_walk(int variant, int nblocks, const int2* groups, const TreeInfo* info, const float4* ipos, const float4* jpos,
                  const uint4* cell_data, const float4* cell_open, const float4* cell_q0, const float4* cell_q1,
                  float eps2, float4* acc, int* ring_pool, int ring_cap, unsigned* group_counter,
                  unsigned long long* stats, int* status, cudaStream_t s);

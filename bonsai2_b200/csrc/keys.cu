@@ -111,8 +111,14 @@ __global__ void __launch_bounds__(256) k_box(const float4* __restrict__ pos, int
       float c[3], h[3];
       for (int k = 0; k < 3; k++) { c[k] = (b[k] + a[k]) * 0.5f; h[k] = (b[k] - a[k]) * 0.5f; }
       const float hm = fmaxf(h[2], fmaxf(h[1], h[0]));
+      // floor max(2^-100, 2^-40 * pow2 >= max|c|): a zero-extent input still
+      // gives a finite box whose centre quantisation fits 64 bits
+      const float cm = fmaxf(fabsf(c[0]), fmaxf(fabsf(c[1]), fabsf(c[2])));
+      float pw = 1.0f;
+      while (pw < cm) pw *= 2.0f;
+      while (pw * 0.5f >= cm && pw > 7.888609052210118e-31f) pw *= 0.5f;
+      const float floor_h = fmaxf(pw * 9.094947017729282e-13f, 7.888609052210118e-31f);
       float hs = 1.0f;
-      const float floor_h = 7.888609052210118e-31f;  // 2^-100: finite box for zero extent
       while (hs > hm && hs > floor_h) hs *= 0.5f;
       while (hs < hm) hs *= 2.0f;
       const float hq = __fdiv_rn(hs, (float)(1 << 20));

@@ -67,7 +67,7 @@ struct Handle {
   int2* groups = nullptr;
   unsigned *g_count = nullptr, *g_seg = nullptr, *g_ng = nullptr;
   int* ring = nullptr;
-  int walk_blocks[3] = {0, 0, 0};  // NI = 1, 2, 4
+  int walk_blocks[6] = {0, 0, 0, 0, 0, 0};  // per walk variant (walk_variant)
   int ring_warps = 0;
   unsigned* group_counter = nullptr;
   unsigned long long* stats = nullptr;
@@ -84,6 +84,7 @@ struct Handle {
   int cur_nleaf = 16, cur_ncrit = 64, cur_ls = 5;
   // stage bookkeeping for the eager API
   bool built = false, mp_done = false, grouped = false, forced = false, moved_after_forces = false;
+  bool ever_built = false, ever_mp = false;  // the cell arrays hold a tree / multipoles
   // graphs, one per state parity and phase (0: build+multipoles+groups, 1: walk, 2: move)
   cudaGraphExec_t gexec[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
   int graph_kernels = 0;
@@ -154,8 +155,8 @@ struct Handle {
     BONSAI_CUDA_TRY(dalloc(&g_count, (size_t)1 << (3 * kMaxLevelSplit)));
     BONSAI_CUDA_TRY(dalloc(&g_seg, (size_t)1 << (3 * kMaxLevelSplit)));
     BONSAI_CUDA_TRY(dalloc(&g_ng, (size_t)1 << (3 * kMaxLevelSplit)));
-    for (int k = 0; k < 3; k++) walk_blocks[k] = nsm * walk_blocks_per_sm(1 << k);
-    ring_warps = *std::max_element(walk_blocks, walk_blocks + 3) * (kWalkThreads / 32);
+    for (int k = 0; k < 6; k++) walk_blocks[k] = nsm * walk_blocks_per_sm(k);
+    ring_warps = *std::max_element(walk_blocks, walk_blocks + 6) * (kWalkThreads / 32);
     BONSAI_CUDA_TRY(dalloc(&ring, (size_t)ring_warps * kRingCap));
     BONSAI_CUDA_TRY(dalloc(&group_counter, 1));
     BONSAI_CUDA_TRY(dalloc(&stats, 4));
@@ -205,11 +206,29 @@ struct Handle {
     BONSAI_CUDA_TRY(dalloc(&chain, N));
     BONSAI_CUDA_TRY(dalloc(&hist, (size_t)2 * (kMaxLevel + 1) * tree_tiles(nn)));
     BONSAI_CUDA_TRY(dalloc(&groups, N));
-    int rc = alloc_cells(2 * nn + 4096);
+    // the reference reserves nPtcl cells (Treecode.h:192); a Plummer tree at
+    // nLeaf 16 uses ~0.23 N.  Grown on demand by the eager build.
+    int rc = alloc_cells(prm.nleaf >= 8 ? nn / 2 + 4096 : 2 * nn + 4096);
     if (rc) return rc;
     par = 0;
     built = mp_done = grouped = forced = moved_after_forces = false;
+    ever_built = ever_mp = false;
     return 0;
+  }
+
+  // eager build that grows the cell arrays until the tree fits
+  int build_checked(int nleaf) {
+    for (int attempt = 0; attempt < 4; attempt++) {
+      enq_build(nleaf);
+      int nc = 0;
+      BONSAI_CUDA_TRY(cudaMemcpyAsync(&nc, &info->ncells, sizeof(int), cudaMemcpyDeviceToHost, st));
+      BONSAI_CUDA_TRY(cudaStreamSynchronize(st));
+      if (nc <= cap_cells) return 0;
+      const int rc = alloc_cells(nc + nc / 4 + 4096);
+      if (rc) return rc;
+      BONSAI_CUDA_TRY(cudaMemsetAsync(&info->status, 0, sizeof(int), st));
+    }
+    return BONSAI_STATUS_CELL_CAPACITY;
   }
 
   // ---------------- stages (enqueue only) ----------------
@@ -234,11 +253,10 @@ struct Handle {
     par = q;
   }
   void enq_forces(int ncrit) {
-    const int ni = walk_ni(ncrit);
-    const int k = ni == 1 ? 0 : (ni == 2 ? 1 : 2);
+    const int k = walk_variant(ncrit);
     cudaMemsetAsync(group_counter, 0, sizeof(unsigned), st);
     cudaMemsetAsync(stats, 0, 4 * sizeof(unsigned long long), st);
-    launch_walk(ni, walk_blocks[k], groups, info, pos[par], jpos, cell_data, cell_open, cell_q0, cell_q1,
+    launch_walk(k, walk_blocks[k], groups, info, pos[par], jpos, cell_data, cell_open, cell_q0, cell_q1,
                 prm.eps * prm.eps, acc, ring, kRingCap, group_counter, stats, &info->status, st);
   }
   void enq_move(bool write) {
@@ -459,18 +477,11 @@ int bonsai_build_tree(bonsai_handle hh, int nleaf) {
   if (nleaf < 1 || nleaf > 64) return BONSAI_ERR_ARG;
   BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
   h->cur_nleaf = nleaf;
-  for (int attempt = 0; attempt < 4; attempt++) {
-    h->enq_build(nleaf);
-    int nc = 0;
-    BONSAI_CUDA_TRY(cudaMemcpyAsync(&nc, &h->info->ncells, sizeof(int), cudaMemcpyDeviceToHost, h->st));
-    BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
-    if (nc <= h->cap_cells) break;
-    // grow the cell arrays and rebuild (the capacity bit is cleared)
-    const int rc = h->alloc_cells(nc + nc / 4 + 4096);
+  {
+    const int rc = h->build_checked(nleaf);
     if (rc) return rc;
-    BONSAI_CUDA_TRY(cudaMemsetAsync(&h->info->status, 0, sizeof(int), h->st));
   }
-  h->built = true;
+  h->built = h->ever_built = true;
   h->mp_done = h->grouped = h->forced = h->moved_after_forces = false;
   return last_cuda();
 }
@@ -481,7 +492,7 @@ int bonsai_compute_multipoles(bonsai_handle hh) {
   if (!h->built) return BONSAI_ERR_ORDER;
   BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
   h->enq_multipoles();
-  h->mp_done = true;
+  h->mp_done = h->ever_mp = true;
   return last_cuda();
 }
 
@@ -552,7 +563,10 @@ int bonsai_step(bonsai_handle hh, int nsteps, int use_graph) {
   if (nsteps < 0) return BONSAI_ERR_ARG;
   BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
   if (use_graph && !h->graph_ok) {
-    const int rc = h->capture_graphs();
+    // size the cell arrays on the current particles before freezing pointers
+    int rc = h->build_checked(h->cur_nleaf);
+    if (rc) return rc;
+    rc = h->capture_graphs();
     if (rc) return rc;
   }
   for (int s = 0; s < nsteps; s++) {
@@ -565,6 +579,7 @@ int bonsai_step(bonsai_handle hh, int nsteps, int use_graph) {
   }
   if (nsteps > 0) {
     h->built = h->mp_done = h->grouped = false;
+    h->ever_built = h->ever_mp = true;
     h->forced = h->moved_after_forces = true;
   }
   return last_cuda();
@@ -577,7 +592,9 @@ int bonsai_step_timed(bonsai_handle hh, int nsteps, float* phase_ms) {
   if (nsteps < 1 || !phase_ms) return BONSAI_ERR_ARG;
   BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
   if (!h->graph_ok) {
-    const int rc = h->capture_graphs();
+    int rc = h->build_checked(h->cur_nleaf);
+    if (rc) return rc;
+    rc = h->capture_graphs();
     if (rc) return rc;
   }
   std::vector<cudaEvent_t> ev((size_t)4 * nsteps);
@@ -597,6 +614,7 @@ int bonsai_step_timed(bonsai_handle hh, int nsteps, float* phase_ms) {
   }
   for (auto& e : ev) cudaEventDestroy(e);
   h->built = h->mp_done = h->grouped = false;
+  h->ever_built = h->ever_mp = true;
   h->forced = h->moved_after_forces = true;
   return rc ? rc : last_cuda();
 }
@@ -708,7 +726,7 @@ int bonsai_get_cells(bonsai_handle hh, uint32_t* cell_data, float* size4, float*
                      int* leaf_list, int* parent) {
   Handle* h = H(hh);
   if (!h) return BONSAI_ERR_HANDLE;
-  if (!h->built) return BONSAI_ERR_ORDER;
+  if (!h->ever_built) return BONSAI_ERR_ORDER;
   BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
   TreeInfo ti;
   BONSAI_CUDA_TRY(cudaMemcpyAsync(&ti, h->info, sizeof(ti), cudaMemcpyDeviceToHost, h->st));
@@ -719,7 +737,7 @@ int bonsai_get_cells(bonsai_handle hh, uint32_t* cell_data, float* size4, float*
     BONSAI_CUDA_TRY(cudaMemcpyAsync(leaf_list, h->leaf_list, (size_t)ti.nleaves * 4, cudaMemcpyDeviceToHost, h->st));
   if (parent) BONSAI_CUDA_TRY(cudaMemcpyAsync(parent, h->cell_parent, C * 4, cudaMemcpyDeviceToHost, h->st));
   if ((size4 || mono4 || quad0 || quad1) && C > 0) {
-    if (!h->mp_done) return BONSAI_ERR_ORDER;
+    if (!h->ever_mp) return BONSAI_ERR_ORDER;
     float4 *s = nullptr, *m = nullptr, *q0 = nullptr;
     float2* q1 = nullptr;
     BONSAI_CUDA_TRY(dalloc(&s, C));

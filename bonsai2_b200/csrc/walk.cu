@@ -1,8 +1,9 @@
 // walk.cu -- the tree walk: one warp per group, FP32, persistent.
 //
 // Semantics follow treewalk / treewalk_warp (computeForces.cu:229-619):
-//   * a warp takes the next group from an atomic counter (:516-522) and holds
-//     NI particles per lane (NI = 1 for nCrit <= 32, 2 for <= 64, 4 for <= 128);
+//   * a warp takes the next group from an atomic counter (:516-522); its
+//     particles are held in registers, up to 128 per group (the reference
+//     allows 64, :661-694);
 //   * group box from the min/max of its particles (:531-555);
 //   * breadth-first walk from all level-1 cells (:259-263, :511-512);
 //   * a cell is opened when split_node_grav_impbh holds (:30-54) or when it
@@ -33,6 +34,18 @@
 namespace bonsai {
 
 constexpr int kWalkWarps = kWalkThreads / 32;
+
+// Tuning knobs (compile time, like the reference's NWARPS_OCTREE2 / NI
+// template switches): half-warp source split, unroll depth of the 32-entry
+// evaluation loops (the loop body must stay inside the instruction cache).
+#ifndef BONSAI_WALK_SPLIT
+#define BONSAI_WALK_SPLIT 1
+#endif
+#ifndef BONSAI_WALK_UNROLL
+#define BONSAI_WALK_UNROLL 2
+#endif
+#define BONSAI_DO_PRAGMA(x) _Pragma(#x)
+#define BONSAI_UNROLL_N(n) BONSAI_DO_PRAGMA(unroll n)
 
 struct IPart {
   float x, y, z;
@@ -99,7 +112,12 @@ __device__ __forceinline__ int find_src(int incl, int s) {
   return src;
 }
 
-template <int NI>
+// Particle ownership.  SPLIT: lane l holds particles (l & 15) + 16k, k < NI,
+// both half-warps hold the same particles, the two halves evaluate alternate
+// entries of every 32-entry batch and their sums are added once per group, so
+// each broadcast shared-memory load feeds NI (= 4 for nCrit <= 64)
+// interactions.  Otherwise lane l holds l + 32k, k < NI.
+template <int NI, bool SPLIT>
 __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
     k_walk(const int2* __restrict__ groups, const TreeInfo* __restrict__ info, const float4* __restrict__ ipos,
            const float4* __restrict__ jpos, const uint4* __restrict__ cell_data,
@@ -107,11 +125,15 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
            const float4* __restrict__ cell_q1, float eps2, float4* __restrict__ acc, int* __restrict__ ring_pool,
            int ring_cap, unsigned* __restrict__ group_counter, unsigned long long* __restrict__ stats,
            int* __restrict__ status) {
+  constexpr int STRIDE = SPLIT ? 16 : 32;
+  constexpr int JSTEP = SPLIT ? 2 : 1;
   __shared__ float4 s_a0[kWalkWarps][64];
   __shared__ float4 s_a1[kWalkWarps][64];
   __shared__ float4 s_a2[kWalkWarps][64];
   __shared__ float4 s_d[kWalkWarps][64];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int sub = SPLIT ? (lane & 15) : lane;
+  const int half = SPLIT ? (lane >> 4) : 0;
   int* ring = ring_pool + (size_t)(blockIdx.x * kWalkWarps + w) * (size_t)ring_cap;
   const int rmask = ring_cap - 1;
   const int ngroups = info->ngroups;
@@ -132,7 +154,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
     float mnx = 3.0e38f, mny = 3.0e38f, mnz = 3.0e38f, mxx = -3.0e38f, mxy = -3.0e38f, mxz = -3.0e38f;
 #pragma unroll
     for (int k = 0; k < NI; k++) {
-      const float4 p = ipos[pbeg + min(k * 32 + lane, np - 1)];
+      const float4 p = ipos[pbeg + min(k * STRIDE + sub, np - 1)];
       pi[k].x = p.x; pi[k].y = p.y; pi[k].z = p.z;
       ai[k] = make_float4(0.f, 0.f, 0.f, 0.f);
       mnx = fminf(mnx, p.x); mny = fminf(mny, p.y); mnz = fminf(mnz, p.z);
@@ -195,10 +217,12 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
         a_cnt += __popc(bal);
         if (a_cnt >= 32) {
           __syncwarp();
-#pragma unroll 4
-          for (int j = 0; j < 32; j++) {
-            const int sl = (a_head + j) & 63;
-            const float4 a0 = s_a0[w][sl], a1 = s_a1[w][sl], a2 = s_a2[w][sl];
+          const float4* A0 = &s_a0[w][a_head + half];
+          const float4* A1 = &s_a1[w][a_head + half];
+          const float4* A2 = &s_a2[w][a_head + half];
+          BONSAI_UNROLL_N(BONSAI_WALK_UNROLL)
+          for (int j = 0; j < 32; j += JSTEP) {
+            const float4 a0 = A0[j], a1 = A1[j], a2 = A2[j];
 #pragma unroll
             for (int k = 0; k < NI; k++) quad_acc(ai[k], pi[k], a0, a1, a2, eps2);
           }
@@ -223,9 +247,10 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
           d_cnt += cnt;
           if (d_cnt >= 32) {
             __syncwarp();
-#pragma unroll 4
-            for (int j = 0; j < 32; j++) {
-              const float4 pj = s_d[w][(d_head + j) & 63];
+            const float4* D = &s_d[w][d_head + half];
+            BONSAI_UNROLL_N(BONSAI_WALK_UNROLL)
+            for (int j = 0; j < 32; j += JSTEP) {
+              const float4 pj = D[j];
 #pragma unroll
               for (int k = 0; k < NI; k++) mono_acc(ai[k], pi[k], pj, eps2);
             }
@@ -244,30 +269,41 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
 
     // flush the partial batches
     __syncwarp();
-    for (int j = 0; j < a_cnt; j++) {
+    for (int j = half; j < a_cnt; j += JSTEP) {
       const int sl = (a_head + j) & 63;
       const float4 a0 = s_a0[w][sl], a1 = s_a1[w][sl], a2 = s_a2[w][sl];
 #pragma unroll
       for (int k = 0; k < NI; k++) quad_acc(ai[k], pi[k], a0, a1, a2, eps2);
     }
     n_app += a_cnt;
-    for (int j = 0; j < d_cnt; j++) {
+    for (int j = half; j < d_cnt; j += JSTEP) {
       const float4 pj = s_d[w][(d_head + j) & 63];
 #pragma unroll
       for (int k = 0; k < NI; k++) mono_acc(ai[k], pi[k], pj, eps2);
     }
     n_dir += d_cnt;
     __syncwarp();
+    if (SPLIT) {
+#pragma unroll
+      for (int k = 0; k < NI; k++) {
+        ai[k].x += __shfl_xor_sync(kFull, ai[k].x, 16);
+        ai[k].y += __shfl_xor_sync(kFull, ai[k].y, 16);
+        ai[k].z += __shfl_xor_sync(kFull, ai[k].z, 16);
+        ai[k].w += __shfl_xor_sync(kFull, ai[k].w, 16);
+      }
+    }
 
     if (overflow) {
       if (lane == 0) set_status(status, kStatusWalkStack);
 #pragma unroll
       for (int k = 0; k < NI; k++) ai[k] = make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, 0.f);
     }
+    if (half == 0) {
 #pragma unroll
-    for (int k = 0; k < NI; k++) {
-      const int idx = k * 32 + lane;
-      if (idx < np) acc[pbeg + idx] = ai[k];
+      for (int k = 0; k < NI; k++) {
+        const int idx = k * STRIDE + sub;
+        if (idx < np) acc[pbeg + idx] = ai[k];
+      }
     }
     sum_app += (unsigned long long)n_app * (unsigned long long)np;
     sum_dir += (unsigned long long)n_dir * (unsigned long long)np;
@@ -282,31 +318,54 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
   }
 }
 
-int walk_ni(int ncrit) { return ncrit <= 32 ? 1 : (ncrit <= 64 ? 2 : 4); }
+// variants: 0..2 half-warp split with NI = 1, 2, 4 (nCrit <= 16, 32, 64);
+// 3..5 full warp with NI = 1, 2, 4 (nCrit <= 32, 64, 128)
+int walk_variant(int ncrit) {
+#if BONSAI_WALK_SPLIT
+  if (ncrit <= 64) return ncrit <= 16 ? 0 : (ncrit <= 32 ? 1 : 2);
+#endif
+  return ncrit <= 32 ? 3 : (ncrit <= 64 ? 4 : 5);
+}
 
-int walk_blocks_per_sm(int ni) {
+template <int NI, bool SPLIT>
+static int occupancy_of() {
   int nb = 0;
-  cudaError_t e;
-  if (ni == 1) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_walk<1>, kWalkThreads, 0);
-  else if (ni == 2) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_walk<2>, kWalkThreads, 0);
-  else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_walk<4>, kWalkThreads, 0);
-  if (e != cudaSuccess || nb < 1) nb = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_walk<NI, SPLIT>, kWalkThreads, 0) != cudaSuccess || nb < 1)
+    nb = 1;
   return nb;
 }
 
-void launch_walk(int ni, int nblocks, const int2* groups, const TreeInfo* info, const float4* ipos,
+int walk_blocks_per_sm(int variant) {
+  switch (variant) {
+#if BONSAI_WALK_SPLIT
+    case 0: return occupancy_of<1, true>();
+    case 1: return occupancy_of<2, true>();
+    case 2: return occupancy_of<4, true>();
+#endif
+    case 3: return occupancy_of<1, false>();
+    case 4: return occupancy_of<2, false>();
+    default: return occupancy_of<4, false>();
+  }
+}
+
+void launch_walk(int variant, int nblocks, const int2* groups, const TreeInfo* info, const float4* ipos,
                  const float4* jpos, const uint4* cell_data, const float4* cell_open, const float4* cell_q0,
                  const float4* cell_q1, float eps2, float4* acc, int* ring_pool, int ring_cap,
                  unsigned* group_counter, unsigned long long* stats, int* status, cudaStream_t s) {
-  if (ni == 1)
-    k_walk<1><<<nblocks, kWalkThreads, 0, s>>>(groups, info, ipos, jpos, cell_data, cell_open, cell_q0, cell_q1, eps2,
-                                               acc, ring_pool, ring_cap, group_counter, stats, status);
-  else if (ni == 2)
-    k_walk<2><<<nblocks, kWalkThreads, 0, s>>>(groups, info, ipos, jpos, cell_data, cell_open, cell_q0, cell_q1, eps2,
-                                               acc, ring_pool, ring_cap, group_counter, stats, status);
-  else
-    k_walk<4><<<nblocks, kWalkThreads, 0, s>>>(groups, info, ipos, jpos, cell_data, cell_open, cell_q0, cell_q1, eps2,
-                                               acc, ring_pool, ring_cap, group_counter, stats, status);
+#define BONSAI_WALK(NI, SP)                                                                                      \
+  k_walk<NI, SP><<<nblocks, kWalkThreads, 0, s>>>(groups, info, ipos, jpos, cell_data, cell_open, cell_q0, cell_q1, \
+                                                  eps2, acc, ring_pool, ring_cap, group_counter, stats, status)
+  switch (variant) {
+#if BONSAI_WALK_SPLIT
+    case 0: BONSAI_WALK(1, true); break;
+    case 1: BONSAI_WALK(2, true); break;
+    case 2: BONSAI_WALK(4, true); break;
+#endif
+    case 3: BONSAI_WALK(1, false); break;
+    case 4: BONSAI_WALK(2, false); break;
+    default: BONSAI_WALK(4, false); break;
+  }
+#undef BONSAI_WALK
 }
 
 }  // namespace bonsai

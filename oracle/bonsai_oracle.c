@@ -91,9 +91,12 @@ void oracle_plummer(long n, unsigned int seed, double *mass, double *pos, double
 /* ------------------------------------------------------------------------ */
 /* Domain box: restates code/buildTree.cu:80-166 (float min/max; hsize is the
  * smallest power of two >= the largest half-extent; centre truncated to a
- * multiple of hsize/2^20).  The halving loop is floored at 2^-100 so a
- * zero-extent input (one particle, all particles coincident) gives a finite
- * box; the reference loops to hsize == 0 there and divides by zero.
+ * multiple of hsize/2^20).  The halving loop is floored at
+ * max(2^-100, 2^-40 * max|centre|) (powers of two) so that a zero-extent input
+ * (one particle, all particles coincident) gives a finite box whose centre
+ * quantisation fits 64 bits; the reference halves to hsize == 0 there and
+ * divides by zero.  The floor never binds for extents above 2^-40 of the
+ * coordinates.
  * Returns 1 when any coordinate is NaN/Inf, else 0.                        */
 /* ------------------------------------------------------------------------ */
 int oracle_bbox(int n, const float *p4, float *box)
@@ -113,8 +116,14 @@ int oracle_bbox(int n, const float *p4, float *box)
     h[k] = (bmax[k] - bmin[k]) * 0.5f;
   }
   const float hm = fmaxf(h[2], fmaxf(h[1], h[0]));
+  /* floor for hsize: max(2^-100, 2^-40 * (power of two >= max |centre|)),
+   * so that centre/hquant fits a 64-bit integer when the extent is ~0 */
+  const float cm = fmaxf(fabsf(c[0]), fmaxf(fabsf(c[1]), fabsf(c[2])));
+  float pw = 1.0f;
+  while (pw < cm) pw *= 2.0f;
+  while (pw * 0.5f >= cm && pw > 7.888609052210118e-31f) pw *= 0.5f;
+  const float floor_h = fmaxf(pw * 9.094947017729282e-13f, 7.888609052210118e-31f); /* 2^-40, 2^-100 */
   float hsize = 1.0f;
-  const float floor_h = 7.888609052210118e-31f; /* 2^-100 */
   while (hsize > hm && hsize > floor_h) hsize *= 0.5f;
   while (hsize < hm) hsize *= 2.0f;
   const float hquant = hsize / (float)(1 << 20);
