@@ -26,7 +26,7 @@ using namespace bonsai;
 
 namespace {
 
-constexpr int kRingCap = 8192;  // per-warp level-list ring of the walk (ints)
+constexpr int kRingCap = 16384;  // per-warp level lists of the walk (ints): two halves of 8192
 constexpr int kMaxLevelSplit = 7;
 
 template <class T>

@@ -19,8 +19,9 @@
 //     implicit warp-synchronous shared memory;
 //   * range expansion (children, leaf particles) with a shuffle binary search
 //     over the warp's inclusive scan: 32 outputs per step;
-//   * the level lists live in a per-warp ring in global memory (L1/L2
-//     resident), bounded; overflow sets a status bit, never traps;
+//   * the level lists live in a per-warp pair of buffers in global memory
+//     (current level / next level, swapped per level; L1/L2 resident),
+//     bounded; overflow sets a status bit, never traps;
 //   * accepted cells and direct particles are staged by value in per-warp
 //     64-entry shared-memory rings as they are found, so the 32-wide
 //     evaluation loops read broadcast LDS.128 only;
@@ -134,8 +135,11 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int sub = SPLIT ? (lane & 15) : lane;
   const int half = SPLIT ? (lane >> 4) : 0;
-  int* ring = ring_pool + (size_t)(blockIdx.x * kWalkWarps + w) * (size_t)ring_cap;
-  const int rmask = ring_cap - 1;
+  // two halves of the warp's list buffer: the current level is read from one
+  // while the next is written to the other, so the hot footprint stays ~2x the
+  // widest level (a sweeping ring would push its dirty lines out to HBM)
+  int* lists = ring_pool + (size_t)(blockIdx.x * kWalkWarps + w) * (size_t)ring_cap;
+  const int half_cap = ring_cap >> 1;
   const int ngroups = info->ngroups;
   const int l1b = info->level_beg[1], l1e = info->level_end[1];
   const unsigned lt = lanemask_lt();
@@ -167,18 +171,19 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
     const float3 gs = make_float3(__fmul_rn(0.5f, __fsub_rn(mxx, mnx)), __fmul_rn(0.5f, __fsub_rn(mxy, mny)),
                                   __fmul_rn(0.5f, __fsub_rn(mxz, mnz)));
 
-    int cur_off = 0, ncur = l1e - l1b, nnext = 0;
-    for (int j = lane; j < ncur; j += 32) ring[j & rmask] = l1b + j;
+    int cb = 0;  // base of the current level's half; the next level's is cb ^ half_cap
+    int ncur = l1e - l1b, nnext = 0;
+    bool overflow = ncur > half_cap;
+    for (int j = lane; j < ncur && !overflow; j += 32) lists[j] = l1b + j;
     int a_head = 0, a_cnt = 0, d_head = 0, d_cnt = 0;
     unsigned n_app = 0, n_dir = 0;
-    bool overflow = ncur > ring_cap;
     __syncwarp();
 
     while (ncur > 0 && !overflow) {
       for (int blk = 0; blk < ncur; blk += 32) {
         const int li = blk + lane;
         const bool valid = li < ncur;
-        const int cell = valid ? ring[(cur_off + li) & rmask] : 0;
+        const int cell = valid ? lists[cb + li] : 0;
         uint4 cd = make_uint4(0u, 0xFFFFFFFFu, 0u, 0u);
         float4 co = make_float4(0.f, 0.f, 0.f, 0.f);
         if (valid) {
@@ -192,15 +197,14 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
         const int nch = (split && !leaf) ? (int)(cd.y >> 29) + 1 : 0;
         const int incl = warp_incl_scan(nch);
         const int tot = __shfl_sync(kFull, incl, 31);
-        if (ncur - blk + nnext + tot > ring_cap) { overflow = true; break; }
-        const int wbase = cur_off + ncur + nnext;
+        if (nnext + tot > half_cap) { overflow = true; break; }
         const int first = (int)(cd.y & 0x1FFFFFFFu);
         for (int base = 0; base < tot; base += 32) {
           const int s = base + lane;
           const int src = find_src(incl, s);
           const int f = __shfl_sync(kFull, first, src);
           const int e = __shfl_sync(kFull, incl - nch, src);
-          if (s < tot) ring[(wbase + s) & rmask] = f + (s - e);
+          if (s < tot) lists[(cb ^ half_cap) + nnext + s] = f + (s - e);
         }
         nnext += tot;
 
@@ -261,7 +265,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
           }
         }
       }
-      cur_off += ncur;
+      cb ^= half_cap;
       ncur = nnext;
       nnext = 0;
       __syncwarp();
