@@ -59,6 +59,7 @@ SIGNATURES = {
     "bonsai_get_groups": (I, [P, P]),
     "bonsai_get_walk_arrays": (I, [P, P, P, P, P]),
     "bonsai_direct_fp64": (I, [P, P, I, I, P]),
+    "bonsai_direct_fp64_noalloc": (I, [P, I, P, I, ctypes.c_double, I, P, P]),
     "bonsai_plummer": (I, [ctypes.c_long, ctypes.c_uint, P, P]),
     "bonsai_host_alloc": (P, [ctypes.c_size_t]),
     "bonsai_host_free": (None, [P]),

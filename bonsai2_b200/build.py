@@ -24,7 +24,8 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INCLUDE
 # extra -D tuning flags (e.g. BONSAI_WALK_SPLIT=0) for alternative builds
 EXTRA = os.environ.get("BONSAI_NVCC_DEFINES", "").split()
 PER_FILE = {"walk.cu": ["-ftz=true"]}
-SOURCES = ["keys.cu", "sort.cu", "tree.cu", "multipoles.cu", "groups.cu", "walk.cu", "move.cu", "treecode.cu"]
+SOURCES = ["keys.cu", "sort.cu", "tree.cu", "multipoles.cu", "groups.cu", "walk.cu", "move.cu", "treecode.cu",
+           "noalloc.cu"]
 HOST_SOURCES = ["plummer.cpp"]
 
 

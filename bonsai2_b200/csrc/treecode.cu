@@ -664,6 +664,7 @@ const char* bonsai_error_string(int code) {
     case BONSAI_ERR_ORDER: return "stage called before the stage it depends on";
     case BONSAI_ERR_ARG: return "invalid argument";
     case BONSAI_ERR_NO_DEVICE: return "no CUDA device";
+    case BONSAI_ERR_TOO_LARGE: return "request exceeds the fixed scratch capacity (bonsai_direct_fp64_noalloc: ns <= 65536)";
     default: break;
   }
   if (code > 0) {

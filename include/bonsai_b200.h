@@ -42,6 +42,7 @@ extern "C" {
 #define BONSAI_ERR_ORDER (-3)     /* a stage was called before the stage it needs */
 #define BONSAI_ERR_ARG (-4)
 #define BONSAI_ERR_NO_DEVICE (-5)
+#define BONSAI_ERR_TOO_LARGE (-6) /* request beyond a fixed capacity (bonsai_direct_fp64_noalloc) */
 
 typedef struct bonsai_handle_s *bonsai_handle;
 
@@ -154,6 +155,20 @@ int bonsai_get_walk_arrays(bonsai_handle h, float *ipos4, float *jpos4, float *a
 /* FP64 direct summation for ns sample particles (caller indices) against all
  * particles -- the force checker.  out double[4*ns] = (ax, ay, az, phi). */
 int bonsai_direct_fp64(bonsai_handle h, const int *sample, int ns, int include_self, double *out);
+
+/* The FP64 direct-sum checker for callers that cannot allocate device memory
+ * (their GPU memory belongs to another framework's allocator, or their loop
+ * must not pay cudaMalloc's device-wide synchronisation).  No counterpart in
+ * the reference.  All pointers are device memory: d_pos4 = n float4 (x,y,z,m),
+ * d_sample = ns particle indices, d_out = double[4*ns] (ax, ay, az, phi);
+ * eps2 = softening squared; stream = a cudaStream_t (NULL: the legacy default
+ * stream).  Allocates nothing: its scratch is a fixed 2 MiB device array in
+ * the library, so ns <= 65536 (larger: BONSAI_ERR_TOO_LARGE).  Calls share
+ * that array: calls that overlap on the GPU race and must be serialised.  The
+ * first call on a device looks the array up (cudaGetSymbolAddress); make it
+ * before any stream capture on that device.  Asynchronous on `stream`. */
+int bonsai_direct_fp64_noalloc(const float *d_pos4, int n, const int *d_sample, int ns, double eps2,
+                               int include_self, double *d_out, void *stream);
 
 /* Plummer sphere initial conditions on the host: the algorithm of
  * code/plummer.h:9-138 (glibc rand(), same stream), converted to float4 like
