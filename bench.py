@@ -61,7 +61,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--particles", type=int, default=1 << 24, dest="n")
     ap.add_argument("--theta", type=float, default=0.6)
-    ap.add_argument("--sweep", default="0.3,0.4,0.5,0.6", help="thetas of the sweep reported beside the headline")
+    ap.add_argument("--sweep", default="0.3,0.4,0.5,0.6,0.7,0.8", help="thetas of the sweep reported beside the headline")
+    ap.add_argument("--learned-target", type=float, default=1e-3,
+                    help="per-group error target of the learned opening angles (0: skip the learned form)")
     ap.add_argument("--eps", type=float, default=0.005)
     ap.add_argument("--nleaf", type=int, default=16)
     ap.add_argument("--ncrit", type=int, default=64)
@@ -330,6 +332,7 @@ def run_ours(a):
 
     t.close()
     sweep = theta_sweep(B, L, pos, vel, a, d.local) if (d.rank == 0 and a.sweep) else None
+    learned = learned_theta(B, L, pos, vel, a, d.local, sweep) if (d.rank == 0 and a.learned_target > 0) else None
 
     cpu = None
     if d.rank == 0 and d.world == 1 and not a.no_cpu_baseline:
@@ -367,7 +370,10 @@ def run_ours(a):
                        "steps_between": a.steps},
             "status": int(status),
             "theta_sweep": sweep,
+            "learned_theta": learned,
         }
+        if learned:
+            learned["vs_fixed_headline"] = learned["value"] / value
         print(json.dumps(line), flush=True)
     for hptr in (hp, hv, ha):
         L.bonsai_host_free(hptr)
@@ -413,6 +419,75 @@ def theta_sweep(B, L, pos, vel, a, device):
                     "approx_per_particle": float(st[0]) / n, "direct_per_particle": float(st[1]) / n,
                     "median_rel_force_err": float(np.median(err)), "p99_rel_force_err": float(np.percentile(err, 99))})
         t.close()
+    return out
+
+
+def learned_theta(B, L, pos, vel, a, device, sweep):
+    """The learned form: per-group opening angles from the MLP, trained on a
+    Plummer sphere of another seed (untimed setup), then timed on the bench
+    system like the headline and judged against the FP64 direct sum; compared
+    with the fixed angles of the sweep at equal median and equal p99 error."""
+    from bonsai2_b200 import learned as Lr
+    from bonsai2_b200.treecode import _p
+    n = pos.shape[0]
+    t0 = time.perf_counter()
+    ptr, vtr = B.plummer(n, a.seed + 1)
+    X, y, _ = Lr.training_set(ptr, vtr, eps=a.eps, target=a.learned_target, max_groups=8192, nleaf=a.nleaf,
+                              ncrit=a.ncrit, level_split=a.level_split, device=device)
+    w, loss = Lr.train(X, y, epochs=3000, lr=3e-3, device=device)
+    t_train = time.perf_counter() - t0
+    t = B.Treecode(eps=a.eps, theta=a.theta, ncrit=a.ncrit, nleaf=a.nleaf, level_split=a.level_split, dt=a.dt,
+                   device=device)
+    t.alloc(n)
+    Lr.set_weights(t, w)
+    Lr.set_theta_mode(t, 1)
+    L.bonsai_set_particles(t.handle, _p(pos), _p(vel), n)
+    t.buildTree(a.nleaf)
+    t.computeMultipoles()
+    t.makeGroups(a.level_split, a.ncrit)
+    t.computeForces(False)
+    acc = t.get_acc().astype(np.float64)
+    th = Lr.group_theta(t)
+    rng = np.random.default_rng(2048)
+    samp = np.ascontiguousarray(rng.choice(n, min(2048, n), replace=False).astype(np.int32))
+    ref = t.direct_fp64(samp, include_self=True)
+    err = np.linalg.norm(acc[samp, :3] - ref[:, :3], axis=1) / np.linalg.norm(ref[:, :3], axis=1)
+    L.bonsai_set_particles(t.handle, _p(pos), _p(vel), n)
+    t.step(2, graph=True)
+    t.synchronize()
+    ph = np.zeros(4 * a.steps + 1, np.float32)
+    rc = L.bonsai_step_timed(t.handle, a.steps, _p(ph))
+    if rc:
+        raise B.BonsaiError(rc, "learned steps")
+    st = np.zeros(4, np.uint64)
+    L.bonsai_get_stats(t.handle, _p(st))
+    t.close()
+    ms = float(ph[4 * a.steps]) / a.steps
+    walk = float(np.median(ph[:4 * a.steps].reshape(a.steps, 4)[:, 1]))
+    flops_pp = (20.0 * float(st[1]) + 64.0 * float(st[0])) / n
+    med, p99 = float(np.median(err)), float(np.percentile(err, 99))
+
+    def at_equal(key):
+        # fixed-angle throughput at the learned error, log-log between sweep points
+        pts = sorted(((s[key], s["value"]) for s in (sweep or [])), key=lambda x: x[0])
+        e = med if key == "median_rel_force_err" else p99
+        for (e0, v0), (e1, v1) in zip(pts, pts[1:]):
+            if e0 <= e <= e1 and e1 > e0:
+                f = (np.log(e) - np.log(e0)) / (np.log(e1) - np.log(e0))
+                return float(np.exp(np.log(v0) + f * (np.log(v1) - np.log(v0))))
+        return None
+
+    out = {"value": n / (ms * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": ms, "walk_ms": walk,
+           "walk_tflops": flops_pp * n / (walk * 1e-3) / 1e12, "flops_per_particle": flops_pp,
+           "median_rel_force_err": med, "p99_rel_force_err": p99, "target": a.learned_target,
+           "theta_mean": float(th.mean()), "theta_p10_p90": [float(np.percentile(th, 10)), float(np.percentile(th, 90))],
+           "training": {"system": "Plummer N=%d seed %d" % (n, a.seed + 1), "pairs": int(X.shape[0]),
+                        "final_loss": loss, "seconds": t_train}}
+    eq_m, eq_p = at_equal("median_rel_force_err"), at_equal("p99_rel_force_err")
+    out["fixed_theta_value_at_equal_median"] = eq_m
+    out["fixed_theta_value_at_equal_p99"] = eq_p
+    out["gain_at_equal_median"] = out["value"] / eq_m if eq_m else None
+    out["gain_at_equal_p99"] = out["value"] / eq_p if eq_p else None
     return out
 
 

@@ -60,6 +60,14 @@ SIGNATURES = {
     "bonsai_get_walk_arrays": (I, [P, P, P, P, P]),
     "bonsai_direct_fp64": (I, [P, P, I, I, P]),
     "bonsai_direct_fp64_noalloc": (I, [P, I, P, I, ctypes.c_double, I, P, P]),
+    "bonsai_set_theta_mode": (I, [P, I, ctypes.c_float, ctypes.c_float]),
+    "bonsai_set_mlp_weights": (I, [P, P, I]),
+    "bonsai_set_group_theta": (I, [P, P, I]),
+    "bonsai_get_group_features": (I, [P, P, P]),
+    "bonsai_get_group_theta": (I, [P, P]),
+    "bonsai_mlp_loss_grad": (I, [I, P, P, I, P, ctypes.c_float, ctypes.c_float, ctypes.c_float, P, P]),
+    "bonsai_mlp_train": (I, [I, P, P, I, P, I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, P]),
+    "bonsai_mlp_predict": (I, [I, P, I, P, ctypes.c_float, ctypes.c_float, P]),
     "bonsai_plummer": (I, [ctypes.c_long, ctypes.c_uint, P, P]),
     "bonsai_host_alloc": (P, [ctypes.c_size_t]),
     "bonsai_host_free": (None, [P]),

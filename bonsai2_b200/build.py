@@ -25,7 +25,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INCLUDE
 EXTRA = os.environ.get("BONSAI_NVCC_DEFINES", "").split()
 PER_FILE = {"walk.cu": ["-ftz=true"]}
 SOURCES = ["keys.cu", "sort.cu", "tree.cu", "multipoles.cu", "groups.cu", "walk.cu", "move.cu", "treecode.cu",
-           "noalloc.cu"]
+           "noalloc.cu", "learned.cu"]
 HOST_SOURCES = ["plummer.cpp"]
 
 

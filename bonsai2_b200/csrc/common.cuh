@@ -28,6 +28,7 @@ enum : int {
   kStatusNonFinite = 1 << 3,      // NaN/Inf coordinate seen by the box reduction
   kStatusGroupCapacity = 1 << 4,  // more groups than the group array holds
   kStatusBadParam = 1 << 5,
+  kStatusSortTimeout = 1 << 6,    // a sort look-back wait hit its bound (results invalid)
 };
 
 // Device-resident tree/group bookkeeping: written by the build kernels and

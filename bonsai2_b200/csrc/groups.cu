@@ -7,43 +7,43 @@
 // particles, numbering groups with an atomic counter.  The masked key of a
 // sorted key is its top 3*levelSplit bits, i.e. a bin index in
 // [0, 8^levelSplit); bins appear in increasing order along the sorted array.
-// So a histogram over bins gives every segment's size, one exclusive scan its
-// start, a second scan over ceil(size/nCrit) the group offsets, and groups are
-// written in PH order (deterministic; the reference's canonical order).
+// So the segment of every bin is found where the bin changes (one pass, no
+// atomics), one exclusive scan over ceil(size/nCrit) gives the group offsets,
+// and groups are written in PH order (deterministic; the reference's
+// canonical order).
 #include "common.cuh"
 #include "kernels.cuh"
 
 namespace bonsai {
 
-__global__ void __launch_bounds__(256) k_group_hist(const unsigned long long* __restrict__ sorted, int n, int shift,
-                                                    unsigned* __restrict__ count) {
-  // 16 consecutive keys per thread; one atomic per run of equal bin
-  const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * 16;
-  if (i0 >= n) return;
-  const int i1 = min(i0 + 16, n);
-  unsigned long long cur = sorted[i0] >> shift;
-  unsigned run = 0;
-  for (int i = i0; i < i1; i++) {
-    const unsigned long long b = sorted[i] >> shift;
-    if (b != cur) {
-      atomicAdd(count + cur, run);
-      cur = b;
-      run = 0;
+// Segment bounds straight from the sorted keys: position i starts the segment
+// of bin(i) when bin(i) != bin(i-1), and ends the segment of bin(i-1) there.
+// Each bin has one start and one end, so every entry is written by exactly one
+// thread (no atomics); empty bins keep [0, 0) from the memset.
+__global__ void __launch_bounds__(256) k_group_bounds(const unsigned long long* __restrict__ sorted, int n,
+                                                      int shift, unsigned* __restrict__ seg_beg,
+                                                      unsigned* __restrict__ seg_end) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const unsigned b = (unsigned)(sorted[i] >> shift);
+    const unsigned p = i > 0 ? (unsigned)(sorted[i - 1] >> shift) : ~0u;
+    if (b != p) {
+      seg_beg[b] = (unsigned)i;
+      if (i > 0) seg_end[p] = (unsigned)i;
     }
-    run++;
+    if (i == n - 1) seg_end[b] = (unsigned)n;
   }
-  atomicAdd(count + cur, run);
 }
 
-__global__ void k_group_sizes(const unsigned* __restrict__ count, int nbins, int ncrit, unsigned* __restrict__ ng) {
+__global__ void k_group_sizes(const unsigned* __restrict__ seg_beg, const unsigned* __restrict__ seg_end, int nbins,
+                              int ncrit, unsigned* __restrict__ ng) {
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nbins; b += gridDim.x * blockDim.x)
-    ng[b] = (count[b] + (unsigned)ncrit - 1u) / (unsigned)ncrit;
+    ng[b] = (seg_end[b] - seg_beg[b] + (unsigned)ncrit - 1u) / (unsigned)ncrit;
 }
 
 // one thread per group: the group's bin is found by binary search over the
 // exclusive scan of group counts (bins near a dense core hold 10^5 groups, so
 // a thread per bin would serialise them)
-__global__ void __launch_bounds__(256) k_group_write(const unsigned* __restrict__ count,
+__global__ void __launch_bounds__(256) k_group_write(const unsigned* __restrict__ seg_end,
                                                      const unsigned* __restrict__ seg_start,
                                                      const unsigned* __restrict__ goff, int nbins, int ncrit,
                                                      int2* __restrict__ groups, int group_cap,
@@ -63,22 +63,22 @@ __global__ void __launch_bounds__(256) k_group_write(const unsigned* __restrict_
     // offset with the next bin)
     const int k = g - (int)goff[lo];
     const int off = k * ncrit;
-    groups[g] = make_int2((int)seg_start[lo] + off, min(ncrit, (int)count[lo] - off));
+    const int count = (int)(seg_end[lo] - seg_start[lo]);
+    groups[g] = make_int2((int)seg_start[lo] + off, min(ncrit, count - off));
   }
 }
 
-void make_groups(const unsigned long long* sorted_ph, int n, int level_split, int ncrit, unsigned* count,
+void make_groups(const unsigned long long* sorted_ph, int n, int level_split, int ncrit, unsigned* seg_end,
                  unsigned* seg_start, unsigned* ng, unsigned* bsum, int2* groups, int group_cap, TreeInfo* info,
                  cudaStream_t s) {
   const int nbins = 1 << (3 * level_split);
   const int shift = 63 - 3 * level_split;
-  cudaMemsetAsync(count, 0, sizeof(unsigned) * (size_t)nbins, s);
-  const int nthr = (n + 15) / 16;
-  k_group_hist<<<(nthr + 255) / 256, 256, 0, s>>>(sorted_ph, n, shift, count);
-  exclusive_scan(count, seg_start, nbins, bsum, nullptr, s);
-  k_group_sizes<<<(nbins + 255) / 256, 256, 0, s>>>(count, nbins, ncrit, ng);
+  cudaMemsetAsync(seg_start, 0, sizeof(unsigned) * (size_t)nbins, s);
+  cudaMemsetAsync(seg_end, 0, sizeof(unsigned) * (size_t)nbins, s);
+  k_group_bounds<<<1184, 256, 0, s>>>(sorted_ph, n, shift, seg_start, seg_end);
+  k_group_sizes<<<(nbins + 255) / 256, 256, 0, s>>>(seg_start, seg_end, nbins, ncrit, ng);
   exclusive_scan(ng, ng, nbins, bsum, (unsigned*)&info->ngroups, s);
-  k_group_write<<<1184, 256, 0, s>>>(count, seg_start, ng, nbins, ncrit, groups, group_cap, info);
+  k_group_write<<<1184, 256, 0, s>>>(seg_end, seg_start, ng, nbins, ncrit, groups, group_cap, info);
 }
 
 // state gather: out[k] = in[perm[k]] for positions, velocities and ids

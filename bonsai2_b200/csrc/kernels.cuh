@@ -6,6 +6,9 @@
 namespace bonsai {
 
 constexpr int kWalkThreads = 256;
+constexpr int kMlpFeatures = 16;
+constexpr int kMlpHidden = 64;
+constexpr int kMlpWeights = kMlpHidden * kMlpFeatures + kMlpHidden + kMlpHidden * kMlpHidden + kMlpHidden + kMlpHidden + 1;
 #ifndef BONSAI_WALK_MINB
 #define BONSAI_WALK_MINB 3
 #endif
@@ -23,8 +26,9 @@ __global__ void k_keys(const float4* __restrict__ pos, int n, const Box* __restr
 int sort_tiles(int n);
 int scan_blocks(int m);
 void exclusive_scan(const unsigned* in, unsigned* out, int m, unsigned* bsum, unsigned* total, cudaStream_t s);
+size_t sort_status_words(int n);
 void radix_sort_pairs(unsigned long long* keys_a, unsigned long long* keys_b, int* vals_a, int* vals_b,
-                      const int* vals_in, int n, unsigned* counts, unsigned* bsum, int passes, cudaStream_t s);
+                      const int* vals_in, int n, unsigned* work, int* err, int passes, cudaStream_t s);
 
 // tree.cu
 int tree_tiles(int n);
@@ -37,7 +41,8 @@ __global__ void k_multipoles(const int* __restrict__ leaf_list, const TreeInfo* 
                              const uint4* __restrict__ cell_data, const int* __restrict__ cell_parent,
                              const float4* __restrict__ jpos, float inv_theta, MpRec* __restrict__ rec,
                              float4* __restrict__ cell_open, float4* __restrict__ cell_q0,
-                             float4* __restrict__ cell_q1, int* __restrict__ mp_count, int cell_cap);
+                             float4* __restrict__ cell_q1, float2* __restrict__ cell_ls, int* __restrict__ mp_count,
+                             int cell_cap);
 __global__ void k_multipoles_ref_layout(const TreeInfo* __restrict__ info, const float4* __restrict__ cell_open,
                                         const MpRec* __restrict__ rec, float4* __restrict__ size,
                                         float4* __restrict__ mono, float4* __restrict__ quad0,
@@ -56,10 +61,12 @@ __global__ void k_gather_pos(const int* __restrict__ perm, int n, const float4* 
 // walk.cu
 int walk_variant(int ncrit);
 int walk_blocks_per_sm(int variant);
+// group_inv_theta == nullptr: the fixed opening angle baked into cell_open.w;
+// else 1/theta per group with (l, s) from cell_ls
 void launch_walk(int variant, int nblocks, const int2* groups, const TreeInfo* info, const float4* ipos, const float4* jpos,
                  const uint4* cell_data, const float4* cell_open, const float4* cell_q0, const float4* cell_q1,
-                 float eps2, float4* acc, int* ring_pool, int ring_cap, unsigned* group_counter,
-                 unsigned long long* stats, int* status, cudaStream_t s);
+                 const float2* cell_ls, const float* group_inv_theta, float eps2, float4* acc, int* ring_pool,
+                 int ring_cap, unsigned* group_counter, unsigned long long* stats, int* status, cudaStream_t s);
 
 // move.cu
 void launch_move(float4* pos, float4* vel, const float4* acc, int n, float dt, int* closing, float eps, int write,
@@ -70,5 +77,21 @@ __global__ void k_scatter_by_id(const int* __restrict__ id, int n, const float4*
                                 float4* __restrict__ out);
 __global__ void k_iota(int* __restrict__ a, int n);
 double fma_probe_tflops(int nsm, cudaStream_t st, float* scratch);
+
+// learned.cu
+size_t mlp_train_scratch_floats(int S);
+void mlp_loss_grad(const float* X, const float* y, int S, const float* w, float lo, float hi, float over,
+                   float* scratch, float* grad, double* loss_out, cudaStream_t st);
+void mlp_adam_step(float* w, const float* grad, float* m, float* v, float lr, int step, cudaStream_t st);
+void mlp_predict(const float* X, int S, const float* w, float lo, float hi, float* scratch, float* pred,
+                 cudaStream_t st);
+void launch_group_features(const int2* groups, const TreeInfo* info, const float4* ipos,
+                           const unsigned long long* ph_sorted, const MpRec* rec, const Box* box, int n, int ncrit,
+                           float eps, float* feat, int nblocks, cudaStream_t st);
+void launch_mlp_infer(const float* feat, const void* wh, const TreeInfo* info, float lo, float hi, float* inv,
+                      int nblocks, cudaStream_t st);
+void launch_weights_to_half(const float* w, void* wh, cudaStream_t st);
+void launch_fill_inv_theta(const TreeInfo* info, const float* theta, float c, float* inv, int nblocks,
+                           cudaStream_t st);
 
 }  // namespace bonsai

@@ -1,0 +1,342 @@
+// learned.cu -- per-group opening angles from a small MLP.
+//
+// A group's opening angle theta_g trades its force error against its walk
+// cost.  Groups differ (a group in the dense core sees most of its force from
+// nearby cells, one in the halo from far away), so one angle for all groups
+// must suit the worst of them.  Here a 16 -> 64 -> 64 -> 1 network maps cheap
+// group features to theta_g; it is trained on pairs (features, largest theta
+// meeting a per-group error target) that the fixed-angle walk and the FP64
+// direct sum generate (bonsai2_b200/learned.py), with this file's own forward
+// and backward kernels.  The walk then runs with per-group angles
+// (walk.cu, PERGROUP).  Fixed-angle walking stays available (theta mode 0).
+//
+// Weight vector layout (kMlpWeights floats): W1[64][16], b1[64], W2[64][64],
+// b2[64], w3[64], b3.  Hidden activations tanh; output
+// theta = lo + (hi - lo) * sigmoid(z).
+#include "common.cuh"
+#include "kernels.cuh"
+
+#include <cuda_fp16.h>
+
+namespace bonsai {
+
+constexpr int kF = kMlpFeatures, kH = kMlpHidden;
+constexpr int oW1 = 0, oB1 = oW1 + kH * kF, oW2 = oB1 + kH, oB2 = oW2 + kH * kH, oW3 = oB2 + kH, oB3 = oW3 + kH;
+static_assert(oB3 + 1 == kMlpWeights, "weight layout");
+
+__device__ __forceinline__ float safe_log10(float x) { return log10f(fmaxf(x, 1e-30f)); }
+
+// ---------------------------------------------------------------------------
+// Group features (one warp per group; groups are contiguous in PH order).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_group_features(const int2* __restrict__ groups,
+                                                        const TreeInfo* __restrict__ info,
+                                                        const float4* __restrict__ ipos,
+                                                        const unsigned long long* __restrict__ ph_sorted,
+                                                        const MpRec* __restrict__ rec, const Box* __restrict__ box,
+                                                        int n, int ncrit, float eps, float* __restrict__ feat) {
+  const int lane = threadIdx.x & 31;
+  const int ng = info->ngroups;
+  // system centre of mass and mass from the level-1 cells
+  double M = 0, X = 0, Y = 0, Z = 0;
+  for (int c = info->level_beg[1]; c < info->level_end[1]; c++) {
+    const double m = rec[c].m;
+    M += m; X += m * rec[c].cx; Y += m * rec[c].cy; Z += m * rec[c].cz;
+  }
+  const float mtot = (float)M;
+  const float cx = M > 0 ? (float)(X / M) : 0.f, cy = M > 0 ? (float)(Y / M) : 0.f, cz = M > 0 ? (float)(Z / M) : 0.f;
+  const float hs = box->hsize;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < ng; g += nw) {
+    const int2 gd = groups[g];
+    const int pb = gd.x, np = gd.y;
+    float mn[3] = {3e38f, 3e38f, 3e38f}, mx[3] = {-3e38f, -3e38f, -3e38f};
+    float mg = 0.f;
+    for (int i = lane; i < np; i += 32) {
+      const float4 p = ipos[pb + i];
+      mn[0] = fminf(mn[0], p.x); mn[1] = fminf(mn[1], p.y); mn[2] = fminf(mn[2], p.z);
+      mx[0] = fmaxf(mx[0], p.x); mx[1] = fmaxf(mx[1], p.y); mx[2] = fmaxf(mx[2], p.z);
+      mg += p.w;
+    }
+    for (int k = 0; k < 3; k++) { mn[k] = warp_min_f32(mn[k]); mx[k] = warp_max_f32(mx[k]); }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) mg += __shfl_xor_sync(kFull, mg, o);
+    const float gx = 0.5f * (mx[0] + mn[0]), gy = 0.5f * (mx[1] + mn[1]), gz = 0.5f * (mx[2] + mn[2]);
+    const float sx = 0.5f * (mx[0] - mn[0]), sy = 0.5f * (mx[1] - mn[1]), sz = 0.5f * (mx[2] - mn[2]);
+    const float rg = fmaxf(sqrtf(sx * sx + sy * sy + sz * sz), 1e-12f * hs);
+    // mean distance from the group centre (concentration)
+    float md = 0.f;
+    for (int i = lane; i < np; i += 32) {
+      const float4 p = ipos[pb + i];
+      md += sqrtf((p.x - gx) * (p.x - gx) + (p.y - gy) * (p.y - gy) + (p.z - gz) * (p.z - gz));
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) md += __shfl_xor_sync(kFull, md, o);
+    if (lane == 0) {
+      const float dg = sqrtf((gx - cx) * (gx - cx) + (gy - cy) * (gy - cy) + (gz - cz) * (gz - cz));
+      const int lvl = diff_level(ph_sorted[pb], ph_sorted[pb + np - 1]) - 1;  // common PH prefix (levels)
+      const float vol = rg * rg * rg;
+      float f[kF];
+      f[0] = (float)np / (float)ncrit;
+      f[1] = safe_log10(rg / hs) / 6.f;
+      f[2] = safe_log10(dg / hs + 1e-7f) / 6.f;
+      f[3] = safe_log10(rg / fmaxf(dg, 1e-12f * hs)) / 3.f;
+      f[4] = (float)min(lvl, kMaxLevel) / (float)kMaxLevel;
+      f[5] = safe_log10(mg / fmaxf(mtot, 1e-30f)) / 8.f;
+      f[6] = safe_log10((float)np / vol * hs * hs * hs / (float)n) / 8.f;
+      f[7] = sx / rg; f[8] = sy / rg; f[9] = sz / rg;
+      f[10] = log10f((float)n) / 8.f;
+      f[11] = safe_log10(fmaxf(eps, 1e-12f) / rg) / 3.f;
+      f[12] = safe_log10(fmaxf(eps, 1e-12f) / hs) / 6.f;
+      f[13] = dg / (dg + rg);
+      f[14] = (md / (float)np) / rg;
+      f[15] = 1.0f;
+      float* o = feat + (size_t)g * kF;
+#pragma unroll
+      for (int k = 0; k < kF; k++) o[k] = f[k];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Inference: FP16 weights in shared memory, FP32 accumulation; one warp per
+// group (lane holds hidden units lane and lane+32) writes 1/theta_g.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_mlp_infer(const float* __restrict__ feat, const __half* __restrict__ wh,
+                                                   const TreeInfo* __restrict__ info, float lo, float hi,
+                                                   float* __restrict__ group_inv_theta) {
+  __shared__ __half sw[kMlpWeights + 1];
+  __shared__ float sh[8][kH];
+  for (int t = threadIdx.x; t < kMlpWeights; t += blockDim.x) sw[t] = wh[t];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+  const int ng = info->ngroups;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < ng; g += nw) {
+    const float xk = lane < kF ? feat[(size_t)g * kF + lane] : 0.f;
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const int j = lane + 32 * u;
+      float a = __half2float(sw[oB1 + j]);
+#pragma unroll
+      for (int k = 0; k < kF; k++) a = fmaf(__half2float(sw[oW1 + j * kF + k]), __shfl_sync(kFull, xk, k), a);
+      sh[wi][j] = tanhf(a);
+    }
+    __syncwarp();
+    float z = 0.f;
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const int j = lane + 32 * u;
+      float a = __half2float(sw[oB2 + j]);
+#pragma unroll 8
+      for (int i = 0; i < kH; i++) a = fmaf(__half2float(sw[oW2 + j * kH + i]), sh[wi][i], a);
+      z = fmaf(__half2float(sw[oW3 + j]), tanhf(a), z);
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) z += __shfl_xor_sync(kFull, z, o);
+    z += __half2float(sw[oB3]);
+    if (lane == 0) group_inv_theta[g] = 1.0f / (lo + (hi - lo) / (1.0f + expf(-z)));
+    __syncwarp();
+  }
+}
+
+__global__ void k_weights_to_half(const float* __restrict__ w, __half* __restrict__ wh) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < kMlpWeights; t += gridDim.x * blockDim.x)
+    wh[t] = __float2half_rn(w[t]);
+}
+
+__global__ void k_fill_inv_theta(const TreeInfo* __restrict__ info, const float* __restrict__ theta, float c,
+                                 float* __restrict__ inv) {
+  const int ng = info->ngroups;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x)
+    inv[g] = 1.0f / (theta ? theta[g] : c);
+}
+
+// ---------------------------------------------------------------------------
+// Training.  Loss per sample: 0.5 (theta - y)^2 (1 + over [theta > y]), mean
+// over the S samples (over-prediction costs accuracy, so it is weighted).
+// k_mlp_fwd_bwd: one warp per sample (lane holds hidden units lane, lane+32),
+// stores the activations and back-propagated deltas; the weight gradients are
+// then fixed-order sums over samples (deterministic).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_mlp_fwd_bwd(const float* __restrict__ X, const float* __restrict__ y, int S,
+                                                     const float* __restrict__ w, float lo, float hi, float over,
+                                                     float* __restrict__ H1, float* __restrict__ D1,
+                                                     float* __restrict__ H2, float* __restrict__ D2,
+                                                     float* __restrict__ G, float* __restrict__ loss,
+                                                     float* __restrict__ pred) {
+  __shared__ float sh[8][2][kH];
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < S; s += nw) {
+    float x[kF];
+#pragma unroll
+    for (int k = 0; k < kF; k++) x[k] = X[(size_t)s * kF + k];
+    float h1[2], h2[2];
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const int j = lane + 32 * u;
+      float a = w[oB1 + j];
+#pragma unroll
+      for (int k = 0; k < kF; k++) a = fmaf(w[oW1 + j * kF + k], x[k], a);
+      h1[u] = tanhf(a);
+      sh[wi][0][j] = h1[u];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const int j = lane + 32 * u;
+      float a = w[oB2 + j];
+      for (int i = 0; i < kH; i++) a = fmaf(w[oW2 + j * kH + i], sh[wi][0][i], a);
+      h2[u] = tanhf(a);
+    }
+    float z = w[oW3 + lane] * h2[0] + w[oW3 + lane + 32] * h2[1];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) z += __shfl_xor_sync(kFull, z, o);
+    z += w[oB3];
+    const float sg = 1.0f / (1.0f + expf(-z));
+    const float th = lo + (hi - lo) * sg;
+    const float e = th - y[s];
+    const float wgt = e > 0.f ? 1.0f + over : 1.0f;
+    const float gz = e * wgt * (hi - lo) * sg * (1.0f - sg) / (float)S;  // d(mean loss)/dz
+    float d2[2];
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const int j = lane + 32 * u;
+      d2[u] = gz * w[oW3 + j] * (1.0f - h2[u] * h2[u]);
+      sh[wi][1][j] = d2[u];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const int i = lane + 32 * u;
+      float a = 0.f;
+      for (int j = 0; j < kH; j++) a = fmaf(w[oW2 + j * kH + i], sh[wi][1][j], a);
+      const float d1 = a * (1.0f - h1[u] * h1[u]);
+      H1[(size_t)s * kH + i] = h1[u];
+      D1[(size_t)s * kH + i] = d1;
+      H2[(size_t)s * kH + i] = h2[u];
+      D2[(size_t)s * kH + i] = d2[u];
+    }
+    if (lane == 0) {
+      G[s] = gz;
+      loss[s] = 0.5f * e * e * wgt;
+      pred[s] = th;
+    }
+    __syncwarp();
+  }
+}
+
+// grad[t] for t in [0, kMlpWeights): fixed-order sums over the samples
+__global__ void __launch_bounds__(256) k_mlp_grad(const float* __restrict__ X, int S, const float* __restrict__ H1,
+                                                  const float* __restrict__ D1, const float* __restrict__ H2,
+                                                  const float* __restrict__ D2, const float* __restrict__ G,
+                                                  float* __restrict__ grad) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= kMlpWeights) return;
+  float acc = 0.f;
+  if (t < oB1) {  // W1[j][k] = sum d1[j] x[k]
+    const int j = t / kF, k = t % kF;
+    for (int s = 0; s < S; s++) acc = fmaf(D1[(size_t)s * kH + j], X[(size_t)s * kF + k], acc);
+  } else if (t < oW2) {
+    const int j = t - oB1;
+    for (int s = 0; s < S; s++) acc += D1[(size_t)s * kH + j];
+  } else if (t < oB2) {  // W2[j][i] = sum d2[j] h1[i]
+    const int j = (t - oW2) / kH, i = (t - oW2) % kH;
+    for (int s = 0; s < S; s++) acc = fmaf(D2[(size_t)s * kH + j], H1[(size_t)s * kH + i], acc);
+  } else if (t < oW3) {
+    const int j = t - oB2;
+    for (int s = 0; s < S; s++) acc += D2[(size_t)s * kH + j];
+  } else if (t < oB3) {  // w3[j] = sum g h2[j]
+    const int j = t - oW3;
+    for (int s = 0; s < S; s++) acc = fmaf(G[s], H2[(size_t)s * kH + j], acc);
+  } else {
+    for (int s = 0; s < S; s++) acc += G[s];
+  }
+  grad[t] = acc;
+}
+
+__global__ void k_adam(float* __restrict__ w, const float* __restrict__ grad, float* __restrict__ m,
+                       float* __restrict__ v, float lr, float b1, float b2, float c1, float c2) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= kMlpWeights) return;
+  const float g = grad[t];
+  const float mt = b1 * m[t] + (1.f - b1) * g;
+  const float vt = b2 * v[t] + (1.f - b2) * g * g;
+  m[t] = mt;
+  v[t] = vt;
+  w[t] -= lr * (mt / c1) / (sqrtf(vt / c2) + 1e-8f);
+}
+
+__global__ void k_sum_f(const float* __restrict__ a, int S, double* __restrict__ out) {
+  // one block: fixed-order partials, then lane 0 folds them
+  __shared__ double sh[256];
+  double s = 0;
+  for (int i = threadIdx.x; i < S; i += blockDim.x) s += a[i];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int i = 0; i < (int)blockDim.x; i++) t += sh[i];
+    *out = t;
+  }
+}
+
+// scratch for training: H1, D1, H2, D2 (S x kH each), G, loss, pred (S each)
+size_t mlp_train_scratch_floats(int S) { return (size_t)S * (4 * kH + 3); }
+
+void mlp_loss_grad(const float* X, const float* y, int S, const float* w, float lo, float hi, float over,
+                   float* scratch, float* grad, double* loss_out, cudaStream_t st) {
+  float* H1 = scratch;
+  float* D1 = H1 + (size_t)S * kH;
+  float* H2 = D1 + (size_t)S * kH;
+  float* D2 = H2 + (size_t)S * kH;
+  float* G = D2 + (size_t)S * kH;
+  float* L = G + S;
+  float* P = L + S;
+  const int blocks = (S + 7) / 8 < 4096 ? (S + 7) / 8 : 4096;
+  k_mlp_fwd_bwd<<<blocks, 256, 0, st>>>(X, y, S, w, lo, hi, over, H1, D1, H2, D2, G, L, P);
+  k_mlp_grad<<<(kMlpWeights + 255) / 256, 256, 0, st>>>(X, S, H1, D1, H2, D2, G, grad);
+  if (loss_out) k_sum_f<<<1, 256, 0, st>>>(L, S, loss_out);
+}
+
+void mlp_adam_step(float* w, const float* grad, float* m, float* v, float lr, int step, cudaStream_t st) {
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
+  k_adam<<<(kMlpWeights + 255) / 256, 256, 0, st>>>(w, grad, m, v, lr, b1, b2, c1, c2);
+}
+
+void mlp_predict(const float* X, int S, const float* w, float lo, float hi, float* scratch, float* pred,
+                 cudaStream_t st) {
+  // reuse the training forward with zero targets; pred is the last scratch row
+  float* H1 = scratch;
+  float* D1 = H1 + (size_t)S * kH;
+  float* H2 = D1 + (size_t)S * kH;
+  float* D2 = H2 + (size_t)S * kH;
+  float* G = D2 + (size_t)S * kH;
+  float* L = G + S;
+  const int blocks = (S + 7) / 8 < 4096 ? (S + 7) / 8 : 4096;
+  k_mlp_fwd_bwd<<<blocks, 256, 0, st>>>(X, pred, S, w, lo, hi, 0.f, H1, D1, H2, D2, G, L, pred);
+}
+
+void launch_group_features(const int2* groups, const TreeInfo* info, const float4* ipos,
+                           const unsigned long long* ph_sorted, const MpRec* rec, const Box* box, int n, int ncrit,
+                           float eps, float* feat, int nblocks, cudaStream_t st) {
+  k_group_features<<<nblocks, 256, 0, st>>>(groups, info, ipos, ph_sorted, rec, box, n, ncrit, eps, feat);
+}
+
+void launch_mlp_infer(const float* feat, const void* wh, const TreeInfo* info, float lo, float hi, float* inv,
+                      int nblocks, cudaStream_t st) {
+  k_mlp_infer<<<nblocks, 256, 0, st>>>(feat, static_cast<const __half*>(wh), info, lo, hi, inv);
+}
+
+void launch_weights_to_half(const float* w, void* wh, cudaStream_t st) {
+  k_weights_to_half<<<(kMlpWeights + 255) / 256, 256, 0, st>>>(w, static_cast<__half*>(wh));
+}
+
+void launch_fill_inv_theta(const TreeInfo* info, const float* theta, float c, float* inv, int nblocks,
+                           cudaStream_t st) {
+  k_fill_inv_theta<<<nblocks, 256, 0, st>>>(info, theta, c, inv);
+}
+
+}  // namespace bonsai

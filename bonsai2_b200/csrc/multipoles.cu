@@ -12,8 +12,9 @@
 //   M, COM; Q = second moment about the COM per unit mass (:148-158);
 //   particle bounding box -> l = max(2 max h, 1e-6), s = |cvec - COM|,
 //   cellOp = l/theta + s, stored squared (:168-177).
-// Stored for the walk (mass-weighted, pre-scaled so the force kernel needs
-// fewer operations):  cell_q0 = (M, 3Ixx, 3Iyy, 3Izz),
+// cell_ls = (l, s) lets a walk with per-group opening angles form
+// (l/theta_g + s)^2.  Stored for the walk (mass-weighted, pre-scaled so the
+// force kernel needs fewer operations):  cell_q0 = (M, 3Ixx, 3Iyy, 3Izz),
 // cell_q1 = (3Ixy, 3Ixz, 3Iyz, 1.5 tr I), with I = M Q.
 #include "common.cuh"
 #include "kernels.cuh"
@@ -22,7 +23,7 @@ namespace bonsai {
 
 __device__ __forceinline__ void store_cell(int c, const MpRec& r, float inv_theta, MpRec* __restrict__ rec,
                                            float4* __restrict__ cell_open, float4* __restrict__ cell_q0,
-                                           float4* __restrict__ cell_q1) {
+                                           float4* __restrict__ cell_q1, float2* __restrict__ cell_ls) {
   rec[c] = r;
   const float cx = (float)r.cx, cy = (float)r.cy, cz = (float)r.cz;
   const float vx = __fmul_rn(__fadd_rn(r.bmax[0], r.bmin[0]), 0.5f);
@@ -36,6 +37,7 @@ __device__ __forceinline__ void store_cell(int c, const MpRec& r, float inv_thet
   const float l = fmaxf(__fmul_rn(2.0f, fmaxf(hx, fmaxf(hy, hz))), 1.0e-6f);
   const float op = __fmaf_rn(l, inv_theta, s);
   cell_open[c] = make_float4(cx, cy, cz, __fmul_rn(op, op));
+  cell_ls[c] = make_float2(l, s);  // per-group opening angles recompute (l/theta_g + s)^2
   const double tr = r.ixx + r.iyy + r.izz;
   cell_q0[c] = make_float4((float)r.m, (float)(3.0 * r.ixx), (float)(3.0 * r.iyy), (float)(3.0 * r.izz));
   cell_q1[c] = make_float4((float)(3.0 * r.ixy), (float)(3.0 * r.ixz), (float)(3.0 * r.iyz), (float)(1.5 * tr));
@@ -47,7 +49,8 @@ __global__ void __launch_bounds__(256) k_multipoles(const int* __restrict__ leaf
                                                     const float4* __restrict__ jpos, float inv_theta,
                                                     MpRec* __restrict__ rec, float4* __restrict__ cell_open,
                                                     float4* __restrict__ cell_q0, float4* __restrict__ cell_q1,
-                                                    int* __restrict__ mp_count, int cell_cap) {
+                                                    float2* __restrict__ cell_ls, int* __restrict__ mp_count,
+                                                    int cell_cap) {
   const int nleaves = info->nleaves;
   if (info->ncells > cell_cap) return;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nleaves; t += gridDim.x * blockDim.x) {
@@ -76,7 +79,7 @@ __global__ void __launch_bounds__(256) k_multipoles(const int* __restrict__ leaf
     r.m = m;
     r.ixx = q[0]; r.iyy = q[1]; r.izz = q[2]; r.ixy = q[3]; r.ixz = q[4]; r.iyz = q[5];
     for (int k = 0; k < 3; k++) { r.bmin[k] = mn[k]; r.bmax[k] = mx[k]; }
-    store_cell(c, r, inv_theta, rec, cell_open, cell_q0, cell_q1);
+    store_cell(c, r, inv_theta, rec, cell_open, cell_q0, cell_q1, cell_ls);
     // climb while this thread is the last child to arrive
     while (true) {
       const int p = cell_parent[c];
@@ -117,7 +120,7 @@ __global__ void __launch_bounds__(256) k_multipoles(const int* __restrict__ leaf
       P.m = M;
       P.ixx = I[0]; P.iyy = I[1]; P.izz = I[2]; P.ixy = I[3]; P.ixz = I[4]; P.iyz = I[5];
       for (int a = 0; a < 3; a++) { P.bmin[a] = bmn[a]; P.bmax[a] = bmx[a]; }
-      store_cell(p, P, inv_theta, rec, cell_open, cell_q0, cell_q1);
+      store_cell(p, P, inv_theta, rec, cell_open, cell_q0, cell_q1, cell_ls);
       c = p;
     }
   }

@@ -4,10 +4,10 @@
 // The reference sorts with Thrust (sort_by_key / stable_sort_by_key,
 // makeGroups.cu:270-277, buildTree.cu:940-944): a stable radix sort, ties in
 // input order.  This is a hand-written replacement with the same semantics:
-// 8 passes of 8 bits; per pass an upsweep (per-tile digit counts), one
-// exclusive scan over the digit-major count matrix, and a downsweep that
-// ranks every key stably inside its 4096-key tile (warp match_any + per-warp
-// digit counters in shared memory) and scatters it.
+// 8 passes of 8 bits, one-sweep (below): keys are ranked stably inside each
+// 4096-key tile with warp match_any and per-warp digit counters in shared
+// memory, tile offsets come from a decoupled look-back, and tiles are written
+// out through shared memory in contiguous digit runs.
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -19,82 +19,6 @@ constexpr int kSortTile = kSortThreads * kSortItems;  // 4096
 constexpr int kScanChunk = 4096;
 
 int sort_tiles(int n) { return (n + kSortTile - 1) / kSortTile; }
-
-// digit-major count matrix: counts[d * ntiles + tile]
-__global__ void __launch_bounds__(kSortThreads) k_sort_upsweep(const unsigned long long* __restrict__ keys, int n,
-                                                               int shift, unsigned* __restrict__ counts,
-                                                               int ntiles) {
-  __shared__ unsigned h[256];
-  h[threadIdx.x] = 0;
-  __syncthreads();
-  const int base = blockIdx.x * kSortTile;
-#pragma unroll
-  for (int k = 0; k < kSortItems; k++) {
-    const int i = base + k * kSortThreads + threadIdx.x;
-    if (i < n) {
-      const unsigned d = (unsigned)(keys[i] >> shift) & 255u;
-      // aggregate equal digits within the warp before the shared atomic
-      const unsigned peers = __match_any_sync(__activemask(), d);
-      if ((peers & lanemask_lt()) == 0) atomicAdd(&h[d], (unsigned)__popc(peers));
-    }
-  }
-  __syncthreads();
-  counts[threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
-}
-
-__global__ void __launch_bounds__(kSortThreads) k_sort_downsweep(const unsigned long long* __restrict__ keys_in,
-                                                                 const int* __restrict__ vals_in, int n, int shift,
-                                                                 const unsigned* __restrict__ offsets, int ntiles,
-                                                                 unsigned long long* __restrict__ keys_out,
-                                                                 int* __restrict__ vals_out) {
-  __shared__ unsigned wcnt[kSortThreads / 32][256];
-  __shared__ unsigned gofs[256];
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int t = threadIdx.x; t < (kSortThreads / 32) * 256; t += kSortThreads) (&wcnt[0][0])[t] = 0;
-  gofs[threadIdx.x] = offsets[threadIdx.x * ntiles + blockIdx.x];
-  __syncthreads();
-  // warp-striped ownership: item k of warp w is tile index w*512 + k*32 + lane
-  const int base = blockIdx.x * kSortTile + w * (32 * kSortItems);
-  unsigned long long key[kSortItems];
-  int val[kSortItems];
-  unsigned rank[kSortItems];
-#pragma unroll
-  for (int k = 0; k < kSortItems; k++) {
-    const int i = base + k * 32 + lane;
-    const bool ok = i < n;
-    key[k] = ok ? keys_in[i] : 0ull;
-    val[k] = ok ? (vals_in ? vals_in[i] : i) : 0;
-    const unsigned d = ok ? ((unsigned)(key[k] >> shift) & 255u) : 256u;
-    const unsigned peers = __match_any_sync(kFull, d);
-    const unsigned before = (unsigned)__popc(peers & lanemask_lt());
-    const unsigned cur = ok ? wcnt[w][d] : 0u;
-    rank[k] = cur + before;
-    __syncwarp();
-    if (ok && before == 0) wcnt[w][d] = cur + (unsigned)__popc(peers);
-    __syncwarp();
-  }
-  __syncthreads();
-  {  // exclusive prefix over warps for digit threadIdx.x
-    unsigned run = 0;
-#pragma unroll
-    for (int ww = 0; ww < kSortThreads / 32; ww++) {
-      const unsigned c = wcnt[ww][threadIdx.x];
-      wcnt[ww][threadIdx.x] = run;
-      run += c;
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int k = 0; k < kSortItems; k++) {
-    const int i = base + k * 32 + lane;
-    if (i < n) {
-      const unsigned d = (unsigned)(key[k] >> shift) & 255u;
-      const unsigned o = gofs[d] + wcnt[w][d] + rank[k];
-      keys_out[o] = key[k];
-      vals_out[o] = val[k];
-    }
-  }
-}
 
 // ---------------------------------------------------------------------------
 // exclusive scan of unsigned ints (length m known on the host)
@@ -184,22 +108,179 @@ void exclusive_scan(const unsigned* in, unsigned* out, int m, unsigned* bsum, un
   k_scan_down<<<nb, 256, 0, s>>>(in, m, bsum, out);
 }
 
+// ---------------------------------------------------------------------------
+// One-sweep passes.  One kernel reads the keys once and builds the digit
+// histograms of all eight passes; one kernel per pass then ranks each
+// 4096-key tile (same stable warp ranking as above), obtains the tile's
+// global offset per digit by decoupled look-back over the preceding tiles
+// (tiles take ids in launch order from an atomic counter, so a tile only waits
+// for tiles that already run; every wait is bounded and sets an error flag
+// when the bound is hit), stages the tile in shared memory in digit order and
+// writes it out in contiguous runs.  One read and one write of the pairs per
+// pass.
+// ---------------------------------------------------------------------------
+constexpr unsigned kFlagAgg = 1u << 30, kFlagInc = 2u << 30, kValMask = (1u << 30) - 1u;
+constexpr int kLookbackSpin = 1 << 22;
+
+__global__ void __launch_bounds__(kSortThreads) k_sort_hist8(const unsigned long long* __restrict__ keys, int n,
+                                                             int passes, unsigned* __restrict__ ghist) {
+  __shared__ unsigned h[8][256];
+  for (int t = threadIdx.x; t < 8 * 256; t += kSortThreads) (&h[0][0])[t] = 0;
+  __syncthreads();
+  for (int i = blockIdx.x * kSortThreads + threadIdx.x; i < n; i += gridDim.x * kSortThreads) {
+    const unsigned long long k = keys[i];
+#pragma unroll
+    for (int p = 0; p < 8; p++)
+      if (p < passes) atomicAdd(&h[p][(unsigned)(k >> (8 * p)) & 255u], 1u);
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < passes * 256; t += kSortThreads) {
+    const unsigned v = (&h[0][0])[t];
+    if (v) atomicAdd(ghist + t, v);
+  }
+}
+
+// exclusive scan of each 256-entry row in place (one block, 256 threads)
+__global__ void __launch_bounds__(256) k_sort_hist_scan(unsigned* __restrict__ ghist, int passes) {
+  __shared__ unsigned sh[32];
+  for (int p = 0; p < passes; p++) {
+    const unsigned v = ghist[p * 256 + threadIdx.x];
+    const unsigned e = block_excl_scan(v, sh, nullptr);
+    ghist[p * 256 + threadIdx.x] = e;
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kSortThreads) k_sort_onesweep(
+    const unsigned long long* __restrict__ keys_in, const int* __restrict__ vals_in, int n, int shift,
+    const unsigned* __restrict__ gbase, unsigned* __restrict__ status, unsigned* __restrict__ tile_counter,
+    unsigned long long* __restrict__ keys_out, int* __restrict__ vals_out, int* __restrict__ err) {
+  __shared__ unsigned wcnt[kSortThreads / 32][256];
+  __shared__ unsigned tile_off[256];
+  __shared__ unsigned dstart[256];
+  __shared__ unsigned long long stage[kSortTile];  // keys, then values (as 32-bit) in digit order
+  __shared__ unsigned sh[32];
+  __shared__ int tile_sh;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) tile_sh = (int)atomicAdd(tile_counter, 1u);
+  for (int t = threadIdx.x; t < (kSortThreads / 32) * 256; t += kSortThreads) (&wcnt[0][0])[t] = 0;
+  __syncthreads();
+  const int tile = tile_sh;
+  const int base = tile * kSortTile + w * (32 * kSortItems);
+  unsigned long long key[kSortItems];
+  unsigned rank[kSortItems];
+#pragma unroll
+  for (int k = 0; k < kSortItems; k++) {
+    const int i = base + k * 32 + lane;
+    const bool ok = i < n;
+    key[k] = ok ? keys_in[i] : 0ull;
+    const unsigned d = ok ? ((unsigned)(key[k] >> shift) & 255u) : 256u;
+    const unsigned peers = __match_any_sync(kFull, d);
+    const unsigned before = (unsigned)__popc(peers & lanemask_lt());
+    const unsigned cur = ok ? wcnt[w][d] : 0u;
+    rank[k] = cur + before;
+    __syncwarp();
+    if (ok && before == 0) wcnt[w][d] = cur + (unsigned)__popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+  // per digit: prefix over warps, tile total, tile-local digit offsets
+  const unsigned d = threadIdx.x;
+  unsigned tot = 0;
+#pragma unroll
+  for (int ww = 0; ww < kSortThreads / 32; ww++) {
+    const unsigned c = wcnt[ww][d];
+    wcnt[ww][d] = tot;
+    tot += c;
+  }
+  tile_off[d] = block_excl_scan(tot, sh, nullptr);
+  // decoupled look-back for the digit's global offset
+  volatile unsigned* st = status;
+  if (tile == 0) {
+    st[d] = kFlagInc | tot;
+    dstart[d] = gbase[d];
+  } else {
+    st[(size_t)tile * 256 + d] = kFlagAgg | tot;
+    unsigned excl = 0;
+    for (int t = tile - 1; t >= 0; t--) {
+      unsigned v = st[(size_t)t * 256 + d];
+      int spin = 0;
+      while ((v & ~kValMask) == 0u && spin < kLookbackSpin) {
+        __nanosleep(32);
+        v = st[(size_t)t * 256 + d];
+        spin++;
+      }
+      if ((v & ~kValMask) == 0u) {  // bound hit: report and give up (results invalid)
+        atomicOr(err, kStatusSortTimeout);
+        break;
+      }
+      excl += v & kValMask;
+      if ((v & ~kValMask) == kFlagInc) break;
+    }
+    st[(size_t)tile * 256 + d] = kFlagInc | (excl + tot);
+    dstart[d] = gbase[d] + excl;
+  }
+  __syncthreads();
+  // stage keys in digit order, write contiguous runs
+  const int tile_n = min(kSortTile, n - tile * kSortTile);
+  unsigned lpos[kSortItems];
+#pragma unroll
+  for (int k = 0; k < kSortItems; k++) {
+    const int i = base + k * 32 + lane;
+    if (i < n) {
+      const unsigned dd = (unsigned)(key[k] >> shift) & 255u;
+      lpos[k] = tile_off[dd] + wcnt[w][dd] + rank[k];
+      stage[lpos[k]] = key[k];
+    }
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < tile_n; j += kSortThreads) {
+    const unsigned long long kk = stage[j];
+    const unsigned dd = (unsigned)(kk >> shift) & 255u;
+    keys_out[dstart[dd] + (unsigned)j - tile_off[dd]] = kk;
+  }
+  __syncthreads();
+  unsigned* stage32 = reinterpret_cast<unsigned*>(stage);
+  unsigned char* digit_of = reinterpret_cast<unsigned char*>(stage32 + kSortTile);
+#pragma unroll
+  for (int k = 0; k < kSortItems; k++) {
+    const int i = base + k * 32 + lane;
+    if (i < n) {
+      stage32[lpos[k]] = (unsigned)(vals_in ? vals_in[i] : i);
+      digit_of[lpos[k]] = (unsigned char)((unsigned)(key[k] >> shift) & 255u);
+    }
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < tile_n; j += kSortThreads) {
+    const unsigned dd = digit_of[j];
+    vals_out[dstart[dd] + (unsigned)j - tile_off[dd]] = (int)stage32[j];
+  }
+}
+
+size_t sort_status_words(int n) { return (size_t)sort_tiles(n) * 256 * 8 + 8 + 8 * 256; }
+
 // Stable sort of n (key, value) pairs; values_in == nullptr means 0..n-1.
-// Result ends in (keys_a, vals_a) after the 8 passes (even pass count).
+// Result ends in (keys_a, vals_a) after an even number of passes.  work holds
+// sort_status_words(n) unsigned ints: look-back status of every pass, the
+// tile counters and the 8 digit histograms; kStatusSortTimeout is or-ed into
+// *err if a look-back wait hit its bound.
 void radix_sort_pairs(unsigned long long* keys_a, unsigned long long* keys_b, int* vals_a, int* vals_b,
-                      const int* vals_in, int n, unsigned* counts, unsigned* bsum, int passes, cudaStream_t s) {
+                      const int* vals_in, int n, unsigned* work, int* err, int passes, cudaStream_t s) {
   if (n <= 0) return;
   const int nt = sort_tiles(n);
-  const int m = 256 * nt;
+  unsigned* status = work;
+  unsigned* counters = work + (size_t)nt * 256 * 8;
+  unsigned* ghist = counters + 8;
+  cudaMemsetAsync(work, 0, sort_status_words(n) * sizeof(unsigned), s);
+  k_sort_hist8<<<1184, kSortThreads, 0, s>>>(keys_a, n, passes, ghist);
+  k_sort_hist_scan<<<1, 256, 0, s>>>(ghist, passes);
   unsigned long long* kin = keys_a;
   unsigned long long* kout = keys_b;
   int* vin = vals_a;
   int* vout = vals_b;
   for (int p = 0; p < passes; p++) {
-    const int shift = 8 * p;
-    k_sort_upsweep<<<nt, kSortThreads, 0, s>>>(kin, n, shift, counts, nt);
-    exclusive_scan(counts, counts, m, bsum, nullptr, s);
-    k_sort_downsweep<<<nt, kSortThreads, 0, s>>>(kin, p == 0 ? vals_in : vin, n, shift, counts, nt, kout, vout);
+    k_sort_onesweep<<<nt, kSortThreads, 0, s>>>(kin, p == 0 ? vals_in : vin, n, 8 * p, ghist + 256 * p,
+                                                status + (size_t)p * nt * 256, counters + p, kout, vout, err);
     unsigned long long* tk = kin; kin = kout; kout = tk;
     int* tv = vin; vin = vout; vout = tv;
   }

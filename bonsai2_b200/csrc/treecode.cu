@@ -64,6 +64,16 @@ struct Handle {
   float4 *cell_open = nullptr, *cell_q0 = nullptr, *cell_q1 = nullptr;
   int *cell_parent = nullptr, *leaf_list = nullptr, *mp_count = nullptr;
   MpRec* rec = nullptr;
+  float2* cell_ls = nullptr;
+  // per-group opening angles (theta mode 1: MLP, 2: caller's array)
+  int theta_mode = 0;
+  float theta_lo = 0.25f, theta_hi = 1.25f;
+  int gcap = 0;
+  float* group_inv = nullptr;
+  float* group_feat = nullptr;
+  float* mlp_w = nullptr;
+  void* mlp_wh = nullptr;
+  bool mlp_loaded = false;
   int2* groups = nullptr;
   unsigned *g_count = nullptr, *g_seg = nullptr, *g_ng = nullptr;
   int* ring = nullptr;
@@ -104,13 +114,13 @@ struct Handle {
     for (int p = 0; p < 2; p++) { dfree(&pos[p]); dfree(&vel[p]); dfree(&id[p]); }
     dfree(&acc); dfree(&jpos); dfree(&tkey); dfree(&pkey); dfree(&kalt);
     dfree(&tperm); dfree(&pperm); dfree(&valt); dfree(&sort_counts); dfree(&bsum);
-    dfree(&dlev); dfree(&chain); dfree(&hist); dfree(&groups);
+    dfree(&dlev); dfree(&chain); dfree(&hist); dfree(&groups); dfree(&group_inv); dfree(&group_feat);
     release_cells();
     n = 0;
   }
   void release_cells() {
     dfree(&cell_data); dfree(&cell_open); dfree(&cell_q0); dfree(&cell_q1);
-    dfree(&cell_parent); dfree(&leaf_list); dfree(&mp_count); dfree(&rec);
+    dfree(&cell_parent); dfree(&leaf_list); dfree(&mp_count); dfree(&rec); dfree(&cell_ls);
     cap_cells = 0;
   }
   void release() {
@@ -120,6 +130,8 @@ struct Handle {
     dfree(&group_counter); dfree(&stats); dfree(&move_partial); dfree(&energies);
     dfree(&move_ticket); dfree(&box_ticket); dfree(&closing); dfree(&box); dfree(&box_partial);
     dfree(&ph_table); dfree(&direct_part); dfree(&direct_out); dfree(&direct_sample);
+    dfree(&mlp_w);
+    if (mlp_wh) { cudaFree(mlp_wh); mlp_wh = nullptr; }
     if (st) { cudaStreamDestroy(st); st = nullptr; }
   }
 
@@ -136,6 +148,7 @@ struct Handle {
     BONSAI_CUDA_TRY(dalloc(&leaf_list, C));
     BONSAI_CUDA_TRY(dalloc(&mp_count, C));
     BONSAI_CUDA_TRY(dalloc(&rec, C));
+    BONSAI_CUDA_TRY(dalloc(&cell_ls, C));
     return 0;
   }
 
@@ -199,13 +212,18 @@ struct Handle {
     BONSAI_CUDA_TRY(dalloc(&tperm, N));
     BONSAI_CUDA_TRY(dalloc(&pperm, N));
     BONSAI_CUDA_TRY(dalloc(&valt, N));
-    BONSAI_CUDA_TRY(dalloc(&sort_counts, (size_t)256 * sort_tiles(nn)));
+    BONSAI_CUDA_TRY(dalloc(&sort_counts, sort_status_words(nn)));
     const int scan_m = std::max(256 * sort_tiles(nn), 1 << (3 * kMaxLevelSplit));
     BONSAI_CUDA_TRY(dalloc(&bsum, (size_t)scan_blocks(scan_m) + 1));
     BONSAI_CUDA_TRY(dalloc(&dlev, N));
     BONSAI_CUDA_TRY(dalloc(&chain, N));
     BONSAI_CUDA_TRY(dalloc(&hist, (size_t)2 * (kMaxLevel + 1) * tree_tiles(nn)));
     BONSAI_CUDA_TRY(dalloc(&groups, N));
+    // group-indexed arrays of the per-group angle: at most N/nCrit groups plus
+    // one partial group per PH segment (groups.cu)
+    gcap = (int)std::min<long long>(N, (long long)N / std::max(1, prm.ncrit) + (1ll << (3 * kMaxLevelSplit)) + 1);
+    BONSAI_CUDA_TRY(dalloc(&group_inv, (size_t)gcap));
+    BONSAI_CUDA_TRY(dalloc(&group_feat, (size_t)gcap * kMlpFeatures));
     // the reference reserves nPtcl cells (Treecode.h:192); a Plummer tree at
     // nLeaf 16 uses ~0.23 N.  Grown on demand by the eager build.
     int rc = alloc_cells(prm.nleaf >= 8 ? nn / 2 + 4096 : 2 * nn + 4096);
@@ -236,18 +254,18 @@ struct Handle {
     cudaMemsetAsync(box_ticket, 0, sizeof(unsigned), st);
     k_box<<<box_blocks, 256, 0, st>>>(pos[par], n, box_partial, box_ticket, box, &info->status);
     k_keys<<<nsm * 8, 256, 0, st>>>(pos[par], n, box, ph_table, tkey, pkey);
-    radix_sort_pairs(tkey, kalt, tperm, valt, nullptr, n, sort_counts, bsum, 8, st);
+    radix_sort_pairs(tkey, kalt, tperm, valt, nullptr, n, sort_counts, &info->status, 8, st);
     k_gather_pos<<<nsm * 8, 256, 0, st>>>(tperm, n, pos[par], jpos);
     build_tree(tkey, n, nleaf, cap_cells, cap_cells, dlev, chain, hist, info, cell_data, cell_parent, leaf_list,
                mp_count, st);
   }
   void enq_multipoles() {
     k_multipoles<<<nsm * 8, 256, 0, st>>>(leaf_list, info, cell_data, cell_parent, jpos, 1.0f / prm.theta, rec,
-                                          cell_open, cell_q0, cell_q1, mp_count, cap_cells);
+                                          cell_open, cell_q0, cell_q1, cell_ls, mp_count, cap_cells);
   }
   void enq_groups(int ls, int ncrit) {
-    radix_sort_pairs(pkey, kalt, pperm, valt, nullptr, n, sort_counts, bsum, 8, st);
-    make_groups(pkey, n, ls, ncrit, g_count, g_seg, g_ng, bsum, groups, n, info, st);
+    radix_sort_pairs(pkey, kalt, pperm, valt, nullptr, n, sort_counts, &info->status, 8, st);
+    make_groups(pkey, n, ls, ncrit, g_count, g_seg, g_ng, bsum, groups, theta_mode ? gcap : n, info, st);
     const int q = par ^ 1;
     k_gather_state<<<nsm * 8, 256, 0, st>>>(pperm, n, pos[par], vel[par], id[par], pos[q], vel[q], id[q]);
     par = q;
@@ -256,8 +274,16 @@ struct Handle {
     const int k = walk_variant(ncrit);
     cudaMemsetAsync(group_counter, 0, sizeof(unsigned), st);
     cudaMemsetAsync(stats, 0, 4 * sizeof(unsigned long long), st);
-    launch_walk(k, walk_blocks[k], groups, info, pos[par], jpos, cell_data, cell_open, cell_q0, cell_q1,
-                prm.eps * prm.eps, acc, ring, kRingCap, group_counter, stats, &info->status, st);
+    const float* ginv = nullptr;
+    if (theta_mode == 1) {
+      launch_group_features(groups, info, pos[par], pkey, rec, box, n, ncrit, prm.eps, group_feat, nsm * 8, st);
+      launch_mlp_infer(group_feat, mlp_wh, info, theta_lo, theta_hi, group_inv, nsm * 4, st);
+      ginv = group_inv;
+    } else if (theta_mode == 2) {
+      ginv = group_inv;
+    }
+    launch_walk(k, walk_blocks[k], groups, info, pos[par], jpos, cell_data, cell_open, cell_q0, cell_q1, cell_ls,
+                ginv, prm.eps * prm.eps, acc, ring, kRingCap, group_counter, stats, &info->status, st);
   }
   void enq_move(bool write) {
     launch_move_wrapper(write);
@@ -674,6 +700,7 @@ const char* bonsai_error_string(int code) {
     if (code & BONSAI_STATUS_GROUP_CAPACITY) return "group capacity exceeded";
     if (code & BONSAI_STATUS_DEPTH) return "tree deeper than 21 levels (fat leaf kept)";
     if (code & BONSAI_STATUS_BAD_PARAM) return "bad parameter";
+    if (code & BONSAI_STATUS_SORT_TIMEOUT) return "radix sort look-back wait timed out";
   }
   return "unknown";
 }
@@ -809,6 +836,159 @@ int bonsai_direct_fp64(bonsai_handle hh, const int* sample, int ns, int include_
   launch_direct_fp64(tmp, h->n, h->direct_sample, ns, e2, include_self, h->direct_part, nsplit, h->direct_out, h->st);
   BONSAI_CUDA_TRY(cudaMemcpyAsync(out, h->direct_out, (size_t)ns * 4 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
   BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  return last_cuda();
+}
+
+int bonsai_set_theta_mode(bonsai_handle hh, int mode, float lo, float hi) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (mode < 0 || mode > 2 || !(lo > 0.f) || !(hi >= lo)) return BONSAI_ERR_ARG;
+  if (mode == 1 && !h->mlp_loaded) return BONSAI_ERR_ORDER;
+  h->theta_mode = mode;
+  h->theta_lo = lo;
+  h->theta_hi = hi;
+  h->release_graphs();
+  return 0;
+}
+
+int bonsai_set_mlp_weights(bonsai_handle hh, const float* w, int nw) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (!w || nw != kMlpWeights) return BONSAI_ERR_ARG;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  if (!h->mlp_w) BONSAI_CUDA_TRY(dalloc(&h->mlp_w, (size_t)kMlpWeights));
+  if (!h->mlp_wh) BONSAI_CUDA_TRY(cudaMalloc(&h->mlp_wh, (size_t)kMlpWeights * 2));
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(h->mlp_w, w, (size_t)kMlpWeights * 4, cudaMemcpyHostToDevice, h->st));
+  launch_weights_to_half(h->mlp_w, h->mlp_wh, h->st);
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  h->mlp_loaded = true;
+  return last_cuda();
+}
+
+int bonsai_set_group_theta(bonsai_handle hh, const float* theta, int ngroups) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (!h->grouped && !h->forced) return BONSAI_ERR_ORDER;
+  if (!theta || ngroups < 1 || ngroups > h->gcap) return BONSAI_ERR_ARG;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  int ng = 0;
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(&ng, &h->info->ngroups, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  if (ng != ngroups) return BONSAI_ERR_ARG;
+  float* tmp = reinterpret_cast<float*>(h->group_feat);  // staging: the feature buffer holds >= G floats
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(tmp, theta, (size_t)ng * 4, cudaMemcpyHostToDevice, h->st));
+  launch_fill_inv_theta(h->info, tmp, 0.f, h->group_inv, h->nsm * 4, h->st);
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  return last_cuda();
+}
+
+int bonsai_get_group_features(bonsai_handle hh, float* out, int* ngroups) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (!h->grouped) return BONSAI_ERR_ORDER;
+  if (!out || !ngroups) return BONSAI_ERR_ARG;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  int ng = 0;
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(&ng, &h->info->ngroups, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  if (ng > h->gcap) return BONSAI_STATUS_GROUP_CAPACITY;
+  launch_group_features(h->groups, h->info, h->pos[h->par], h->pkey, h->rec, h->box, h->n, h->cur_ncrit, h->prm.eps,
+                        h->group_feat, h->nsm * 8, h->st);
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(out, h->group_feat, (size_t)ng * kMlpFeatures * 4, cudaMemcpyDeviceToHost, h->st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  *ngroups = ng;
+  return last_cuda();
+}
+
+int bonsai_get_group_theta(bonsai_handle hh, float* out) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (!out) return BONSAI_ERR_ARG;
+  if (h->theta_mode == 0) return BONSAI_ERR_ORDER;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  int ng = 0;
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(&ng, &h->info->ngroups, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(out, h->group_inv, (size_t)ng * 4, cudaMemcpyDeviceToHost, h->st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  for (int g = 0; g < ng; g++) out[g] = 1.0f / out[g];
+  return 0;
+}
+
+// standalone MLP training helpers (host arrays in and out)
+struct MlpJob {
+  float *X = nullptr, *y = nullptr, *w = nullptr, *g = nullptr, *m = nullptr, *v = nullptr, *scr = nullptr,
+        *pred = nullptr;
+  double* loss = nullptr;
+  cudaStream_t st = nullptr;
+  ~MlpJob() {
+    dfree(&X); dfree(&y); dfree(&w); dfree(&g); dfree(&m); dfree(&v); dfree(&scr); dfree(&pred); dfree(&loss);
+    if (st) cudaStreamDestroy(st);
+  }
+  int init(int device, const float* hX, const float* hy, int S, const float* hw) {
+    BONSAI_CUDA_TRY(cudaSetDevice(device));
+    BONSAI_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    BONSAI_CUDA_TRY(dalloc(&X, (size_t)S * kMlpFeatures));
+    BONSAI_CUDA_TRY(dalloc(&y, (size_t)S));
+    BONSAI_CUDA_TRY(dalloc(&w, (size_t)kMlpWeights));
+    BONSAI_CUDA_TRY(dalloc(&g, (size_t)kMlpWeights));
+    BONSAI_CUDA_TRY(dalloc(&m, (size_t)kMlpWeights));
+    BONSAI_CUDA_TRY(dalloc(&v, (size_t)kMlpWeights));
+    BONSAI_CUDA_TRY(dalloc(&scr, mlp_train_scratch_floats(S)));
+    BONSAI_CUDA_TRY(dalloc(&pred, (size_t)S));
+    BONSAI_CUDA_TRY(dalloc(&loss, 1));
+    BONSAI_CUDA_TRY(cudaMemcpyAsync(X, hX, (size_t)S * kMlpFeatures * 4, cudaMemcpyHostToDevice, st));
+    if (hy) BONSAI_CUDA_TRY(cudaMemcpyAsync(y, hy, (size_t)S * 4, cudaMemcpyHostToDevice, st));
+    BONSAI_CUDA_TRY(cudaMemcpyAsync(w, hw, (size_t)kMlpWeights * 4, cudaMemcpyHostToDevice, st));
+    BONSAI_CUDA_TRY(cudaMemsetAsync(m, 0, (size_t)kMlpWeights * 4, st));
+    BONSAI_CUDA_TRY(cudaMemsetAsync(v, 0, (size_t)kMlpWeights * 4, st));
+    return 0;
+  }
+};
+
+int bonsai_mlp_loss_grad(int device, const float* X, const float* y, int S, const float* w, float lo, float hi,
+                         float over, float* grad, double* loss) {
+  if (!X || !y || !w || S < 1 || !(hi > lo)) return BONSAI_ERR_ARG;
+  MlpJob j;
+  int rc = j.init(device, X, y, S, w);
+  if (rc) return rc;
+  mlp_loss_grad(j.X, j.y, S, j.w, lo, hi, over, j.scr, j.g, j.loss, j.st);
+  if (grad) BONSAI_CUDA_TRY(cudaMemcpyAsync(grad, j.g, (size_t)kMlpWeights * 4, cudaMemcpyDeviceToHost, j.st));
+  double l = 0;
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(&l, j.loss, sizeof(double), cudaMemcpyDeviceToHost, j.st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(j.st));
+  if (loss) *loss = l / S;
+  return last_cuda();
+}
+
+int bonsai_mlp_train(int device, const float* X, const float* y, int S, float* w, int epochs, float lr, float lo,
+                     float hi, float over, double* loss) {
+  if (!X || !y || !w || S < 1 || epochs < 0 || !(hi > lo)) return BONSAI_ERR_ARG;
+  MlpJob j;
+  int rc = j.init(device, X, y, S, w);
+  if (rc) return rc;
+  for (int e = 1; e <= epochs; e++) {
+    mlp_loss_grad(j.X, j.y, S, j.w, lo, hi, over, j.scr, j.g, nullptr, j.st);
+    mlp_adam_step(j.w, j.g, j.m, j.v, lr, e, j.st);
+  }
+  mlp_loss_grad(j.X, j.y, S, j.w, lo, hi, over, j.scr, j.g, j.loss, j.st);
+  double l = 0;
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(w, j.w, (size_t)kMlpWeights * 4, cudaMemcpyDeviceToHost, j.st));
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(&l, j.loss, sizeof(double), cudaMemcpyDeviceToHost, j.st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(j.st));
+  if (loss) *loss = l / S;
+  return last_cuda();
+}
+
+int bonsai_mlp_predict(int device, const float* X, int S, const float* w, float lo, float hi, float* theta) {
+  if (!X || !w || !theta || S < 1 || !(hi > lo)) return BONSAI_ERR_ARG;
+  MlpJob j;
+  int rc = j.init(device, X, nullptr, S, w);
+  if (rc) return rc;
+  BONSAI_CUDA_TRY(cudaMemsetAsync(j.pred, 0, (size_t)S * 4, j.st));
+  mlp_predict(j.X, S, j.w, lo, hi, j.scr, j.pred, j.st);
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(theta, j.pred, (size_t)S * 4, cudaMemcpyDeviceToHost, j.st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(j.st));
   return last_cuda();
 }
 

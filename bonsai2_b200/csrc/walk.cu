@@ -118,14 +118,19 @@ __device__ __forceinline__ int find_src(int incl, int s) {
 // entries of every 32-entry batch and their sums are added once per group, so
 // each broadcast shared-memory load feeds NI (= 4 for nCrit <= 64)
 // interactions.  Otherwise lane l holds l + 32k, k < NI.
-template <int NI, bool SPLIT>
+// PERGROUP: each group has its own opening angle (1/theta_g in
+// group_inv_theta); the opening size is re-formed as (l/theta_g + s)^2 from
+// cell_ls with the same rounding as the multipole kernel, so theta_g = theta
+// reproduces the fixed-angle walk exactly.
+template <int NI, bool SPLIT, bool PERGROUP>
 __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
     k_walk(const int2* __restrict__ groups, const TreeInfo* __restrict__ info, const float4* __restrict__ ipos,
            const float4* __restrict__ jpos, const uint4* __restrict__ cell_data,
            const float4* __restrict__ cell_open, const float4* __restrict__ cell_q0,
-           const float4* __restrict__ cell_q1, float eps2, float4* __restrict__ acc, int* __restrict__ ring_pool,
-           int ring_cap, unsigned* __restrict__ group_counter, unsigned long long* __restrict__ stats,
-           int* __restrict__ status) {
+           const float4* __restrict__ cell_q1, const float2* __restrict__ cell_ls,
+           const float* __restrict__ group_inv_theta, float eps2, float4* __restrict__ acc,
+           int* __restrict__ ring_pool, int ring_cap, unsigned* __restrict__ group_counter,
+           unsigned long long* __restrict__ stats, int* __restrict__ status) {
   constexpr int STRIDE = SPLIT ? 16 : 32;
   constexpr int JSTEP = SPLIT ? 2 : 1;
   __shared__ float4 s_a0[kWalkWarps][64];
@@ -153,6 +158,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
     if (g >= ngroups) break;
     const int2 gd = groups[g];
     const int pbeg = gd.x, np = gd.y;
+    const float inv_theta_g = PERGROUP ? group_inv_theta[g] : 0.0f;
     IPart pi[NI];
     float4 ai[NI];
     float mnx = 3.0e38f, mny = 3.0e38f, mnz = 3.0e38f, mxx = -3.0e38f, mxy = -3.0e38f, mxz = -3.0e38f;
@@ -189,6 +195,11 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
         if (valid) {
           cd = __ldg(cell_data + cell);
           co = __ldg(cell_open + cell);
+          if (PERGROUP) {
+            const float2 ls = __ldg(cell_ls + cell);
+            const float op = __fmaf_rn(ls.x, inv_theta_g, ls.y);
+            co.w = __fmul_rn(op, op);
+          }
         }
         const bool leaf = cd.y == 0xFFFFFFFFu;
         const bool split = valid && (open_cell(co, gc, gs) || ((int)(cd.w - cd.z) < 3));
@@ -333,10 +344,13 @@ int walk_variant(int ncrit) {
 
 template <int NI, bool SPLIT>
 static int occupancy_of() {
-  int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_walk<NI, SPLIT>, kWalkThreads, 0) != cudaSuccess || nb < 1)
+  int nb = 0, nb2 = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_walk<NI, SPLIT, false>, kWalkThreads, 0) != cudaSuccess)
     nb = 1;
-  return nb;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb2, k_walk<NI, SPLIT, true>, kWalkThreads, 0) != cudaSuccess)
+    nb2 = 1;
+  nb = nb < nb2 ? nb : nb2;
+  return nb < 1 ? 1 : nb;
 }
 
 int walk_blocks_per_sm(int variant) {
@@ -354,11 +368,20 @@ int walk_blocks_per_sm(int variant) {
 
 void launch_walk(int variant, int nblocks, const int2* groups, const TreeInfo* info, const float4* ipos,
                  const float4* jpos, const uint4* cell_data, const float4* cell_open, const float4* cell_q0,
-                 const float4* cell_q1, float eps2, float4* acc, int* ring_pool, int ring_cap,
-                 unsigned* group_counter, unsigned long long* stats, int* status, cudaStream_t s) {
-#define BONSAI_WALK(NI, SP)                                                                                      \
-  k_walk<NI, SP><<<nblocks, kWalkThreads, 0, s>>>(groups, info, ipos, jpos, cell_data, cell_open, cell_q0, cell_q1, \
-                                                  eps2, acc, ring_pool, ring_cap, group_counter, stats, status)
+                 const float4* cell_q1, const float2* cell_ls, const float* group_inv_theta, float eps2,
+                 float4* acc, int* ring_pool, int ring_cap, unsigned* group_counter, unsigned long long* stats,
+                 int* status, cudaStream_t s) {
+#define BONSAI_WALK(NI, SP)                                                                                        \
+  do {                                                                                                             \
+    if (group_inv_theta)                                                                                           \
+      k_walk<NI, SP, true><<<nblocks, kWalkThreads, 0, s>>>(groups, info, ipos, jpos, cell_data, cell_open,         \
+                                                            cell_q0, cell_q1, cell_ls, group_inv_theta, eps2, acc,  \
+                                                            ring_pool, ring_cap, group_counter, stats, status);    \
+    else                                                                                                           \
+      k_walk<NI, SP, false><<<nblocks, kWalkThreads, 0, s>>>(groups, info, ipos, jpos, cell_data, cell_open,        \
+                                                             cell_q0, cell_q1, cell_ls, nullptr, eps2, acc,         \
+                                                             ring_pool, ring_cap, group_counter, stats, status);   \
+  } while (0)
   switch (variant) {
 #if BONSAI_WALK_SPLIT
     case 0: BONSAI_WALK(1, true); break;

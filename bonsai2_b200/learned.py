@@ -1,0 +1,160 @@
+"""Learned per-group opening angles: training-set generation, training and
+use of the 16 -> 64 -> 64 -> 1 network of csrc/learned.cu.
+
+Training pairs come from the plain method and the FP64 direct sum, both on
+the GPU: for a random subset of groups and a few particles in each, the walk
+runs with every group at each angle of a grid (theta mode 2) and the largest
+angle whose error (geometric mean over the group's sampled particles of
+|da|/|a| against the direct sum) stays below the target is the label.  The
+network is trained with the library's own forward/backward kernels
+(bonsai_mlp_train, Adam, full batch) and used in theta mode 1, where a
+feature kernel and an FP16-weight inference kernel set each group's angle
+inside the step.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from ._lib import BonsaiError, load
+from .treecode import Treecode, _check, _p
+
+NFEAT = 16
+NWEIGHTS = 5313
+LO, HI, OVER = 0.25, 1.25, 3.0
+
+
+def init_weights(seed: int = 0) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    H, F = 64, NFEAT
+    parts = [rng.normal(0, np.sqrt(1.0 / F), H * F), np.zeros(H), rng.normal(0, np.sqrt(1.0 / H), H * H), np.zeros(H),
+             rng.normal(0, np.sqrt(1.0 / H), H), [0.0]]
+    return np.ascontiguousarray(np.concatenate(parts).astype(np.float32))
+
+
+def loss_grad(X, y, w, lo=LO, hi=HI, over=OVER, device=0):
+    X = np.ascontiguousarray(X, np.float32)
+    y = np.ascontiguousarray(y, np.float32)
+    w = np.ascontiguousarray(w, np.float32)
+    g = np.empty(NWEIGHTS, np.float32)
+    loss = ctypes.c_double(0)
+    _check(load().bonsai_mlp_loss_grad(device, _p(X), _p(y), X.shape[0], _p(w), lo, hi, over, _p(g),
+                                       ctypes.byref(loss)), "mlp_loss_grad")
+    return loss.value, g
+
+
+def train(X, y, w0=None, epochs=2000, lr=3e-3, lo=LO, hi=HI, over=OVER, device=0, seed=0):
+    X = np.ascontiguousarray(X, np.float32)
+    y = np.ascontiguousarray(y, np.float32)
+    w = np.ascontiguousarray(init_weights(seed) if w0 is None else w0, np.float32).copy()
+    loss = ctypes.c_double(0)
+    _check(load().bonsai_mlp_train(device, _p(X), _p(y), X.shape[0], _p(w), epochs, lr, lo, hi, over,
+                                   ctypes.byref(loss)), "mlp_train")
+    return w, loss.value
+
+
+def predict(X, w, lo=LO, hi=HI, device=0):
+    X = np.ascontiguousarray(X, np.float32)
+    w = np.ascontiguousarray(w, np.float32)
+    out = np.empty(X.shape[0], np.float32)
+    _check(load().bonsai_mlp_predict(device, _p(X), X.shape[0], _p(w), lo, hi, _p(out)), "mlp_predict")
+    return out
+
+
+def group_features(t: Treecode) -> np.ndarray:
+    G = t.tree_info()["ngroups"]
+    F = np.empty((max(G, 1), NFEAT), np.float32)
+    ng = ctypes.c_int(0)
+    _check(t._L.bonsai_get_group_features(t.handle, _p(F), ctypes.byref(ng)), "get_group_features")
+    return F[:ng.value]
+
+
+def set_group_theta(t: Treecode, theta):
+    th = np.ascontiguousarray(theta, np.float32)
+    _check(t._L.bonsai_set_group_theta(t.handle, _p(th), th.shape[0]), "set_group_theta")
+
+
+def set_theta_mode(t: Treecode, mode: int, lo=LO, hi=HI):
+    _check(t._L.bonsai_set_theta_mode(t.handle, mode, lo, hi), "set_theta_mode")
+
+
+def set_weights(t: Treecode, w):
+    w = np.ascontiguousarray(w, np.float32)
+    _check(t._L.bonsai_set_mlp_weights(t.handle, _p(w), w.shape[0]), "set_mlp_weights")
+
+
+def group_theta(t: Treecode) -> np.ndarray:
+    G = t.tree_info()["ngroups"]
+    out = np.empty(max(G, 1), np.float32)
+    _check(t._L.bonsai_get_group_theta(t.handle, _p(out)), "get_group_theta")
+    return out[:G]
+
+
+DEFAULT_GRID = tuple(np.round(np.arange(0.30, 1.2501, 0.05), 2))
+
+
+def training_set(pos, vel, eps, thetas=DEFAULT_GRID, target=5e-4, samples_per_group=8, max_groups=8192, seed=0,
+                 nleaf=16, ncrit=64, level_split=5, device=0):
+    """(features, label theta, error table) for a random subset of groups.
+
+    The label is the angle at which the group's error (geometric mean over its
+    sampled particles of |da|/|a| against the FP64 direct sum) crosses the
+    target, interpolated linearly in log error between grid angles; clipped to
+    the grid's ends."""
+    n = pos.shape[0]
+    t = Treecode(eps=eps, theta=0.5, ncrit=ncrit, nleaf=nleaf, level_split=level_split, device=device)
+    try:
+        t.alloc(n)
+        t.h_ptclPos[:] = pos
+        t.h_ptclVel[:] = vel
+        t.ptcl_h2d()
+        t.buildTree(nleaf)
+        t.computeMultipoles()
+        t.makeGroups(level_split, ncrit)
+        F = group_features(t)
+        groups = t.groups()
+        G = groups.shape[0]
+        ids = t.walk_arrays()["ids"]
+        rng = np.random.default_rng(seed)
+        gsel = np.sort(rng.choice(G, min(max_groups, G), replace=False))
+        spos = []  # PH positions of the sampled particles
+        owner = []
+        for k, g in enumerate(gsel):
+            pb, np_ = groups[g]
+            take = rng.choice(np_, min(samples_per_group, np_), replace=False)
+            spos.extend(pb + take)
+            owner.extend([k] * len(take))
+        spos = np.asarray(spos, np.int64)
+        owner = np.asarray(owner, np.int64)
+        ref = t.direct_fp64(ids[spos].astype(np.int32), include_self=True)
+        refn = np.linalg.norm(ref[:, :3], axis=1)
+        set_theta_mode(t, 2)
+        E = np.zeros((gsel.shape[0], len(thetas)))
+        for j, th in enumerate(thetas):
+            set_group_theta(t, np.full(G, th, np.float32))
+            t.computeForces(False)
+            acc = t.walk_arrays()["acc"][spos].astype(np.float64)
+            err = np.linalg.norm(acc[:, :3] - ref[:, :3], axis=1) / refn
+            le = np.log(np.maximum(err, 1e-30))
+            E[:, j] = np.exp(np.bincount(owner, weights=le, minlength=gsel.shape[0]) /
+                             np.bincount(owner, minlength=gsel.shape[0]))
+        th = np.asarray(thetas, np.float64)
+        lt = np.log(target)
+        logE = np.log(np.maximum(E, 1e-30))
+        label = np.full(gsel.shape[0], th[0])
+        for g in range(gsel.shape[0]):
+            above = np.nonzero(logE[g] > lt)[0]
+            if above.size == 0:
+                label[g] = th[-1]
+                continue
+            j = above[0]
+            if j == 0:
+                label[g] = th[0]
+                continue
+            e0, e1 = logE[g, j - 1], logE[g, j]
+            f = (lt - e0) / (e1 - e0) if e1 > e0 else 0.0
+            label[g] = th[j - 1] + f * (th[j] - th[j - 1])
+        return F[gsel], label.astype(np.float32), E
+    finally:
+        t.close()

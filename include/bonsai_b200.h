@@ -35,6 +35,7 @@ extern "C" {
 #define BONSAI_STATUS_NONFINITE 8      /* NaN/Inf coordinate in the input */
 #define BONSAI_STATUS_GROUP_CAPACITY 16
 #define BONSAI_STATUS_BAD_PARAM 32
+#define BONSAI_STATUS_SORT_TIMEOUT 64  /* a radix-sort look-back wait hit its bound: results invalid */
 
 /* API errors */
 #define BONSAI_ERR_HANDLE (-1)
@@ -169,6 +170,30 @@ int bonsai_direct_fp64(bonsai_handle h, const int *sample, int ns, int include_s
  * before any stream capture on that device.  Asynchronous on `stream`. */
 int bonsai_direct_fp64_noalloc(const float *d_pos4, int n, const int *d_sample, int ns, double eps2,
                                int include_self, double *d_out, void *stream);
+
+/* ---- per-group opening angles (learned form; no counterpart in the
+ * reference, whose angle is one number baked into every cell's opening size,
+ * computeMultipoles.cu:168-177) ---- */
+#define BONSAI_MLP_FEATURES 16
+#define BONSAI_MLP_WEIGHTS 5313 /* W1[64][16], b1[64], W2[64][64], b2[64], w3[64], b3 */
+/* mode 0: fixed theta (params); 1: theta_g = lo + (hi-lo)*sigmoid(MLP(features_g))
+ * from the weights of bonsai_set_mlp_weights; 2: theta_g from bonsai_set_group_theta. */
+int bonsai_set_theta_mode(bonsai_handle h, int mode, float lo, float hi);
+int bonsai_set_mlp_weights(bonsai_handle h, const float *w, int nw);
+/* host array of ngroups angles for the current groups (after bonsai_make_groups) */
+int bonsai_set_group_theta(bonsai_handle h, const float *theta, int ngroups);
+/* features of the current groups, host float[ngroups * 16] */
+int bonsai_get_group_features(bonsai_handle h, float *out, int *ngroups);
+/* angles used by the last walk in mode 1 or 2, host float[ngroups] */
+int bonsai_get_group_theta(bonsai_handle h, float *out);
+/* MLP on the GPU, host arrays: loss (mean of 0.5 (theta - y)^2 (1 + over [theta > y]))
+ * and its gradient; Adam training for `epochs` full-batch steps (w in/out);
+ * prediction of theta for S feature rows. */
+int bonsai_mlp_loss_grad(int device, const float *X, const float *y, int S, const float *w, float lo, float hi,
+                         float over, float *grad, double *loss);
+int bonsai_mlp_train(int device, const float *X, const float *y, int S, float *w, int epochs, float lr, float lo,
+                     float hi, float over, double *loss);
+int bonsai_mlp_predict(int device, const float *X, int S, const float *w, float lo, float hi, float *theta);
 
 /* Plummer sphere initial conditions on the host: the algorithm of
  * code/plummer.h:9-138 (glibc rand(), same stream), converted to float4 like
