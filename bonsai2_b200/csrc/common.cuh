@@ -90,6 +90,48 @@ __device__ __forceinline__ int set_status(int* status, int bit) {
   return atomicOr(status, bit);
 }
 
+// Ensemble layout: system s owns particles [off[s], off[s+1]) of the state
+// arrays; every stage keeps that partition (sorts and gathers stay inside a
+// system).  Chunks are the per-block work units of the per-system passes: at
+// most kChunk particles of one system, {begin, end, system, 0}.
+constexpr int kChunk = 4096;
+
+// largest s in [0, nsys) with off[s] <= i
+__device__ __forceinline__ int sys_of(const int* __restrict__ off, int nsys, int i) {
+  int lo = 0, hi = nsys;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(off + mid) <= i) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// computeBoundingBox's finalisation (buildTree.cu:145-161) from the particle
+// extent [a, b]: hsize = smallest power of two >= the largest half extent
+// (floored at max(2^-100, 2^-40 * pow2 >= max|c|), so that a zero-extent
+// input still gives a finite box whose centre quantisation fits 64 bits),
+// centre quantised to hsize/2^20.
+__device__ __forceinline__ Box box_from_extent(const float a[3], const float b[3]) {
+  float c[3], h[3];
+  for (int k = 0; k < 3; k++) { c[k] = (b[k] + a[k]) * 0.5f; h[k] = (b[k] - a[k]) * 0.5f; }
+  const float hm = fmaxf(h[2], fmaxf(h[1], h[0]));
+  const float cm = fmaxf(fabsf(c[0]), fmaxf(fabsf(c[1]), fabsf(c[2])));
+  float pw = 1.0f;
+  while (pw < cm) pw *= 2.0f;
+  while (pw * 0.5f >= cm && pw > 7.888609052210118e-31f) pw *= 0.5f;
+  const float floor_h = fmaxf(pw * 9.094947017729282e-13f, 7.888609052210118e-31f);
+  float hs = 1.0f;
+  while (hs > hm && hs > floor_h) hs *= 0.5f;
+  while (hs < hm) hs *= 2.0f;
+  const float hq = __fdiv_rn(hs, (float)(1 << 20));
+  Box bx;
+  bx.cx = __fmul_rn(hq, (float)(long long)__fdiv_rn(c[0], hq));
+  bx.cy = __fmul_rn(hq, (float)(long long)__fdiv_rn(c[1], hq));
+  bx.cz = __fmul_rn(hq, (float)(long long)__fdiv_rn(c[2], hq));
+  bx.hsize = hs;
+  return bx;
+}
+
 // Level (1..21) of the first octant digit where two sorted 63-bit keys
 // differ; kMaxLevel+1 when they are equal.
 __device__ __forceinline__ int diff_level(unsigned long long a, unsigned long long b) {

@@ -81,6 +81,59 @@ void make_groups(const unsigned long long* sorted_ph, int n, int level_split, in
   k_group_write<<<1184, 256, 0, s>>>(seg_end, seg_start, ng, nbins, ncrit, groups, group_cap, info);
 }
 
+// Ensembles.  Bins repeat from system to system, so segments are numbered by
+// position instead: flag[i] = 1 where a segment starts (bin change or system
+// start), an exclusive scan gives every start its segment index, and the
+// group sizes and offsets follow as above over the segment list (capacity n,
+// tail entries sized 0).  Inside a system the segments and groups are those
+// the system gets alone.
+__global__ void __launch_bounds__(256) k_seg_flags(const unsigned long long* __restrict__ sorted, int n, int shift,
+                                                   unsigned* __restrict__ flag) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    flag[i] = (i == 0 || (sorted[i] >> shift) != (sorted[i - 1] >> shift)) ? 1u : 0u;
+}
+
+__global__ void k_seg_mark_systems(const int* __restrict__ sys_off, int nsys, unsigned* __restrict__ flag) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nsys; s += gridDim.x * blockDim.x) flag[sys_off[s]] = 1u;
+}
+
+// seg_beg/seg_end of every segment (flag is reused for the group counts next)
+__global__ void __launch_bounds__(256) k_seg_bounds(const unsigned* __restrict__ flag,
+                                                    const unsigned* __restrict__ sid, int n,
+                                                    unsigned* __restrict__ seg_beg, unsigned* __restrict__ seg_end) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const unsigned f = flag[i], k = sid[i];
+    if (f) {
+      seg_beg[k] = (unsigned)i;
+      if (i > 0) seg_end[k - 1] = (unsigned)i;
+    }
+    if (i == n - 1) seg_end[k + f - 1] = (unsigned)n;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_seg_group_sizes(const unsigned* __restrict__ seg_beg,
+                                                         const unsigned* __restrict__ seg_end,
+                                                         const unsigned* __restrict__ nseg, int m, int ncrit,
+                                                         unsigned* __restrict__ ng) {
+  const int ns = (int)*nseg;
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < m; b += gridDim.x * blockDim.x)
+    ng[b] = b < ns ? (seg_end[b] - seg_beg[b] + (unsigned)ncrit - 1u) / (unsigned)ncrit : 0u;
+}
+
+void make_groups_sys(const unsigned long long* sorted_ph, int n, int level_split, int ncrit, const int* sys_off,
+                     int nsys, unsigned* flag, unsigned* sid, unsigned* seg_beg, unsigned* seg_end, unsigned* nseg,
+                     unsigned* bsum, int2* groups, int group_cap, TreeInfo* info, cudaStream_t s) {
+  const int shift = 63 - 3 * level_split;
+  k_seg_flags<<<1184, 256, 0, s>>>(sorted_ph, n, shift, flag);
+  k_seg_mark_systems<<<(nsys + 255) / 256, 256, 0, s>>>(sys_off, nsys, flag);
+  exclusive_scan(flag, sid, n, bsum, nseg, s);
+  k_seg_bounds<<<1184, 256, 0, s>>>(flag, sid, n, seg_beg, seg_end);
+  unsigned* ng = flag;
+  k_seg_group_sizes<<<1184, 256, 0, s>>>(seg_beg, seg_end, nseg, n, ncrit, ng);
+  exclusive_scan(ng, ng, n, bsum, (unsigned*)&info->ngroups, s);
+  k_group_write<<<1184, 256, 0, s>>>(seg_end, seg_beg, ng, n, ncrit, groups, group_cap, info);
+}
+
 // state gather: out[k] = in[perm[k]] for positions, velocities and ids
 __global__ void __launch_bounds__(256) k_gather_state(const int* __restrict__ perm, int n,
                                                       const float4* __restrict__ pos, const float4* __restrict__ vel,

@@ -21,6 +21,10 @@ __global__ void k_box(const float4* __restrict__ pos, int n, float* __restrict__
 __global__ void k_keys(const float4* __restrict__ pos, int n, const Box* __restrict__ boxp,
                        const uint16_t* __restrict__ ph_table, unsigned long long* __restrict__ tkey,
                        unsigned long long* __restrict__ pkey);
+// ensemble: per-system boxes (chunk extents folded per system) and keys
+void launch_sys_keys(const float4* pos, const int4* chunks, int nchunks, const int* chunk_beg, int nsys,
+                     float* box_partial, Box* boxes, const uint16_t* ph_table, unsigned long long* tkey,
+                     unsigned long long* pkey, int* status, int nblocks, cudaStream_t s);
 
 // sort.cu
 int sort_tiles(int n);
@@ -28,13 +32,14 @@ int scan_blocks(int m);
 void exclusive_scan(const unsigned* in, unsigned* out, int m, unsigned* bsum, unsigned* total, cudaStream_t s);
 size_t sort_status_words(int n);
 void radix_sort_pairs(unsigned long long* keys_a, unsigned long long* keys_b, int* vals_a, int* vals_b,
-                      const int* vals_in, int n, unsigned* work, int* err, int passes, cudaStream_t s);
+                      const int* vals_in, int n, unsigned* work, int* err, int passes, const int* sys_off, int nsys,
+                      cudaStream_t s);
 
 // tree.cu
 int tree_tiles(int n);
 void build_tree(const unsigned long long* sorted_keys, int n, int nleaf, int cell_cap, int leaf_cap, uint8_t* dlev,
                 uint16_t* chain, unsigned* hist, TreeInfo* info, uint4* cell_data, int* cell_parent, int* leaf_list,
-                int* mp_count, cudaStream_t s);
+                int* mp_count, const int* sys_off, int nsys, int* root_beg, cudaStream_t s);
 
 // multipoles.cu
 __global__ void k_multipoles(const int* __restrict__ leaf_list, const TreeInfo* __restrict__ info,
@@ -52,6 +57,9 @@ __global__ void k_multipoles_ref_layout(const TreeInfo* __restrict__ info, const
 void make_groups(const unsigned long long* sorted_ph, int n, int level_split, int ncrit, unsigned* count,
                  unsigned* seg_start, unsigned* ng, unsigned* bsum, int2* groups, int group_cap, TreeInfo* info,
                  cudaStream_t s);
+void make_groups_sys(const unsigned long long* sorted_ph, int n, int level_split, int ncrit, const int* sys_off,
+                     int nsys, unsigned* flag, unsigned* sid, unsigned* seg_beg, unsigned* seg_end, unsigned* nseg,
+                     unsigned* bsum, int2* groups, int group_cap, TreeInfo* info, cudaStream_t s);
 __global__ void k_gather_state(const int* __restrict__ perm, int n, const float4* __restrict__ pos,
                                const float4* __restrict__ vel, const int* __restrict__ id, float4* __restrict__ pos_o,
                                float4* __restrict__ vel_o, int* __restrict__ id_o);
@@ -59,18 +67,26 @@ __global__ void k_gather_pos(const int* __restrict__ perm, int n, const float4* 
                              float4* __restrict__ out);
 
 // walk.cu
-int walk_variant(int ncrit);
+int walk_variant(int ncrit, int layout);
 int walk_blocks_per_sm(int variant);
 // group_inv_theta == nullptr: the fixed opening angle baked into cell_open.w;
 // else 1/theta per group with (l, s) from cell_ls
 void launch_walk(int variant, int nblocks, const int2* groups, const TreeInfo* info, const float4* ipos, const float4* jpos,
                  const uint4* cell_data, const float4* cell_open, const float4* cell_q0, const float4* cell_q1,
                  const float2* cell_ls, const float* group_inv_theta, float eps2, float4* acc, int* ring_pool,
-                 int ring_cap, unsigned* group_counter, unsigned long long* stats, int* status, cudaStream_t s);
+                 int ring_cap, unsigned* group_counter, unsigned long long* stats, int* status, const int* sys_off,
+                 int nsys, const int* root_beg, cudaStream_t s);
 
 // move.cu
 void launch_move(float4* pos, float4* vel, const float4* acc, int n, float dt, int* closing, float eps, int write,
                  double* partial, int nblocks, unsigned* ticket, double* energies, cudaStream_t s);
+// ensemble move: energies per chunk, folded per system and in total
+void launch_move_sys(float4* pos, float4* vel, const float4* acc, const int4* chunks, int nchunks,
+                     const int* chunk_beg, int nsys, float dt, int* closing, float eps, int write, double* chunk_part,
+                     int nblocks, unsigned* ticket, double* energies, double* sys_energies, cudaStream_t s);
+// FP64 direct sum inside each sample's own system (one block per sample)
+void launch_direct_fp64_sys(const float4* pos, const int* sys_off, int nsys, const int* sample, int ns, double eps2,
+                            int include_self, double* out, cudaStream_t s);
 void launch_direct_fp64(const float4* pos, int n, const int* sample, int ns, double eps2, int include_self,
                         double* part, int nsplit, double* out, cudaStream_t s);
 __global__ void k_scatter_by_id(const int* __restrict__ id, int n, const float4* __restrict__ in,

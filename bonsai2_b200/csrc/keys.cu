@@ -107,27 +107,7 @@ __global__ void __launch_bounds__(256) k_box(const float4* __restrict__ pos, int
       }
     for (int k = 0; k < 3; k++) { a[k] = warp_min_f32(a[k]); b[k] = warp_max_f32(b[k]); }
     if (threadIdx.x == 0) {
-      // buildTree.cu:145-161
-      float c[3], h[3];
-      for (int k = 0; k < 3; k++) { c[k] = (b[k] + a[k]) * 0.5f; h[k] = (b[k] - a[k]) * 0.5f; }
-      const float hm = fmaxf(h[2], fmaxf(h[1], h[0]));
-      // floor max(2^-100, 2^-40 * pow2 >= max|c|): a zero-extent input still
-      // gives a finite box whose centre quantisation fits 64 bits
-      const float cm = fmaxf(fabsf(c[0]), fmaxf(fabsf(c[1]), fabsf(c[2])));
-      float pw = 1.0f;
-      while (pw < cm) pw *= 2.0f;
-      while (pw * 0.5f >= cm && pw > 7.888609052210118e-31f) pw *= 0.5f;
-      const float floor_h = fmaxf(pw * 9.094947017729282e-13f, 7.888609052210118e-31f);
-      float hs = 1.0f;
-      while (hs > hm && hs > floor_h) hs *= 0.5f;
-      while (hs < hm) hs *= 2.0f;
-      const float hq = __fdiv_rn(hs, (float)(1 << 20));
-      Box bx;
-      bx.cx = __fmul_rn(hq, (float)(long long)__fdiv_rn(c[0], hq));
-      bx.cy = __fmul_rn(hq, (float)(long long)__fdiv_rn(c[1], hq));
-      bx.cz = __fmul_rn(hq, (float)(long long)__fdiv_rn(c[2], hq));
-      bx.hsize = hs;
-      *box = bx;
+      *box = box_from_extent(a, b);
       *ticket = 0u;
     }
   }
@@ -138,6 +118,48 @@ __device__ __forceinline__ int quantise(float x, float bmin, float inv) {
   return __float2int_rz(__fmul_rn(__fmul_rn(__fsub_rn(x, bmin), inv), 2097152.0f));
 }
 
+struct KeyFrame {
+  float cx, cy, cz, hsize, inv, bx, by, bz;
+};
+
+__device__ __forceinline__ KeyFrame key_frame(const Box b) {
+  KeyFrame f;
+  f.cx = b.cx; f.cy = b.cy; f.cz = b.cz; f.hsize = b.hsize;
+  f.inv = __fdiv_rn(0.5f, b.hsize);
+  f.bx = __fsub_rn(b.cx, b.hsize); f.by = __fsub_rn(b.cy, b.hsize); f.bz = __fsub_rn(b.cz, b.hsize);
+  return f;
+}
+
+__device__ __forceinline__ void particle_keys(const float4 p, const KeyFrame& f, const uint16_t* tab,
+                                              unsigned long long& tkey, unsigned long long& pkey) {
+  // exact octant path (comparison partition)
+  float cx = f.cx, cy = f.cy, cz = f.cz, h = f.hsize;
+  unsigned long long tk = 0ull;
+#pragma unroll
+  for (int L = 0; L < kMaxLevel; L++) {
+    const bool ox = cx <= p.x, oy = cy <= p.y, oz = cz <= p.z;
+    tk = (tk << 3) | (unsigned long long)((int)ox | ((int)oy << 1) | ((int)oz << 2));
+    const float s = __fmul_rn(0.5f, h);
+    cx = __fadd_rn(cx, ox ? s : -s);
+    cy = __fadd_rn(cy, oy ? s : -s);
+    cz = __fadd_rn(cz, oz ? s : -s);
+    h = s;
+  }
+  tkey = tk;
+  // Peano-Hilbert key through the state table
+  const int qx = quantise(p.x, f.bx, f.inv), qy = quantise(p.y, f.by, f.inv), qz = quantise(p.z, f.bz, f.inv);
+  unsigned st = 0;
+  unsigned long long pk = 0ull;
+#pragma unroll
+  for (int L = kMaxLevel - 1; L >= 0; L--) {
+    const int o = (((qx >> L) & 1) << 2) | (((qy >> L) & 1) << 1) | ((qz >> L) & 1);
+    const unsigned e = tab[st * 8 + o];
+    pk = (pk << 3) | (unsigned long long)(e & 7u);
+    st = e >> 3;
+  }
+  pkey = pk;
+}
+
 __global__ void __launch_bounds__(256) k_keys(const float4* __restrict__ pos, int n, const Box* __restrict__ boxp,
                                               const uint16_t* __restrict__ ph_table,
                                               unsigned long long* __restrict__ tkey,
@@ -145,38 +167,86 @@ __global__ void __launch_bounds__(256) k_keys(const float4* __restrict__ pos, in
   __shared__ uint16_t tab[384];
   for (int t = threadIdx.x; t < 384; t += blockDim.x) tab[t] = ph_table[t];
   __syncthreads();
-  const Box b = *boxp;
-  const float inv = __fdiv_rn(0.5f, b.hsize);
-  const float bx = __fsub_rn(b.cx, b.hsize), by = __fsub_rn(b.cy, b.hsize), bz = __fsub_rn(b.cz, b.hsize);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const float4 p = pos[i];
-    // exact octant path (comparison partition)
-    float cx = b.cx, cy = b.cy, cz = b.cz, h = b.hsize;
-    unsigned long long tk = 0ull;
-#pragma unroll
-    for (int L = 0; L < kMaxLevel; L++) {
-      const bool ox = cx <= p.x, oy = cy <= p.y, oz = cz <= p.z;
-      tk = (tk << 3) | (unsigned long long)((int)ox | ((int)oy << 1) | ((int)oz << 2));
-      const float s = __fmul_rn(0.5f, h);
-      cx = __fadd_rn(cx, ox ? s : -s);
-      cy = __fadd_rn(cy, oy ? s : -s);
-      cz = __fadd_rn(cz, oz ? s : -s);
-      h = s;
+  const KeyFrame f = key_frame(*boxp);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    particle_keys(pos[i], f, tab, tkey[i], pkey[i]);
+}
+
+// ---------------------------------------------------------------------------
+// Ensembles: every system gets its own box (the same finalisation, so a
+// system's box equals the box it gets alone) and its keys are taken in that
+// box.  One block per chunk (a chunk never spans two systems).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_sys_box(const float4* __restrict__ pos, const int4* __restrict__ chunks,
+                                                 int nchunks, float* __restrict__ partial,
+                                                 int* __restrict__ status) {
+  __shared__ float sm[6][8];
+  for (int c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    const int4 ch = chunks[c];
+    float mn[3] = {1e10f, 1e10f, 1e10f}, mx[3] = {-1e10f, -1e10f, -1e10f};
+    bool bad = false;
+    for (int i = ch.x + threadIdx.x; i < ch.y; i += blockDim.x) {
+      const float4 p = __ldcs(pos + i);
+      bad |= !(isfinite(p.x) && isfinite(p.y) && isfinite(p.z));
+      mn[0] = fminf(mn[0], p.x); mn[1] = fminf(mn[1], p.y); mn[2] = fminf(mn[2], p.z);
+      mx[0] = fmaxf(mx[0], p.x); mx[1] = fmaxf(mx[1], p.y); mx[2] = fmaxf(mx[2], p.z);
     }
-    tkey[i] = tk;
-    // Peano-Hilbert key through the state table
-    const int qx = quantise(p.x, bx, inv), qy = quantise(p.y, by, inv), qz = quantise(p.z, bz, inv);
-    unsigned st = 0;
-    unsigned long long pk = 0ull;
-#pragma unroll
-    for (int L = kMaxLevel - 1; L >= 0; L--) {
-      const int o = (((qx >> L) & 1) << 2) | (((qy >> L) & 1) << 1) | ((qz >> L) & 1);
-      const unsigned e = tab[st * 8 + o];
-      pk = (pk << 3) | (unsigned long long)(e & 7u);
-      st = e >> 3;
+    if (__any_sync(kFull, bad) && lane_id() == 0) set_status(status, kStatusNonFinite);
+    for (int k = 0; k < 3; k++) {
+      const float a = warp_min_f32(mn[k]), b = warp_max_f32(mx[k]);
+      if (lane_id() == 0) { sm[k][threadIdx.x >> 5] = a; sm[3 + k][threadIdx.x >> 5] = b; }
     }
-    pkey[i] = pk;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      const int nw = blockDim.x >> 5;
+      for (int k = 0; k < 3; k++) {
+        const float a = warp_min_f32(threadIdx.x < nw ? sm[k][threadIdx.x] : 1e10f);
+        const float b = warp_max_f32(threadIdx.x < nw ? sm[3 + k][threadIdx.x] : -1e10f);
+        if (threadIdx.x == 0) { partial[6 * c + k] = a; partial[6 * c + 3 + k] = b; }
+      }
+    }
+    __syncthreads();
   }
+}
+
+// one warp per system: fold the system's chunk extents, finalise its box
+__global__ void __launch_bounds__(256) k_sys_box_final(const float* __restrict__ partial,
+                                                       const int* __restrict__ chunk_beg, int nsys,
+                                                       Box* __restrict__ boxes) {
+  const int lane = threadIdx.x & 31;
+  for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < nsys; s += (gridDim.x * blockDim.x) >> 5) {
+    float a[3] = {1e10f, 1e10f, 1e10f}, b[3] = {-1e10f, -1e10f, -1e10f};
+    for (int c = chunk_beg[s] + lane; c < chunk_beg[s + 1]; c += 32)
+      for (int k = 0; k < 3; k++) {
+        a[k] = fminf(a[k], partial[6 * c + k]);
+        b[k] = fmaxf(b[k], partial[6 * c + 3 + k]);
+      }
+    for (int k = 0; k < 3; k++) { a[k] = warp_min_f32(a[k]); b[k] = warp_max_f32(b[k]); }
+    if (lane == 0) boxes[s] = box_from_extent(a, b);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_keys_sys(const float4* __restrict__ pos, const int4* __restrict__ chunks,
+                                                  int nchunks, const Box* __restrict__ boxes,
+                                                  const uint16_t* __restrict__ ph_table,
+                                                  unsigned long long* __restrict__ tkey,
+                                                  unsigned long long* __restrict__ pkey) {
+  __shared__ uint16_t tab[384];
+  for (int t = threadIdx.x; t < 384; t += blockDim.x) tab[t] = ph_table[t];
+  __syncthreads();
+  for (int c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    const int4 ch = chunks[c];
+    const KeyFrame f = key_frame(boxes[ch.z]);
+    for (int i = ch.x + threadIdx.x; i < ch.y; i += blockDim.x) particle_keys(pos[i], f, tab, tkey[i], pkey[i]);
+  }
+}
+
+void launch_sys_keys(const float4* pos, const int4* chunks, int nchunks, const int* chunk_beg, int nsys,
+                     float* box_partial, Box* boxes, const uint16_t* ph_table, unsigned long long* tkey,
+                     unsigned long long* pkey, int* status, int nblocks, cudaStream_t s) {
+  k_sys_box<<<nblocks, 256, 0, s>>>(pos, chunks, nchunks, box_partial, status);
+  k_sys_box_final<<<(nsys + 7) / 8, 256, 0, s>>>(box_partial, chunk_beg, nsys, boxes);
+  k_keys_sys<<<nblocks, 256, 0, s>>>(pos, chunks, nchunks, boxes, ph_table, tkey, pkey);
 }
 
 }  // namespace bonsai

@@ -18,6 +18,51 @@ namespace bonsai {
 
 constexpr int kNE = 8;
 
+struct EnergySums {
+  double T = 0, W = 0, S = 0, px = 0, py = 0, pz = 0, mt = 0;
+};
+
+// one particle: closing kick (hc = 0 on the first step), energy terms at the
+// synchronised point, then opening kick and drift when write is set
+__device__ __forceinline__ void move_one(float4* __restrict__ pos, float4* __restrict__ vel,
+                                         const float4* __restrict__ acc, int i, float dt, float h, float hc,
+                                         double ieps, int write, EnergySums& e) {
+  float4 p = pos[i], v = vel[i];
+  const float4 a = acc[i];
+  v.x = fmaf(a.x, hc, v.x); v.y = fmaf(a.y, hc, v.y); v.z = fmaf(a.z, hc, v.z);
+  const double m = p.w;
+  e.T += 0.5 * m * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
+  e.W += 0.5 * m * a.w;
+  e.S += 0.5 * m * m * ieps;
+  e.px += m * v.x; e.py += m * v.y; e.pz += m * v.z; e.mt += m;
+  if (write) {
+    v.x = fmaf(a.x, h, v.x); v.y = fmaf(a.y, h, v.y); v.z = fmaf(a.z, h, v.z);
+    p.x = fmaf(v.x, dt, p.x); p.y = fmaf(v.y, dt, p.y); p.z = fmaf(v.z, dt, p.z);
+    pos[i] = p;
+    vel[i] = v;
+  }
+}
+
+// block sum of the eight energy terms {T, W, W+S, T+W+S, Px, Py, Pz, M};
+// thread k < 8 returns term k
+__device__ __forceinline__ double block_energy_sum(const EnergySums& s, double (*sh)[8]) {
+  const double e[kNE] = {s.T, s.W, s.W + s.S, s.T + s.W + s.S, s.px, s.py, s.pz, s.mt};
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < kNE; k++) {
+    double x = e[k];
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
+    if (lane == 0) sh[k][w] = x;
+  }
+  __syncthreads();
+  double x = 0;
+  if (threadIdx.x < kNE)
+    for (int q = 0; q < (int)(blockDim.x >> 5); q++) x += sh[threadIdx.x][q];
+  __syncthreads();
+  return x;
+}
+
 // closing kick taken when *closing is set (device flag: set by every writing
 // move, cleared when particles are loaded), so the same captured graph serves
 // the first and later steps.  write == 0 computes the energies only.
@@ -28,41 +73,14 @@ __global__ void __launch_bounds__(256) k_move(float4* __restrict__ pos, float4* 
                                               double* __restrict__ energies) {
   const float h = 0.5f * dt;
   const float hc = (*closing) ? h : 0.0f;
-  double T = 0, W = 0, S = 0, px = 0, py = 0, pz = 0, mt = 0;
   const double ieps = eps > 0.f ? 1.0 / (double)eps : 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    float4 p = pos[i], v = vel[i];
-    const float4 a = acc[i];
-    v.x = fmaf(a.x, hc, v.x); v.y = fmaf(a.y, hc, v.y); v.z = fmaf(a.z, hc, v.z);
-    const double m = p.w;
-    T += 0.5 * m * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
-    W += 0.5 * m * a.w;
-    S += 0.5 * m * m * ieps;
-    px += m * v.x; py += m * v.y; pz += m * v.z; mt += m;
-    if (write) {
-      v.x = fmaf(a.x, h, v.x); v.y = fmaf(a.y, h, v.y); v.z = fmaf(a.z, h, v.z);
-      p.x = fmaf(v.x, dt, p.x); p.y = fmaf(v.y, dt, p.y); p.z = fmaf(v.z, dt, p.z);
-      pos[i] = p;
-      vel[i] = v;
-    }
-  }
-  double e[kNE] = {T, W, W + S, T + W + S, px, py, pz, mt};
+  EnergySums e;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    move_one(pos, vel, acc, i, dt, h, hc, ieps, write, e);
   __shared__ double sh[kNE][8];
   __shared__ bool last;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-#pragma unroll
-  for (int k = 0; k < kNE; k++) {
-    double x = e[k];
-#pragma unroll
-    for (int o = 16; o >= 1; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
-    if (lane == 0) sh[k][w] = x;
-  }
-  __syncthreads();
-  if (threadIdx.x < kNE) {
-    double x = 0;
-    for (int q = 0; q < (int)(blockDim.x >> 5); q++) x += sh[threadIdx.x][q];
-    partial[blockIdx.x * kNE + threadIdx.x] = x;
-  }
+  const double x = block_energy_sum(e, sh);
+  if (threadIdx.x < kNE) partial[blockIdx.x * kNE + threadIdx.x] = x;
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
@@ -72,14 +90,67 @@ __global__ void __launch_bounds__(256) k_move(float4* __restrict__ pos, float4* 
   if (!last) return;
   __threadfence();
   if (threadIdx.x < kNE) {
-    double x = 0;
-    for (int b = 0; b < (int)gridDim.x; b++) x += __ldcg(partial + b * kNE + threadIdx.x);
-    energies[threadIdx.x] = x;
+    double y = 0;
+    for (int b = 0; b < (int)gridDim.x; b++) y += __ldcg(partial + b * kNE + threadIdx.x);
+    energies[threadIdx.x] = y;
   }
   if (threadIdx.x == 0) {
     *ticket = 0u;
     if (write) *closing = 1;
   }
+}
+
+// Ensemble move: the same per-particle update, blocks over chunks; each
+// chunk's energy terms are kept, and the last block folds them per system
+// (chunk order) and in total.
+__global__ void __launch_bounds__(256) k_move_sys(float4* __restrict__ pos, float4* __restrict__ vel,
+                                                  const float4* __restrict__ acc, const int4* __restrict__ chunks,
+                                                  int nchunks, const int* __restrict__ chunk_beg, int nsys, float dt,
+                                                  int* __restrict__ closing, float eps, int write,
+                                                  double* __restrict__ chunk_part, unsigned* __restrict__ ticket,
+                                                  double* __restrict__ energies, double* __restrict__ sys_energies) {
+  const float h = 0.5f * dt;
+  const float hc = (*closing) ? h : 0.0f;
+  const double ieps = eps > 0.f ? 1.0 / (double)eps : 0.0;
+  __shared__ double sh[kNE][8];
+  __shared__ bool last;
+  for (int c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    const int4 ch = chunks[c];
+    EnergySums e;
+    for (int i = ch.x + threadIdx.x; i < ch.y; i += blockDim.x) move_one(pos, vel, acc, i, dt, h, hc, ieps, write, e);
+    const double x = block_energy_sum(e, sh);
+    if (threadIdx.x < kNE) chunk_part[(size_t)c * kNE + threadIdx.x] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int s = threadIdx.x; s < nsys; s += blockDim.x) {
+    double y[kNE] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int c = chunk_beg[s]; c < chunk_beg[s + 1]; c++)
+      for (int k = 0; k < kNE; k++) y[k] += __ldcg(chunk_part + (size_t)c * kNE + k);
+    for (int k = 0; k < kNE; k++) sys_energies[(size_t)s * kNE + k] = y[k];
+  }
+  if (threadIdx.x < kNE) {
+    double y = 0;
+    for (int c = 0; c < nchunks; c++) y += __ldcg(chunk_part + (size_t)c * kNE + threadIdx.x);
+    energies[threadIdx.x] = y;
+  }
+  if (threadIdx.x == 0) {
+    *ticket = 0u;
+    if (write) *closing = 1;
+  }
+}
+
+void launch_move_sys(float4* pos, float4* vel, const float4* acc, const int4* chunks, int nchunks,
+                     const int* chunk_beg, int nsys, float dt, int* closing, float eps, int write, double* chunk_part,
+                     int nblocks, unsigned* ticket, double* energies, double* sys_energies, cudaStream_t s) {
+  k_move_sys<<<nblocks, 256, 0, s>>>(pos, vel, acc, chunks, nchunks, chunk_beg, nsys, dt, closing, eps, write,
+                                     chunk_part, ticket, energies, sys_energies);
 }
 
 void launch_move(float4* pos, float4* vel, const float4* acc, int n, float dt, int* closing, float eps, int write,
@@ -139,6 +210,54 @@ void launch_direct_fp64(const float4* pos, int n, const int* sample, int ns, dou
   dim3 grid((ns + 255) / 256, nsplit);
   k_direct_fp64<<<grid, 256, 0, s>>>(pos, n, sample, ns, eps2, include_self, part);
   k_direct_fold<<<(4 * ns + 255) / 256, 256, 0, s>>>(part, ns, nsplit, out);
+}
+
+// Ensemble checker: each sample's force from the particles of its own system
+// only (positions in the caller's order, systems contiguous); one block per
+// sample, fixed-order block reduction.
+__global__ void __launch_bounds__(256) k_direct_fp64_sys(const float4* __restrict__ pos,
+                                                         const int* __restrict__ sys_off, int nsys,
+                                                         const int* __restrict__ sample, int ns, double eps2,
+                                                         int include_self, double* __restrict__ out) {
+  __shared__ double sh[4][8];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int s = blockIdx.x; s < ns; s += gridDim.x) {
+    const int i = sample[s];
+    const int sy = sys_of(sys_off, nsys, i);
+    const int jb = sys_off[sy], je = sys_off[sy + 1];
+    const float4 pi = pos[i];
+    const double xi = pi.x, yi = pi.y, zi = pi.z;
+    double a[4] = {0, 0, 0, 0};
+    for (int j = jb + threadIdx.x; j < je; j += blockDim.x) {
+      if (j == i && !include_self) continue;
+      const float4 q = pos[j];
+      const double dx = q.x - xi, dy = q.y - yi, dz = q.z - zi;
+      const double r2 = fma(dz, dz, fma(dy, dy, fma(dx, dx, eps2)));
+      const double rinv = rsqrt(r2);
+      const double mr = q.w * rinv;
+      const double mr3 = mr * rinv * rinv;
+      a[0] = fma(mr3, dx, a[0]); a[1] = fma(mr3, dy, a[1]); a[2] = fma(mr3, dz, a[2]); a[3] -= mr;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      double x = a[k];
+#pragma unroll
+      for (int o = 16; o >= 1; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
+      if (lane == 0) sh[k][w] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+      double x = 0;
+      for (int q = 0; q < (int)(blockDim.x >> 5); q++) x += sh[threadIdx.x][q];
+      out[(size_t)s * 4 + threadIdx.x] = x;
+    }
+    __syncthreads();
+  }
+}
+
+void launch_direct_fp64_sys(const float4* pos, const int* sys_off, int nsys, const int* sample, int ns, double eps2,
+                            int include_self, double* out, cudaStream_t s) {
+  k_direct_fp64_sys<<<ns < 65535 ? ns : 65535, 256, 0, s>>>(pos, sys_off, nsys, sample, ns, eps2, include_self, out);
 }
 
 // out[id[k]] = in[k]

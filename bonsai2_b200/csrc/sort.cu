@@ -151,14 +151,20 @@ __global__ void __launch_bounds__(256) k_sort_hist_scan(unsigned* __restrict__ g
   }
 }
 
+// SYSD: the digit is a byte of the element's system index (sys_of of its
+// value, the element's position in the sort's input order), not of its key:
+// the passes that make an ensemble sort stable-partition by system last.
+template <bool SYSD>
 __global__ void __launch_bounds__(kSortThreads) k_sort_onesweep(
     const unsigned long long* __restrict__ keys_in, const int* __restrict__ vals_in, int n, int shift,
     const unsigned* __restrict__ gbase, unsigned* __restrict__ status, unsigned* __restrict__ tile_counter,
-    unsigned long long* __restrict__ keys_out, int* __restrict__ vals_out, int* __restrict__ err) {
+    unsigned long long* __restrict__ keys_out, int* __restrict__ vals_out, int* __restrict__ err,
+    const int* __restrict__ sys_off, int nsys) {
   __shared__ unsigned wcnt[kSortThreads / 32][256];
   __shared__ unsigned tile_off[256];
   __shared__ unsigned dstart[256];
   __shared__ unsigned long long stage[kSortTile];  // keys, then values (as 32-bit) in digit order
+  __shared__ unsigned char sdig[SYSD ? kSortTile : 1];
   __shared__ unsigned sh[32];
   __shared__ int tile_sh;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -169,12 +175,20 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_onesweep(
   const int base = tile * kSortTile + w * (32 * kSortItems);
   unsigned long long key[kSortItems];
   unsigned rank[kSortItems];
+  unsigned dpack[SYSD ? kSortItems / 4 : 1];
 #pragma unroll
   for (int k = 0; k < kSortItems; k++) {
     const int i = base + k * 32 + lane;
     const bool ok = i < n;
     key[k] = ok ? keys_in[i] : 0ull;
-    const unsigned d = ok ? ((unsigned)(key[k] >> shift) & 255u) : 256u;
+    unsigned d;
+    if constexpr (SYSD) {
+      d = ok ? (((unsigned)sys_of(sys_off, nsys, vals_in ? vals_in[i] : i) >> shift) & 255u) : 256u;
+      if ((k & 3) == 0) dpack[k >> 2] = 0u;
+      dpack[k >> 2] |= (d & 255u) << (8 * (k & 3));
+    } else {
+      d = ok ? ((unsigned)(key[k] >> shift) & 255u) : 256u;
+    }
     const unsigned peers = __match_any_sync(kFull, d);
     const unsigned before = (unsigned)__popc(peers & lanemask_lt());
     const unsigned cur = ok ? wcnt[w][d] : 0u;
@@ -228,26 +242,31 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_onesweep(
   for (int k = 0; k < kSortItems; k++) {
     const int i = base + k * 32 + lane;
     if (i < n) {
-      const unsigned dd = (unsigned)(key[k] >> shift) & 255u;
+      unsigned dd;
+      if constexpr (SYSD) dd = (dpack[k >> 2] >> (8 * (k & 3))) & 255u;
+      else dd = (unsigned)(key[k] >> shift) & 255u;
       lpos[k] = tile_off[dd] + wcnt[w][dd] + rank[k];
       stage[lpos[k]] = key[k];
+      if constexpr (SYSD) sdig[lpos[k]] = (unsigned char)dd;
     }
   }
   __syncthreads();
   for (int j = threadIdx.x; j < tile_n; j += kSortThreads) {
     const unsigned long long kk = stage[j];
-    const unsigned dd = (unsigned)(kk >> shift) & 255u;
+    unsigned dd;
+    if constexpr (SYSD) dd = sdig[j];
+    else dd = (unsigned)(kk >> shift) & 255u;
     keys_out[dstart[dd] + (unsigned)j - tile_off[dd]] = kk;
   }
   __syncthreads();
   unsigned* stage32 = reinterpret_cast<unsigned*>(stage);
-  unsigned char* digit_of = reinterpret_cast<unsigned char*>(stage32 + kSortTile);
+  unsigned char* digit_of = SYSD ? sdig : reinterpret_cast<unsigned char*>(stage32 + kSortTile);
 #pragma unroll
   for (int k = 0; k < kSortItems; k++) {
     const int i = base + k * 32 + lane;
     if (i < n) {
       stage32[lpos[k]] = (unsigned)(vals_in ? vals_in[i] : i);
-      digit_of[lpos[k]] = (unsigned char)((unsigned)(key[k] >> shift) & 255u);
+      if constexpr (!SYSD) digit_of[lpos[k]] = (unsigned char)((unsigned)(key[k] >> shift) & 255u);
     }
   }
   __syncthreads();
@@ -257,30 +276,54 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_onesweep(
   }
 }
 
-size_t sort_status_words(int n) { return (size_t)sort_tiles(n) * 256 * 8 + 8 + 8 * 256; }
+// digit histograms of the two system-index passes, from the system sizes
+__global__ void __launch_bounds__(256) k_sort_hist_sys(const int* __restrict__ sys_off, int nsys,
+                                                       unsigned* __restrict__ ghist) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nsys; s += gridDim.x * blockDim.x) {
+    const unsigned c = (unsigned)(sys_off[s + 1] - sys_off[s]);
+    atomicAdd(ghist + (s & 255), c);
+    atomicAdd(ghist + 256 + ((s >> 8) & 255), c);
+  }
+}
+
+constexpr int kMaxPasses = 10;  // 8 key bytes + 2 system-index bytes
+
+size_t sort_status_words(int n) { return (size_t)sort_tiles(n) * 256 * kMaxPasses + kMaxPasses + kMaxPasses * 256; }
 
 // Stable sort of n (key, value) pairs; values_in == nullptr means 0..n-1.
 // Result ends in (keys_a, vals_a) after an even number of passes.  work holds
 // sort_status_words(n) unsigned ints: look-back status of every pass, the
-// tile counters and the 8 digit histograms; kStatusSortTimeout is or-ed into
-// *err if a look-back wait hit its bound.
+// tile counters and the digit histograms; kStatusSortTimeout is or-ed into
+// *err if a look-back wait hit its bound.  With nsys > 1 (an ensemble laid
+// out as sys_off), two more passes order by system index, so each system's
+// pairs are sorted by key within the system's own index range, ties in input
+// order: the order each system gets when sorted alone.
 void radix_sort_pairs(unsigned long long* keys_a, unsigned long long* keys_b, int* vals_a, int* vals_b,
-                      const int* vals_in, int n, unsigned* work, int* err, int passes, cudaStream_t s) {
+                      const int* vals_in, int n, unsigned* work, int* err, int passes, const int* sys_off, int nsys,
+                      cudaStream_t s) {
   if (n <= 0) return;
   const int nt = sort_tiles(n);
+  const int sys_passes = nsys > 1 ? 2 : 0;
   unsigned* status = work;
-  unsigned* counters = work + (size_t)nt * 256 * 8;
-  unsigned* ghist = counters + 8;
+  unsigned* counters = work + (size_t)nt * 256 * kMaxPasses;
+  unsigned* ghist = counters + kMaxPasses;
   cudaMemsetAsync(work, 0, sort_status_words(n) * sizeof(unsigned), s);
   k_sort_hist8<<<1184, kSortThreads, 0, s>>>(keys_a, n, passes, ghist);
-  k_sort_hist_scan<<<1, 256, 0, s>>>(ghist, passes);
+  if (sys_passes) k_sort_hist_sys<<<(nsys + 255) / 256, 256, 0, s>>>(sys_off, nsys, ghist + 256 * passes);
+  k_sort_hist_scan<<<1, 256, 0, s>>>(ghist, passes + sys_passes);
   unsigned long long* kin = keys_a;
   unsigned long long* kout = keys_b;
   int* vin = vals_a;
   int* vout = vals_b;
-  for (int p = 0; p < passes; p++) {
-    k_sort_onesweep<<<nt, kSortThreads, 0, s>>>(kin, p == 0 ? vals_in : vin, n, 8 * p, ghist + 256 * p,
-                                                status + (size_t)p * nt * 256, counters + p, kout, vout, err);
+  for (int p = 0; p < passes + sys_passes; p++) {
+    const int* vi = p == 0 ? vals_in : vin;
+    unsigned* stp = status + (size_t)p * nt * 256;
+    if (p < passes)
+      k_sort_onesweep<false><<<nt, kSortThreads, 0, s>>>(kin, vi, n, 8 * p, ghist + 256 * p, stp, counters + p, kout,
+                                                         vout, err, nullptr, 0);
+    else
+      k_sort_onesweep<true><<<nt, kSortThreads, 0, s>>>(kin, vi, n, 8 * (p - passes), ghist + 256 * p, stp,
+                                                        counters + p, kout, vout, err, sys_off, nsys);
     unsigned long long* tk = kin; kin = kout; kout = tk;
     int* tv = vin; vin = vout; vout = tv;
   }

@@ -74,8 +74,11 @@ __device__ __forceinline__ Chain make_chain(const uint8_t* sd, int loc, int i, i
 }
 
 // Loads d for positions [t0-kHalo, t0+kTreeTile+kHalo) into sd, from keys.
+// In an ensemble d = 0 at every system start: a system's first particle
+// starts a level-1 cell, and no run crosses into the next system (the same
+// values d takes at 0 and past n when the system is alone).
 __device__ void load_d_from_keys(const unsigned long long* __restrict__ keys, int n, int t0, uint8_t* sd,
-                                 unsigned long long* sk) {
+                                 unsigned long long* sk, const int* __restrict__ sys_off, int nsys) {
   const int nk = kTreeTile + 2 * kHalo + 1;
   for (int j = threadIdx.x; j < nk; j += blockDim.x) {
     const int g = t0 - kHalo - 1 + j;
@@ -87,19 +90,32 @@ __device__ void load_d_from_keys(const unsigned long long* __restrict__ keys, in
     sd[j] = (p <= 0 || p >= n) ? (uint8_t)0 : (uint8_t)diff_level(sk[j], sk[j + 1]);
   }
   __syncthreads();
+  if (nsys > 1) {
+    const int lo = t0 - kHalo, hi = t0 + kTreeTile + kHalo;
+    // systems whose start lies in [lo, hi): few per tile
+    if (threadIdx.x == 0) {
+      for (int s = sys_of(sys_off, nsys, max(lo, 0)); s < nsys; s++) {
+        const int p = sys_off[s];
+        if (p >= hi) break;
+        if (p >= lo) sd[p - lo] = 0;
+      }
+    }
+    __syncthreads();
+  }
 }
 
 __global__ void __launch_bounds__(kTreeThreads) k_tree_chains(const unsigned long long* __restrict__ keys, int n,
                                                               int nleaf, uint8_t* __restrict__ dlev,
                                                               uint16_t* __restrict__ chain,
                                                               unsigned* __restrict__ hist, int nb,
-                                                              int* __restrict__ status) {
+                                                              int* __restrict__ status,
+                                                              const int* __restrict__ sys_off, int nsys) {
   __shared__ unsigned long long sk[kTreeTile + 2 * kHalo + 1];
   __shared__ uint8_t sd[kTreeTile + 2 * kHalo];
   __shared__ unsigned hc[kNL], hl[kNL];
   const int t0 = blockIdx.x * kTreeTile;
   if (threadIdx.x < kNL) { hc[threadIdx.x] = 0; hl[threadIdx.x] = 0; }
-  load_d_from_keys(keys, n, t0, sd, sk);
+  load_d_from_keys(keys, n, t0, sd, sk, sys_off, nsys);
   for (int j = threadIdx.x; j < kTreeTile; j += blockDim.x)
     if (t0 + j < n) dlev[t0 + j] = sd[kHalo + j];
   bool anyfat = false;
@@ -215,12 +231,14 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_cells(
     const unsigned long long* __restrict__ keys, const uint8_t* __restrict__ dlev,
     const uint16_t* __restrict__ chain, const unsigned* __restrict__ hist, int n, int nleaf, int nb, int cell_cap,
     TreeInfo* __restrict__ info, uint4* __restrict__ cell_data, int* __restrict__ cell_parent,
-    int* __restrict__ leaf_list, int* __restrict__ mp_count) {
+    int* __restrict__ leaf_list, int* __restrict__ mp_count, const int* __restrict__ sys_off, int nsys,
+    int* __restrict__ root_beg) {
   __shared__ uint8_t sd[kTreeTile + 2 * kHalo];
   __shared__ uint16_t cpre[kNL][kTreeThreads];
   __shared__ uint16_t lpre[kNL][kTreeThreads];
   __shared__ unsigned boff[2][kNL];
   if (info->ncells > cell_cap || info->nleaves > cell_cap) return;
+  if (nsys > 1 && blockIdx.x == 0 && threadIdx.x == 0) root_beg[nsys] = info->level_end[1];
   const int t0 = blockIdx.x * kTreeTile;
   for (int j = threadIdx.x; j < kTreeTile + 2 * kHalo; j += blockDim.x) {
     const int p = t0 - kHalo + j;
@@ -299,11 +317,17 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_cells(
           if ((int)sd[loc + j] <= L) { pend = i + j; small_leaf = true; break; }
         }
       }
-      if (!small_leaf) pend = gallop_u64(keys, min(i + nleaf + 1, n), n, (pre + 1ull) << sh);
+      if (!small_leaf) {
+        // keys increase only inside a system: search up to the system's end
+        const int send = nsys > 1 ? sys_off[sys_of(sys_off, nsys, i) + 1] : n;
+        pend = gallop_u64(keys, min(i + nleaf + 1, send), send, (pre + 1ull) << sh);
+      }
       uint4* cd = cell_data + cidx;
       if (L == 1) {
         cd->x = (unsigned)(1 << 27);  // level-1 cells: parent 0, as the reference stores them
         cell_parent[cidx] = -1;
+        // a system's first level-1 cell starts at the system's first particle
+        if (nsys > 1 && sd[loc] == 0) root_beg[sys_of(sys_off, nsys, i)] = cidx;
       }
       unsigned ywd = 0xFFFFFFFFu;
       if (!leaf) {
@@ -333,12 +357,14 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_cells(
 
 void build_tree(const unsigned long long* sorted_keys, int n, int nleaf, int cell_cap, int leaf_cap,
                 uint8_t* dlev, uint16_t* chain, unsigned* hist, TreeInfo* info, uint4* cell_data,
-                int* cell_parent, int* leaf_list, int* mp_count, cudaStream_t s) {
+                int* cell_parent, int* leaf_list, int* mp_count, const int* sys_off, int nsys, int* root_beg,
+                cudaStream_t s) {
   const int nb = tree_tiles(n);
-  k_tree_chains<<<nb, kTreeThreads, 0, s>>>(sorted_keys, n, nleaf, dlev, chain, hist, nb, &info->status);
+  k_tree_chains<<<nb, kTreeThreads, 0, s>>>(sorted_keys, n, nleaf, dlev, chain, hist, nb, &info->status, sys_off,
+                                            nsys);
   k_tree_scan<<<1, 1024, 0, s>>>(hist, nb, cell_cap, leaf_cap, info);
   k_tree_cells<<<nb, kTreeThreads, 0, s>>>(sorted_keys, dlev, chain, hist, n, nleaf, nb, cell_cap, info, cell_data,
-                                           cell_parent, leaf_list, mp_count);
+                                           cell_parent, leaf_list, mp_count, sys_off, nsys, root_beg);
 }
 
 }  // namespace bonsai

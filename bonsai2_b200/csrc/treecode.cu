@@ -92,6 +92,17 @@ struct Handle {
   int direct_cap = 0;
   int box_blocks = 0, move_blocks = 0;
   int cur_nleaf = 16, cur_ncrit = 64, cur_ls = 5;
+  int walk_layout = 0;  // walk_variant layout: 0 half-warp pairs where nCrit <= 64, 1 full warp
+  // ensemble layout (nsys > 1): system s owns particles [off[s], off[s+1]) of
+  // the state; every stage works per system in the same launches
+  int nsys = 1, nchunks = 0;
+  int *sys_off = nullptr, *chunk_beg = nullptr, *root_beg = nullptr;
+  int4* chunks = nullptr;
+  Box* sys_box = nullptr;
+  float* sys_box_part = nullptr;
+  unsigned *seg_beg = nullptr, *seg_end = nullptr, *nseg = nullptr;
+  double *chunk_energy = nullptr, *sys_energy = nullptr;
+  const int* so() const { return nsys > 1 ? sys_off : nullptr; }
   // stage bookkeeping for the eager API
   bool built = false, mp_done = false, grouped = false, forced = false, moved_after_forces = false;
   bool ever_built = false, ever_mp = false;  // the cell arrays hold a tree / multipoles
@@ -109,8 +120,16 @@ struct Handle {
     graph_ok = false;
   }
 
+  void release_systems() {
+    dfree(&sys_off); dfree(&chunk_beg); dfree(&root_beg); dfree(&chunks); dfree(&sys_box); dfree(&sys_box_part);
+    dfree(&seg_beg); dfree(&seg_end); dfree(&nseg); dfree(&chunk_energy); dfree(&sys_energy);
+    nsys = 1;
+    nchunks = 0;
+  }
+
   void release_particles() {
     release_graphs();
+    release_systems();
     for (int p = 0; p < 2; p++) { dfree(&pos[p]); dfree(&vel[p]); dfree(&id[p]); }
     dfree(&acc); dfree(&jpos); dfree(&tkey); dfree(&pkey); dfree(&kalt);
     dfree(&tperm); dfree(&pperm); dfree(&valt); dfree(&sort_counts); dfree(&bsum);
@@ -213,7 +232,8 @@ struct Handle {
     BONSAI_CUDA_TRY(dalloc(&pperm, N));
     BONSAI_CUDA_TRY(dalloc(&valt, N));
     BONSAI_CUDA_TRY(dalloc(&sort_counts, sort_status_words(nn)));
-    const int scan_m = std::max(256 * sort_tiles(nn), 1 << (3 * kMaxLevelSplit));
+    // scans: group counts per bin (8^7), and per position for ensembles (n)
+    const int scan_m = std::max(std::max(256 * sort_tiles(nn), 1 << (3 * kMaxLevelSplit)), nn);
     BONSAI_CUDA_TRY(dalloc(&bsum, (size_t)scan_blocks(scan_m) + 1));
     BONSAI_CUDA_TRY(dalloc(&dlev, N));
     BONSAI_CUDA_TRY(dalloc(&chain, N));
@@ -234,6 +254,48 @@ struct Handle {
     return 0;
   }
 
+  // ensemble layout from the per-system particle counts (all >= 1)
+  int set_systems(const int* counts, int ns) {
+    long long tot = 0;
+    for (int k = 0; k < ns; k++) {
+      if (counts[k] < 1) return BONSAI_ERR_ARG;
+      tot += counts[k];
+    }
+    if (tot > (long long)0x7fffffff - kChunk) return BONSAI_ERR_ARG;
+    int rc = alloc((int)tot);
+    if (rc) return rc;
+    if (ns == 1) return 0;
+    std::vector<int> off(ns + 1), cbeg(ns + 1);
+    std::vector<int4> ch;
+    off[0] = 0;
+    for (int k = 0; k < ns; k++) {
+      off[k + 1] = off[k] + counts[k];
+      cbeg[k] = (int)ch.size();
+      for (int b = off[k]; b < off[k + 1]; b += kChunk) ch.push_back(make_int4(b, std::min(b + kChunk, off[k + 1]), k, 0));
+    }
+    cbeg[ns] = (int)ch.size();
+    nsys = ns;
+    nchunks = (int)ch.size();
+    BONSAI_CUDA_TRY(dalloc(&sys_off, (size_t)ns + 1));
+    BONSAI_CUDA_TRY(dalloc(&chunk_beg, (size_t)ns + 1));
+    BONSAI_CUDA_TRY(dalloc(&root_beg, (size_t)ns + 1));
+    BONSAI_CUDA_TRY(dalloc(&chunks, (size_t)nchunks));
+    BONSAI_CUDA_TRY(dalloc(&sys_box, (size_t)ns));
+    BONSAI_CUDA_TRY(dalloc(&sys_box_part, (size_t)nchunks * 6));
+    BONSAI_CUDA_TRY(dalloc(&seg_beg, (size_t)n));
+    BONSAI_CUDA_TRY(dalloc(&seg_end, (size_t)n));
+    BONSAI_CUDA_TRY(dalloc(&nseg, 1));
+    BONSAI_CUDA_TRY(dalloc(&chunk_energy, (size_t)nchunks * 8));
+    BONSAI_CUDA_TRY(dalloc(&sys_energy, (size_t)ns * 8));
+    BONSAI_CUDA_TRY(cudaMemcpy(sys_off, off.data(), (ns + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    BONSAI_CUDA_TRY(cudaMemcpy(chunk_beg, cbeg.data(), (ns + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    BONSAI_CUDA_TRY(cudaMemcpy(chunks, ch.data(), ch.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    BONSAI_CUDA_TRY(cudaMemset(sys_energy, 0, (size_t)ns * 8 * sizeof(double)));
+    BONSAI_CUDA_TRY(cudaMemset(root_beg, 0, (size_t)(ns + 1) * sizeof(int)));
+    theta_mode = 0;  // per-group angles are a single-system feature
+    return 0;
+  }
+
   // eager build that grows the cell arrays until the tree fits
   int build_checked(int nleaf) {
     for (int attempt = 0; attempt < 4; attempt++) {
@@ -251,27 +313,39 @@ struct Handle {
 
   // ---------------- stages (enqueue only) ----------------
   void enq_build(int nleaf) {
-    cudaMemsetAsync(box_ticket, 0, sizeof(unsigned), st);
-    k_box<<<box_blocks, 256, 0, st>>>(pos[par], n, box_partial, box_ticket, box, &info->status);
-    k_keys<<<nsm * 8, 256, 0, st>>>(pos[par], n, box, ph_table, tkey, pkey);
-    radix_sort_pairs(tkey, kalt, tperm, valt, nullptr, n, sort_counts, &info->status, 8, st);
+    if (nsys > 1) {
+      launch_sys_keys(pos[par], chunks, nchunks, chunk_beg, nsys, sys_box_part, sys_box, ph_table, tkey, pkey,
+                      &info->status, nsm * 8, st);
+    } else {
+      cudaMemsetAsync(box_ticket, 0, sizeof(unsigned), st);
+      k_box<<<box_blocks, 256, 0, st>>>(pos[par], n, box_partial, box_ticket, box, &info->status);
+      k_keys<<<nsm * 8, 256, 0, st>>>(pos[par], n, box, ph_table, tkey, pkey);
+    }
+    radix_sort_pairs(tkey, kalt, tperm, valt, nullptr, n, sort_counts, &info->status, 8, so(), nsys, st);
     k_gather_pos<<<nsm * 8, 256, 0, st>>>(tperm, n, pos[par], jpos);
     build_tree(tkey, n, nleaf, cap_cells, cap_cells, dlev, chain, hist, info, cell_data, cell_parent, leaf_list,
-               mp_count, st);
+               mp_count, so(), nsys, root_beg, st);
   }
   void enq_multipoles() {
     k_multipoles<<<nsm * 8, 256, 0, st>>>(leaf_list, info, cell_data, cell_parent, jpos, 1.0f / prm.theta, rec,
                                           cell_open, cell_q0, cell_q1, cell_ls, mp_count, cap_cells);
   }
   void enq_groups(int ls, int ncrit) {
-    radix_sort_pairs(pkey, kalt, pperm, valt, nullptr, n, sort_counts, &info->status, 8, st);
-    make_groups(pkey, n, ls, ncrit, g_count, g_seg, g_ng, bsum, groups, theta_mode ? gcap : n, info, st);
+    radix_sort_pairs(pkey, kalt, pperm, valt, nullptr, n, sort_counts, &info->status, 8, so(), nsys, st);
+    if (nsys > 1) {
+      // kalt (8 bytes per particle) is free after the sort: segment flags and indices
+      unsigned* flag = reinterpret_cast<unsigned*>(kalt);
+      make_groups_sys(pkey, n, ls, ncrit, sys_off, nsys, flag, flag + n, seg_beg, seg_end, nseg, bsum, groups, n, info,
+                      st);
+    } else {
+      make_groups(pkey, n, ls, ncrit, g_count, g_seg, g_ng, bsum, groups, theta_mode ? gcap : n, info, st);
+    }
     const int q = par ^ 1;
     k_gather_state<<<nsm * 8, 256, 0, st>>>(pperm, n, pos[par], vel[par], id[par], pos[q], vel[q], id[q]);
     par = q;
   }
   void enq_forces(int ncrit) {
-    const int k = walk_variant(ncrit);
+    const int k = walk_variant(ncrit, walk_layout);
     cudaMemsetAsync(group_counter, 0, sizeof(unsigned), st);
     cudaMemsetAsync(stats, 0, 4 * sizeof(unsigned long long), st);
     const float* ginv = nullptr;
@@ -283,7 +357,8 @@ struct Handle {
       ginv = group_inv;
     }
     launch_walk(k, walk_blocks[k], groups, info, pos[par], jpos, cell_data, cell_open, cell_q0, cell_q1, cell_ls,
-                ginv, prm.eps * prm.eps, acc, ring, kRingCap, group_counter, stats, &info->status, st);
+                ginv, prm.eps * prm.eps, acc, ring, kRingCap, group_counter, stats, &info->status, so(), nsys, root_beg,
+                st);
   }
   void enq_move(bool write) {
     launch_move_wrapper(write);
@@ -353,6 +428,84 @@ struct Handle {
     return 0;
   }
 
+  // Times `steps` graph steps (after one warm-up step) of every candidate
+  // (nLeaf, nCrit, walk layout) on the current particles, restoring them
+  // before each trial and at the end, and keeps the fastest.
+  int autotune(const int* nl, int nnl, const int* nc, int nnc, int steps, float* results, int* best) {
+    const size_t N = (size_t)n;
+    float4 *sp = nullptr, *sv = nullptr;
+    int* si = nullptr;
+    int closing0 = 0;
+    BONSAI_CUDA_TRY(dalloc(&sp, N));
+    BONSAI_CUDA_TRY(dalloc(&sv, N));
+    BONSAI_CUDA_TRY(dalloc(&si, N));
+    BONSAI_CUDA_TRY(cudaMemcpyAsync(sp, pos[par], N * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+    BONSAI_CUDA_TRY(cudaMemcpyAsync(sv, vel[par], N * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+    BONSAI_CUDA_TRY(cudaMemcpyAsync(si, id[par], N * sizeof(int), cudaMemcpyDeviceToDevice, st));
+    BONSAI_CUDA_TRY(cudaMemcpyAsync(&closing0, closing, sizeof(int), cudaMemcpyDeviceToHost, st));
+    BONSAI_CUDA_TRY(cudaStreamSynchronize(st));
+    auto restore = [&]() -> int {
+      BONSAI_CUDA_TRY(cudaMemcpyAsync(pos[par], sp, N * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+      BONSAI_CUDA_TRY(cudaMemcpyAsync(vel[par], sv, N * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+      BONSAI_CUDA_TRY(cudaMemcpyAsync(id[par], si, N * sizeof(int), cudaMemcpyDeviceToDevice, st));
+      BONSAI_CUDA_TRY(cudaMemcpyAsync(closing, &closing0, sizeof(int), cudaMemcpyHostToDevice, st));
+      return 0;
+    };
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    BONSAI_CUDA_TRY(cudaEventCreate(&e0));
+    BONSAI_CUDA_TRY(cudaEventCreate(&e1));
+    float best_ms = 3.0e38f;
+    int bl = cur_nleaf, bc = cur_ncrit, blay = walk_layout;
+    int rc = 0;
+    for (int lay = 0; lay < 2 && rc >= 0; lay++)
+      for (int a = 0; a < nnl && rc >= 0; a++)
+        for (int b = 0; b < nnc && rc >= 0; b++) {
+          const int idx = (lay * nnl + a) * nnc + b;
+          if (results) results[idx] = -1.0f;
+          if (nl[a] < 1 || nl[a] > 64 || nc[b] < 1 || nc[b] > 128) continue;
+          if (lay == 0 && nc[b] > 64) continue;  // no half-warp layout above 64: same as layout 1
+          rc = restore();
+          if (rc) break;
+          cur_nleaf = nl[a];
+          cur_ncrit = nc[b];
+          walk_layout = lay;
+          release_graphs();
+          rc = build_checked(cur_nleaf);
+          if (rc > 0) { rc = read_status(true) < 0 ? -1 : 0; continue; }
+          if (rc) break;
+          rc = capture_graphs();
+          if (rc) break;
+          rc = launch_graph_step(nullptr);
+          if (rc) break;
+          cudaEventRecord(e0, st);
+          for (int k = 0; k < steps && !rc; k++) rc = launch_graph_step(nullptr);
+          cudaEventRecord(e1, st);
+          if (rc) break;
+          const int status = read_status(true);
+          if (status < 0) { rc = status; break; }
+          float ms = 0.f;
+          cudaEventElapsedTime(&ms, e0, e1);
+          if (status != 0) continue;
+          ms /= (float)steps;
+          if (results) results[idx] = ms;
+          if (ms < best_ms) { best_ms = ms; bl = cur_nleaf; bc = cur_ncrit; blay = lay; }
+        }
+    if (rc >= 0) rc = restore();
+    if (rc >= 0) rc = (int)cudaStreamSynchronize(st) == 0 ? 0 : -1000 - (int)cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    dfree(&sp); dfree(&sv); dfree(&si);
+    cur_nleaf = bl;
+    cur_ncrit = bc;
+    walk_layout = blay;
+    prm.nleaf = bl;
+    prm.ncrit = bc;
+    release_graphs();
+    built = mp_done = grouped = forced = moved_after_forces = false;
+    if (best) { best[0] = bl; best[1] = bc; best[2] = blay; }
+    return rc;
+  }
+
   int read_status(bool clear) {
     int s = 0;
     cudaError_t e = cudaMemcpyAsync(&s, &info->status, sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -367,8 +520,12 @@ struct Handle {
 };
 
 void Handle::launch_move_wrapper(bool write) {
-  launch_move(pos[par], vel[par], acc, n, prm.dt, closing, prm.eps, write ? 1 : 0, move_partial, move_blocks,
-              move_ticket, energies, st);
+  if (nsys > 1)
+    launch_move_sys(pos[par], vel[par], acc, chunks, nchunks, chunk_beg, nsys, prm.dt, closing, prm.eps, write ? 1 : 0,
+                    chunk_energy, move_blocks, move_ticket, energies, sys_energy, st);
+  else
+    launch_move(pos[par], vel[par], acc, n, prm.dt, closing, prm.eps, write ? 1 : 0, move_partial, move_blocks,
+                move_ticket, energies, st);
 }
 
 Handle* H(bonsai_handle h) { return reinterpret_cast<Handle*>(h); }
@@ -645,6 +802,47 @@ int bonsai_step_timed(bonsai_handle hh, int nsteps, float* phase_ms) {
   return rc ? rc : last_cuda();
 }
 
+int bonsai_set_systems(bonsai_handle hh, const int* counts, int nsys) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (!counts || nsys < 1 || nsys > 65536) return BONSAI_ERR_ARG;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  return h->set_systems(counts, nsys);
+}
+
+int bonsai_get_system_energies(bonsai_handle hh, double* out) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (h->n == 0) return BONSAI_ERR_NOT_ALLOCATED;
+  if (!h->forced) return BONSAI_ERR_ORDER;
+  if (!out) return BONSAI_ERR_ARG;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  if (!h->moved_after_forces) h->enq_move(false);
+  const double* src = h->nsys > 1 ? h->sys_energy : h->energies;
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(out, src, (size_t)h->nsys * 8 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  return last_cuda();
+}
+
+int bonsai_set_walk_layout(bonsai_handle hh, int layout) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (layout < 0 || layout > 1) return BONSAI_ERR_ARG;
+  h->walk_layout = layout;
+  h->release_graphs();
+  return 0;
+}
+
+int bonsai_autotune(bonsai_handle hh, const int* nleaf, int n_nleaf, const int* ncrit, int n_ncrit, int steps,
+                    float* results, int* best) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (h->n == 0) return BONSAI_ERR_NOT_ALLOCATED;
+  if (!nleaf || !ncrit || n_nleaf < 1 || n_ncrit < 1 || steps < 1) return BONSAI_ERR_ARG;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  return h->autotune(nleaf, n_nleaf, ncrit, n_ncrit, steps, results, best);
+}
+
 int bonsai_graph_kernel_count(bonsai_handle hh) {
   Handle* h = H(hh);
   if (!h) return BONSAI_ERR_HANDLE;
@@ -728,7 +926,8 @@ int bonsai_get_box(bonsai_handle hh, float* box4) {
   if (!h) return BONSAI_ERR_HANDLE;
   if (!box4) return BONSAI_ERR_ARG;
   BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
-  BONSAI_CUDA_TRY(cudaMemcpyAsync(box4, h->box, 4 * sizeof(float), cudaMemcpyDeviceToHost, h->st));
+  const Box* b = h->nsys > 1 ? h->sys_box : h->box;  // an ensemble's first system
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(box4, b, 4 * sizeof(float), cudaMemcpyDeviceToHost, h->st));
   BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
   return 0;
 }
@@ -833,7 +1032,11 @@ int bonsai_direct_fp64(bonsai_handle hh, const int* sample, int ns, int include_
   k_scatter_by_id<<<h->nsm * 8, 256, 0, h->st>>>(h->id[h->par], h->n, h->pos[h->par], tmp);
   BONSAI_CUDA_TRY(cudaMemcpyAsync(h->direct_sample, sample, (size_t)ns * 4, cudaMemcpyHostToDevice, h->st));
   const double e2 = (double)h->prm.eps * (double)h->prm.eps;
-  launch_direct_fp64(tmp, h->n, h->direct_sample, ns, e2, include_self, h->direct_part, nsplit, h->direct_out, h->st);
+  if (h->nsys > 1)
+    launch_direct_fp64_sys(tmp, h->sys_off, h->nsys, h->direct_sample, ns, e2, include_self, h->direct_out, h->st);
+  else
+    launch_direct_fp64(tmp, h->n, h->direct_sample, ns, e2, include_self, h->direct_part, nsplit, h->direct_out,
+                       h->st);
   BONSAI_CUDA_TRY(cudaMemcpyAsync(out, h->direct_out, (size_t)ns * 4 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
   BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
   return last_cuda();
@@ -844,6 +1047,7 @@ int bonsai_set_theta_mode(bonsai_handle hh, int mode, float lo, float hi) {
   if (!h) return BONSAI_ERR_HANDLE;
   if (mode < 0 || mode > 2 || !(lo > 0.f) || !(hi >= lo)) return BONSAI_ERR_ARG;
   if (mode == 1 && !h->mlp_loaded) return BONSAI_ERR_ORDER;
+  if (mode != 0 && h->nsys > 1) return BONSAI_ERR_ARG;  // per-group angles: single systems only
   h->theta_mode = mode;
   h->theta_lo = lo;
   h->theta_hi = hi;

@@ -122,7 +122,10 @@ __device__ __forceinline__ int find_src(int incl, int s) {
 // group_inv_theta); the opening size is re-formed as (l/theta_g + s)^2 from
 // cell_ls with the same rounding as the multipole kernel, so theta_g = theta
 // reproduces the fixed-angle walk exactly.
-template <int NI, bool SPLIT, bool PERGROUP>
+// ENS: the particles form an ensemble of independent systems (sys_off); a
+// group walks from its own system's level-1 cells [root_beg[s], root_beg[s+1])
+// only, in the order the system alone would.
+template <int NI, bool SPLIT, bool PERGROUP, bool ENS>
 __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
     k_walk(const int2* __restrict__ groups, const TreeInfo* __restrict__ info, const float4* __restrict__ ipos,
            const float4* __restrict__ jpos, const uint4* __restrict__ cell_data,
@@ -130,7 +133,8 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
            const float4* __restrict__ cell_q1, const float2* __restrict__ cell_ls,
            const float* __restrict__ group_inv_theta, float eps2, float4* __restrict__ acc,
            int* __restrict__ ring_pool, int ring_cap, unsigned* __restrict__ group_counter,
-           unsigned long long* __restrict__ stats, int* __restrict__ status) {
+           unsigned long long* __restrict__ stats, int* __restrict__ status, const int* __restrict__ sys_off,
+           int nsys, const int* __restrict__ root_beg) {
   constexpr int STRIDE = SPLIT ? 16 : 32;
   constexpr int JSTEP = SPLIT ? 2 : 1;
   __shared__ float4 s_a0[kWalkWarps][64];
@@ -146,7 +150,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
   int* lists = ring_pool + (size_t)(blockIdx.x * kWalkWarps + w) * (size_t)ring_cap;
   const int half_cap = ring_cap >> 1;
   const int ngroups = info->ngroups;
-  const int l1b = info->level_beg[1], l1e = info->level_end[1];
+  int l1b = info->level_beg[1], l1e = info->level_end[1];
   const unsigned lt = lanemask_lt();
   unsigned long long sum_app = 0, sum_dir = 0;
   unsigned max_app = 0, max_dir = 0;
@@ -159,6 +163,11 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
     const int2 gd = groups[g];
     const int pbeg = gd.x, np = gd.y;
     const float inv_theta_g = PERGROUP ? group_inv_theta[g] : 0.0f;
+    if (ENS) {
+      const int sy = sys_of(sys_off, nsys, pbeg);
+      l1b = __ldg(root_beg + sy);
+      l1e = __ldg(root_beg + sy + 1);
+    }
     IPart pi[NI];
     float4 ai[NI];
     float mnx = 3.0e38f, mny = 3.0e38f, mnz = 3.0e38f, mxx = -3.0e38f, mxy = -3.0e38f, mxz = -3.0e38f;
@@ -334,22 +343,29 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
 }
 
 // variants: 0..2 half-warp split with NI = 1, 2, 4 (nCrit <= 16, 32, 64);
-// 3..5 full warp with NI = 1, 2, 4 (nCrit <= 32, 64, 128)
-int walk_variant(int ncrit) {
+// 3..5 full warp with NI = 1, 2, 4 (nCrit <= 32, 64, 128).  layout 0: split
+// where nCrit <= 64 (the default); 1: full warp.
+int walk_variant(int ncrit, int layout) {
 #if BONSAI_WALK_SPLIT
-  if (ncrit <= 64) return ncrit <= 16 ? 0 : (ncrit <= 32 ? 1 : 2);
+  if (ncrit <= 64 && layout != 1) return ncrit <= 16 ? 0 : (ncrit <= 32 ? 1 : 2);
 #endif
   return ncrit <= 32 ? 3 : (ncrit <= 64 ? 4 : 5);
 }
 
 template <int NI, bool SPLIT>
 static int occupancy_of() {
-  int nb = 0, nb2 = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_walk<NI, SPLIT, false>, kWalkThreads, 0) != cudaSuccess)
+  int nb = 0, nb2 = 0, nb3 = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_walk<NI, SPLIT, false, false>, kWalkThreads, 0) !=
+      cudaSuccess)
     nb = 1;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb2, k_walk<NI, SPLIT, true>, kWalkThreads, 0) != cudaSuccess)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb2, k_walk<NI, SPLIT, true, false>, kWalkThreads, 0) !=
+      cudaSuccess)
     nb2 = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb3, k_walk<NI, SPLIT, false, true>, kWalkThreads, 0) !=
+      cudaSuccess)
+    nb3 = 1;
   nb = nb < nb2 ? nb : nb2;
+  nb = nb < nb3 ? nb : nb3;
   return nb < 1 ? 1 : nb;
 }
 
@@ -370,17 +386,18 @@ void launch_walk(int variant, int nblocks, const int2* groups, const TreeInfo* i
                  const float4* jpos, const uint4* cell_data, const float4* cell_open, const float4* cell_q0,
                  const float4* cell_q1, const float2* cell_ls, const float* group_inv_theta, float eps2,
                  float4* acc, int* ring_pool, int ring_cap, unsigned* group_counter, unsigned long long* stats,
-                 int* status, cudaStream_t s) {
-#define BONSAI_WALK(NI, SP)                                                                                        \
-  do {                                                                                                             \
-    if (group_inv_theta)                                                                                           \
-      k_walk<NI, SP, true><<<nblocks, kWalkThreads, 0, s>>>(groups, info, ipos, jpos, cell_data, cell_open,         \
-                                                            cell_q0, cell_q1, cell_ls, group_inv_theta, eps2, acc,  \
-                                                            ring_pool, ring_cap, group_counter, stats, status);    \
-    else                                                                                                           \
-      k_walk<NI, SP, false><<<nblocks, kWalkThreads, 0, s>>>(groups, info, ipos, jpos, cell_data, cell_open,        \
-                                                             cell_q0, cell_q1, cell_ls, nullptr, eps2, acc,         \
-                                                             ring_pool, ring_cap, group_counter, stats, status);   \
+                 int* status, const int* sys_off, int nsys, const int* root_beg, cudaStream_t s) {
+#define BONSAI_WALK_ARGS                                                                                          \
+  groups, info, ipos, jpos, cell_data, cell_open, cell_q0, cell_q1, cell_ls, group_inv_theta, eps2, acc, ring_pool, \
+      ring_cap, group_counter, stats, status, sys_off, nsys, root_beg
+#define BONSAI_WALK(NI, SP)                                                                \
+  do {                                                                                     \
+    if (nsys > 1)                                                                          \
+      k_walk<NI, SP, false, true><<<nblocks, kWalkThreads, 0, s>>>(BONSAI_WALK_ARGS);      \
+    else if (group_inv_theta)                                                              \
+      k_walk<NI, SP, true, false><<<nblocks, kWalkThreads, 0, s>>>(BONSAI_WALK_ARGS);      \
+    else                                                                                   \
+      k_walk<NI, SP, false, false><<<nblocks, kWalkThreads, 0, s>>>(BONSAI_WALK_ARGS);     \
   } while (0)
   switch (variant) {
 #if BONSAI_WALK_SPLIT
@@ -393,6 +410,7 @@ void launch_walk(int variant, int nblocks, const int2* groups, const TreeInfo* i
     default: BONSAI_WALK(4, false); break;
   }
 #undef BONSAI_WALK
+#undef BONSAI_WALK_ARGS
 }
 
 }  // namespace bonsai

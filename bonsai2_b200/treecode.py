@@ -137,6 +137,42 @@ class Treecode:
         self.h_ptclPos = np.zeros((n, 4), np.float32)
         self.h_ptclVel = np.zeros((n, 4), np.float32)
 
+    def set_systems(self, counts):
+        """Ensemble layout: system s owns counts[s] consecutive particles of
+        h_ptclPos/h_ptclVel (no counterpart in the reference, which holds one
+        tree per process).  Allocates like alloc(sum(counts))."""
+        c = np.ascontiguousarray(counts, np.int32)
+        _check(self._L.bonsai_set_systems(self._h, _p(c), c.shape[0]), "bonsai_set_systems")
+        n = int(c.sum())
+        self.nPtcl = n
+        self.nsys = int(c.shape[0])
+        self.h_ptclPos = np.zeros((n, 4), np.float32)
+        self.h_ptclVel = np.zeros((n, 4), np.float32)
+
+    def system_energies(self) -> np.ndarray:
+        """(nsys, 8) energies per system, columns as computeEnergies."""
+        ns = getattr(self, "nsys", 1)
+        e = np.empty((ns, 8), np.float64)
+        _check(self._L.bonsai_get_system_energies(self._h, _p(e)), "bonsai_get_system_energies")
+        return e
+
+    def set_walk_layout(self, layout: int):
+        """0: two half-warps per group (nCrit <= 64), 1: one warp per group."""
+        _check(self._L.bonsai_set_walk_layout(self._h, layout), "bonsai_set_walk_layout")
+
+    def autotune(self, nleaf=(8, 16, 32), ncrit=(16, 32, 64, 128), steps: int = 2) -> dict:
+        """Times every (layout, nLeaf, nCrit) candidate on the current
+        particles (restored afterwards) and keeps the fastest."""
+        nl = np.ascontiguousarray(nleaf, np.int32)
+        nc = np.ascontiguousarray(ncrit, np.int32)
+        res = np.empty((2, nl.shape[0], nc.shape[0]), np.float32)
+        best = np.zeros(3, np.int32)
+        _check(self._L.bonsai_autotune(self._h, _p(nl), nl.shape[0], _p(nc), nc.shape[0], steps, _p(res), _p(best)),
+               "bonsai_autotune")
+        self.nLeaf, self.nCrit = int(best[0]), int(best[1])
+        self._params.nleaf, self._params.ncrit = self.nLeaf, self.nCrit
+        return {"nleaf": int(best[0]), "ncrit": int(best[1]), "layout": int(best[2]), "ms": res}
+
     def ptcl_h2d(self):
         pos = np.ascontiguousarray(self.h_ptclPos, np.float32)
         vel = np.ascontiguousarray(self.h_ptclVel, np.float32)

@@ -195,6 +195,44 @@ int bonsai_mlp_train(int device, const float *X, const float *y, int S, float *w
                      float hi, float over, double *loss);
 int bonsai_mlp_predict(int device, const float *X, int S, const float *w, float lo, float hi, float *theta);
 
+/* ---- Ensembles of independent systems (batching) ----
+ * No counterpart in the reference, which holds one tree per process (its stage
+ * state lives in file-scope device globals, buildTree.cu:23-36).
+ * bonsai_set_systems lays the handle's particles out as nsys independent
+ * systems: system s owns the counts[s] >= 1 particles that follow system
+ * s-1's in the arrays given to bonsai_set_particles.  It allocates like
+ * bonsai_alloc(h, sum of counts); bonsai_alloc and a bonsai_set_particles
+ * with another n return to one system.  Every stage then treats each system
+ * as if it were alone (own box, keys, tree and groups; no force between
+ * systems) in the same kernel launches for all systems, so the positions,
+ * velocities and accelerations of each system are bit-identical to those of a
+ * handle that holds that system alone with the same parameters.
+ * bonsai_compute_energies then sums over all systems; bonsai_get_box returns
+ * system 0's box; bonsai_direct_fp64 sums inside each sample's system.
+ * Per-group opening angles (bonsai_set_theta_mode != 0) are for single
+ * systems only (BONSAI_ERR_ARG).  nsys <= 65536. */
+int bonsai_set_systems(bonsai_handle h, const int *counts, int nsys);
+/* energies of every system, 8 doubles per system in the layout and with the
+ * timing rules of bonsai_compute_energies (a single system: its 8 values) */
+int bonsai_get_system_energies(bonsai_handle h, double *out);
+/* walk thread layout, the analogue of the reference's warps-per-group
+ * choice (NWARPS_OCTREE2 / NI, computeForces.cu:475-619): 0 (default) = two
+ * half-warps per group, each holding all the group's particles and taking
+ * alternate sources (nCrit <= 64; above that as 1); 1 = one warp per group,
+ * one lane per particle slot. */
+int bonsai_set_walk_layout(bonsai_handle h, int layout);
+/* Autotuner (no counterpart in the reference): on the handle's current
+ * particles, for every walk layout L in {0, 1}, nleaf[a] and ncrit[b],
+ * builds, captures and times one warm-up plus `steps` graph steps, restoring
+ * the particles before each trial and at the end.  results (optional,
+ * 2 * n_nleaf * n_ncrit floats, index (L*n_nleaf + a)*n_ncrit + b) receives
+ * ms per step, or -1 for a skipped or failed candidate (layout 0 with
+ * nCrit > 64, a value out of range, a device status).  The fastest candidate
+ * becomes the handle's nLeaf / nCrit / layout; best (optional, 3 ints)
+ * receives them.  Allocates a copy of the particle state while it runs. */
+int bonsai_autotune(bonsai_handle h, const int *nleaf, int n_nleaf, const int *ncrit, int n_ncrit, int steps,
+                    float *results, int *best);
+
 /* Plummer sphere initial conditions on the host: the algorithm of
  * code/plummer.h:9-138 (glibc rand(), same stream), converted to float4 like
  * treecode.cu:65-87: pos4 = (x,y,z,m), vel4 = (vx,vy,vz,m).  n >= 1. */

@@ -1,0 +1,175 @@
+"""Ensembles of independent systems (batching form): every system advanced in
+the same launches must give, bit for bit, what the system gives alone.
+
+The single-system path is itself pinned to the oracle (test_gpu_parity.py),
+so bit-identity with it carries that parity over to every system of an
+ensemble.  Edge systems of 1 and 2 particles are included."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+PARAMS = dict(eps=0.01, theta=0.5, nleaf=16, ncrit=64, level_split=5, dt=1.0 / 64)
+
+
+def _ensemble_inputs(counts, seed=777):
+    from bonsai2_b200.ensemble import plummer_ensemble
+    return plummer_ensemble(counts, base_seed=seed)
+
+
+def _offsets(counts):
+    return np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+
+
+def _run(t, pos, vel, steps, eager):
+    t.h_ptclPos[:] = pos
+    t.h_ptclVel[:] = vel
+    t.ptcl_h2d()
+    stats = None
+    if eager:
+        for _ in range(steps):
+            t.buildTree(t.nLeaf)
+            t.computeMultipoles()
+            t.makeGroups(5, t.nCrit)
+            stats = t.computeForces(True)
+            t.moveParticles()
+    else:
+        t.step(steps, graph=True)
+    assert t.synchronize() == 0
+    t.ptcl_d2h()
+    return t.h_ptclPos.copy(), t.h_ptclVel.copy(), t.get_acc(), stats
+
+
+def _alone(pos, vel, steps, eager, params=PARAMS, layout=0):
+    import bonsai2_b200 as B
+    t = B.Treecode(**params)
+    t.set_walk_layout(layout)
+    t.alloc(pos.shape[0])
+    out = _run(t, pos, vel, steps, eager)
+    e = t.computeEnergies()
+    t.close()
+    return out, e
+
+
+@pytest.mark.parametrize("eager", [False, True])
+def test_ensemble_bit_identical_to_alone(eager):
+    import bonsai2_b200 as B
+    from bonsai2_b200.ensemble import system_sizes
+    counts = np.concatenate([[1, 2, 17], system_sizes(13, 1 << 8, 1 << 14, seed=5)]).astype(np.int32)
+    pos, vel = _ensemble_inputs(counts)
+    steps = 3
+    t = B.Treecode(**PARAMS)
+    t.set_systems(counts)
+    p, v, a, stats = _run(t, pos, vel, steps, eager)
+    es = t.system_energies()
+    off = _offsets(counts)
+    sum_app = sum_dir = 0
+    for s in range(len(counts)):
+        b, e = off[s], off[s + 1]
+        (pa, va, aa, st), ea = _alone(pos[b:e], vel[b:e], steps, eager)
+        assert np.array_equal(p[b:e].view(np.uint32), pa.view(np.uint32)), f"positions of system {s}"
+        assert np.array_equal(v[b:e].view(np.uint32), va.view(np.uint32)), f"velocities of system {s}"
+        assert np.array_equal(a[b:e].view(np.uint32), aa.view(np.uint32)), f"accelerations of system {s}"
+        np.testing.assert_allclose(es[s], ea, rtol=1e-12, atol=1e-300)
+        if eager:
+            sum_dir += st[0] * (e - b)
+            sum_app += st[2] * (e - b)
+    if eager:
+        n = int(off[-1])
+        # {<direct>, max direct, <approx>, max approx}: per-particle sums add up exactly
+        assert round(stats[0] * n) == round(sum_dir)
+        assert round(stats[2] * n) == round(sum_app)
+    t.close()
+
+
+def test_ensemble_direct_sum_is_per_system():
+    import bonsai2_b200 as B
+    counts = np.array([300, 1, 4000, 57], np.int32)
+    pos, vel = _ensemble_inputs(counts, seed=31)
+    t = B.Treecode(**PARAMS)
+    t.set_systems(counts)
+    t.h_ptclPos[:] = pos
+    t.h_ptclVel[:] = vel
+    t.ptcl_h2d()
+    off = _offsets(counts)
+    sample = np.array([0, 299, 300, 301, 2000, 4300, 4357], np.int32)
+    d = t.direct_fp64(sample)
+    for k, i in enumerate(sample):
+        s = int(np.searchsorted(off, i, side="right") - 1)
+        q = pos[off[s]:off[s + 1]].astype(np.float64)
+        dr = q[:, :3] - pos[i, :3].astype(np.float64)
+        r2 = (dr * dr).sum(1) + np.float64(np.float32(0.01)) ** 2
+        rinv = 1.0 / np.sqrt(r2)
+        ref = np.concatenate([(q[:, 3] * rinv ** 3)[:, None] * dr, -(q[:, 3] * rinv)[:, None]], 1).sum(0)
+        np.testing.assert_allclose(d[k], ref, rtol=1e-10, atol=1e-12)
+    t.close()
+
+
+def test_ensemble_rejects_per_group_theta_and_bad_counts():
+    import bonsai2_b200 as B
+    from bonsai2_b200._lib import BonsaiError
+    t = B.Treecode(**PARAMS)
+    with pytest.raises(BonsaiError):
+        t.set_systems(np.array([10, 0, 5], np.int32))
+    t.set_systems(np.array([10, 5], np.int32))
+    # per-group opening angles are a single-system feature
+    assert t._L.bonsai_set_theta_mode(t.handle, 2, 0.25, 1.25) == -4
+    t.close()
+
+
+def test_autotune_restores_state_and_keeps_bit_identity():
+    import bonsai2_b200 as B
+    from bonsai2_b200.ensemble import system_sizes
+    counts = system_sizes(24, 1 << 9, 1 << 14, seed=9)
+    pos, vel = _ensemble_inputs(counts, seed=99)
+    t = B.Treecode(**PARAMS)
+    t.set_systems(counts)
+    t.h_ptclPos[:] = pos
+    t.h_ptclVel[:] = vel
+    t.ptcl_h2d()
+    r = t.autotune(nleaf=(8, 16), ncrit=(32, 64, 128), steps=1)
+    ms = r["ms"]
+    assert r["nleaf"] in (8, 16) and r["ncrit"] in (32, 64, 128) and r["layout"] in (0, 1)
+    assert np.all(ms[1] > 0)                        # full-warp layout: every candidate ran
+    assert np.all(ms[0][:, :2] > 0) and np.all(ms[0][:, 2] == -1)  # no half-warp layout above nCrit 64
+    assert ms[r["layout"]].min() == ms[ms > 0].min()
+    # the state was restored: stepping now equals a fresh ensemble with the chosen parameters
+    t.step(2, graph=True)
+    assert t.synchronize() == 0
+    t.ptcl_d2h()
+    p1 = t.h_ptclPos.copy()
+    prm = dict(PARAMS, nleaf=r["nleaf"], ncrit=r["ncrit"])
+    u = B.Treecode(**prm)
+    u.set_walk_layout(r["layout"])
+    u.set_systems(counts)
+    p2, _, _, _ = _run(u, pos, vel, 2, eager=False)
+    assert np.array_equal(p1.view(np.uint32), p2.view(np.uint32))
+    # and each system still matches itself alone under the chosen parameters
+    off = _offsets(counts)
+    for s in (0, len(counts) // 2, len(counts) - 1):
+        b, e = off[s], off[s + 1]
+        (pa, _, _, _), _ = _alone(pos[b:e], vel[b:e], 2, False, params=prm, layout=r["layout"])
+        assert np.array_equal(p2[b:e].view(np.uint32), pa.view(np.uint32))
+    t.close()
+    u.close()
+
+
+def test_ensemble_512_systems_spot_check():
+    """The batching configuration's shape (512 systems, N_s log-uniform in
+    [2^10, 2^18], theta 0.5, eps 0.01), 2 graph steps, three systems checked
+    against themselves alone."""
+    import bonsai2_b200 as B
+    from bonsai2_b200.ensemble import system_sizes
+    counts = system_sizes(512, 1 << 10, 1 << 18, seed=2024)
+    pos, vel = _ensemble_inputs(counts, seed=1)
+    t = B.Treecode(**PARAMS)
+    t.set_systems(counts)
+    p, v, a, _ = _run(t, pos, vel, 2, eager=False)
+    assert np.isfinite(a).all()
+    off = _offsets(counts)
+    for s in (0, int(np.argmax(counts)), 511):
+        b, e = off[s], off[s + 1]
+        (pa, va, aa, _), _ = _alone(pos[b:e], vel[b:e], 2, False)
+        assert np.array_equal(p[b:e].view(np.uint32), pa.view(np.uint32))
+        assert np.array_equal(a[b:e].view(np.uint32), aa.view(np.uint32))
+    t.close()
