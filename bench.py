@@ -64,6 +64,9 @@ def parse():
     ap.add_argument("--sweep", default="0.3,0.4,0.5,0.6,0.7,0.8", help="thetas of the sweep reported beside the headline")
     ap.add_argument("--learned-target", type=float, default=1e-3,
                     help="per-group error target of the learned opening angles (0: skip the learned form)")
+    ap.add_argument("--batch-systems", type=int, default=512,
+                    help="systems of the batching form reported beside the headline (0: skip)")
+    ap.add_argument("--batch-steps", type=int, default=32)
     ap.add_argument("--eps", type=float, default=0.005)
     ap.add_argument("--nleaf", type=int, default=16)
     ap.add_argument("--ncrit", type=int, default=64)
@@ -333,6 +336,7 @@ def run_ours(a):
     t.close()
     sweep = theta_sweep(B, L, pos, vel, a, d.local) if (d.rank == 0 and a.sweep) else None
     learned = learned_theta(B, L, pos, vel, a, d.local, sweep) if (d.rank == 0 and a.learned_target > 0) else None
+    batching = batching_form(B, L, a, d.local) if (d.rank == 0 and a.batch_systems > 0) else None
 
     cpu = None
     if d.rank == 0 and d.world == 1 and not a.no_cpu_baseline:
@@ -371,6 +375,7 @@ def run_ours(a):
             "status": int(status),
             "theta_sweep": sweep,
             "learned_theta": learned,
+            "batching": batching,
         }
         if learned:
             learned["vs_fixed_headline"] = learned["value"] / value
@@ -489,6 +494,76 @@ def learned_theta(B, L, pos, vel, a, device, sweep):
     out["gain_at_equal_median"] = out["value"] / eq_m if eq_m else None
     out["gain_at_equal_p99"] = out["value"] / eq_p if eq_p else None
     return out
+
+
+def batching_form(B, L, a, device):
+    """The batching form: an ensemble of independent Plummer spheres (N per
+    system log-uniform in [2^10, 2^18], seeded; theta 0.5, eps 0.01), every
+    stage one launch over all systems, the step replayed as captured graphs;
+    nLeaf / nCrit / walk layout from the autotuner (untimed setup); then
+    batch_steps timed steps.  Three systems are re-run alone for the same
+    steps and compared bit for bit; forces are judged on 2048 samples against
+    the FP64 direct sum inside each sample's system."""
+    from bonsai2_b200.ensemble import plummer_ensemble, system_sizes
+    from bonsai2_b200.treecode import _p
+    counts = system_sizes(a.batch_systems, 1 << 10, 1 << 18, seed=2024)
+    pos, vel = plummer_ensemble(counts, base_seed=a.seed)
+    n = pos.shape[0]
+    prm = dict(eps=0.01, theta=0.5, ncrit=64, nleaf=16, level_split=a.level_split, dt=1.0 / 64, device=device)
+    t = B.Treecode(**prm)
+    t.set_systems(counts)
+    L.bonsai_set_particles(t.handle, _p(pos), _p(vel), n)
+    t0 = time.perf_counter()
+    tune = t.autotune(nleaf=(8, 16, 32), ncrit=(16, 32, 64, 128), steps=2)
+    t_tune = time.perf_counter() - t0
+    nl, nc, lay = tune["nleaf"], tune["ncrit"], tune["layout"]
+    # accuracy at the initial positions
+    t.buildTree(nl)
+    t.computeMultipoles()
+    t.makeGroups(a.level_split, nc)
+    t.computeForces(False)
+    acc = t.get_acc().astype(np.float64)
+    rng = np.random.default_rng(2048)
+    samp = np.ascontiguousarray(rng.choice(n, 2048, replace=False).astype(np.int32))
+    ref = t.direct_fp64(samp, include_self=True)
+    err = np.linalg.norm(acc[samp, :3] - ref[:, :3], axis=1) / np.linalg.norm(ref[:, :3], axis=1)
+    # timed steps from the initial state
+    L.bonsai_set_particles(t.handle, _p(pos), _p(vel), n)
+    nkern = L.bonsai_graph_kernel_count(t.handle)
+    ph = np.zeros(4 * a.batch_steps + 1, np.float32)
+    rc = L.bonsai_step_timed(t.handle, a.batch_steps, _p(ph))
+    if rc:
+        raise B.BonsaiError(rc, "batching steps")
+    status = t.synchronize()
+    ms = float(ph[4 * a.batch_steps]) / a.batch_steps
+    steps_ph = ph[:4 * a.batch_steps].reshape(a.batch_steps, 4)
+    fin = np.empty((n, 4), np.float32)
+    L.bonsai_get_particles(t.handle, _p(fin), None, None)
+    t.close()
+    off = np.concatenate([[0], np.cumsum(counts)])
+    same = []
+    for s in (0, int(np.argmax(counts)), len(counts) - 1):
+        u = B.Treecode(**dict(prm, nleaf=nl, ncrit=nc))
+        u.set_walk_layout(lay)
+        b, e = int(off[s]), int(off[s + 1])
+        u.alloc(e - b)
+        ps, vs = np.ascontiguousarray(pos[b:e]), np.ascontiguousarray(vel[b:e])
+        L.bonsai_set_particles(u.handle, _p(ps), _p(vs), e - b)
+        u.step(a.batch_steps, graph=True)
+        u.synchronize()
+        one = np.empty((e - b, 4), np.float32)
+        L.bonsai_get_particles(u.handle, _p(one), None, None)
+        u.close()
+        same.append(bool(np.array_equal(one.view(np.uint32), fin[b:e].view(np.uint32))))
+    return {"value": n / (ms * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": ms, "systems": int(len(counts)),
+            "particles": int(n), "n_min": int(counts.min()), "n_max": int(counts.max()), "steps": a.batch_steps,
+            "stages_ms": {"build_multipoles_groups": float(steps_ph[:, 0].mean()),
+                          "walk": float(steps_ph[:, 1].mean()), "move_energies": float(steps_ph[:, 2].mean())},
+            "kernels_per_step": int(nkern), "autotuned": {"nleaf": nl, "ncrit": nc, "walk_layout": lay,
+                                                          "seconds": t_tune},
+            "median_rel_force_err": float(np.median(err)), "p99_rel_force_err": float(np.percentile(err, 99)),
+            "bit_identical_to_alone": same, "status": int(status),
+            "config": "512 Plummer spheres, N_s = floor(2^U(10,18)) seed 2024, theta 0.5, eps 0.01, dt 1/64"}
 
 
 def main():

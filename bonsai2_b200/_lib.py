@@ -68,11 +68,16 @@ SIGNATURES = {
     "bonsai_mlp_loss_grad": (I, [I, P, P, I, P, ctypes.c_float, ctypes.c_float, ctypes.c_float, P, P]),
     "bonsai_mlp_train": (I, [I, P, P, I, P, I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, P]),
     "bonsai_mlp_predict": (I, [I, P, I, P, ctypes.c_float, ctypes.c_float, P]),
+    "bonsai_set_precision": (I, [P, I]),
+    "bonsai_set_particles_f64": (I, [P, P, P, I]),
+    "bonsai_get_particles_f64": (I, [P, P, P, P]),
     "bonsai_set_systems": (I, [P, P, I]),
     "bonsai_get_system_energies": (I, [P, P]),
     "bonsai_set_walk_layout": (I, [P, I]),
     "bonsai_autotune": (I, [P, P, I, P, I, I, P, P]),
     "bonsai_plummer": (I, [ctypes.c_long, ctypes.c_uint, P, P]),
+    "bonsai_galaxy": (I, [ctypes.c_long, ctypes.c_ulonglong, P, P]),
+    "bonsai_clustered_field": (I, [ctypes.c_long, ctypes.c_ulonglong, I, P, P]),
     "bonsai_host_alloc": (P, [ctypes.c_size_t]),
     "bonsai_host_free": (None, [P]),
 }

@@ -45,11 +45,13 @@ struct TreeInfo {
   int level_end[kLevels];
 };
 
-// Per-cell FP64 record used by the bottom-up multipole pass.
+// Per-cell FP64 record used by the bottom-up multipole pass.  The particle
+// bounding box is kept in double so that double-single positions keep exact
+// cell extents (float positions convert to it exactly).
 struct MpRec {
   double m, cx, cy, cz;
   double ixx, iyy, izz, ixy, ixz, iyz;
-  float bmin[3], bmax[3];
+  double bmin[3], bmax[3];
 };
 
 struct Box {

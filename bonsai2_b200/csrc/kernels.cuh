@@ -47,7 +47,7 @@ __global__ void k_multipoles(const int* __restrict__ leaf_list, const TreeInfo* 
                              const float4* __restrict__ jpos, float inv_theta, MpRec* __restrict__ rec,
                              float4* __restrict__ cell_open, float4* __restrict__ cell_q0,
                              float4* __restrict__ cell_q1, float2* __restrict__ cell_ls, int* __restrict__ mp_count,
-                             int cell_cap);
+                             int cell_cap, const float4* __restrict__ jlo, float4* __restrict__ cell_lo);
 __global__ void k_multipoles_ref_layout(const TreeInfo* __restrict__ info, const float4* __restrict__ cell_open,
                                         const MpRec* __restrict__ rec, float4* __restrict__ size,
                                         float4* __restrict__ mono, float4* __restrict__ quad0,
@@ -75,11 +75,14 @@ void launch_walk(int variant, int nblocks, const int2* groups, const TreeInfo* i
                  const uint4* cell_data, const float4* cell_open, const float4* cell_q0, const float4* cell_q1,
                  const float2* cell_ls, const float* group_inv_theta, float eps2, float4* acc, int* ring_pool,
                  int ring_cap, unsigned* group_counter, unsigned long long* stats, int* status, const int* sys_off,
-                 int nsys, const int* root_beg, cudaStream_t s);
+                 int nsys, const int* root_beg, const float4* ipos_lo, const float4* jpos_lo, const float4* cell_lo,
+                 cudaStream_t s);
 
 // move.cu
+// lo (nullable): double-single position low parts, drifted with the high parts
 void launch_move(float4* pos, float4* vel, const float4* acc, int n, float dt, int* closing, float eps, int write,
-                 double* partial, int nblocks, unsigned* ticket, double* energies, cudaStream_t s);
+                 double* partial, int nblocks, unsigned* ticket, double* energies, cudaStream_t s,
+                 float4* lo = nullptr);
 // ensemble move: energies per chunk, folded per system and in total
 void launch_move_sys(float4* pos, float4* vel, const float4* acc, const int4* chunks, int nchunks,
                      const int* chunk_beg, int nsys, float dt, int* closing, float eps, int write, double* chunk_part,
@@ -87,8 +90,9 @@ void launch_move_sys(float4* pos, float4* vel, const float4* acc, const int4* ch
 // FP64 direct sum inside each sample's own system (one block per sample)
 void launch_direct_fp64_sys(const float4* pos, const int* sys_off, int nsys, const int* sample, int ns, double eps2,
                             int include_self, double* out, cudaStream_t s);
+// lo (nullable): double-single low parts, positions taken as hi + lo
 void launch_direct_fp64(const float4* pos, int n, const int* sample, int ns, double eps2, int include_self,
-                        double* part, int nsplit, double* out, cudaStream_t s);
+                        double* part, int nsplit, double* out, cudaStream_t s, const float4* lo = nullptr);
 __global__ void k_scatter_by_id(const int* __restrict__ id, int n, const float4* __restrict__ in,
                                 float4* __restrict__ out);
 __global__ void k_iota(int* __restrict__ a, int n);

@@ -22,11 +22,24 @@ struct EnergySums {
   double T = 0, W = 0, S = 0, px = 0, py = 0, pz = 0, mt = 0;
 };
 
+// x_hi + x_lo += d in double-single: exact two-sum of hi and d, the error
+// and the old low part folded into lo, renormalised (Dekker 1971; Knuth TAOCP
+// vol. 2, 4.2.2)
+__device__ __forceinline__ void ds_add(float& hi, float& lo, float d) {
+  const float s = __fadd_rn(hi, d);
+  const float bb = __fsub_rn(s, hi);
+  const float err = __fadd_rn(__fsub_rn(hi, __fsub_rn(s, bb)), __fsub_rn(d, bb));
+  const float l = __fadd_rn(lo, err);
+  hi = __fadd_rn(s, l);
+  lo = __fsub_rn(l, __fsub_rn(hi, s));
+}
+
 // one particle: closing kick (hc = 0 on the first step), energy terms at the
-// synchronised point, then opening kick and drift when write is set
+// synchronised point, then opening kick and drift when write is set.  lo
+// (nullable): double-single low parts of the positions
 __device__ __forceinline__ void move_one(float4* __restrict__ pos, float4* __restrict__ vel,
                                          const float4* __restrict__ acc, int i, float dt, float h, float hc,
-                                         double ieps, int write, EnergySums& e) {
+                                         double ieps, int write, EnergySums& e, float4* __restrict__ lo = nullptr) {
   float4 p = pos[i], v = vel[i];
   const float4 a = acc[i];
   v.x = fmaf(a.x, hc, v.x); v.y = fmaf(a.y, hc, v.y); v.z = fmaf(a.z, hc, v.z);
@@ -37,7 +50,15 @@ __device__ __forceinline__ void move_one(float4* __restrict__ pos, float4* __res
   e.px += m * v.x; e.py += m * v.y; e.pz += m * v.z; e.mt += m;
   if (write) {
     v.x = fmaf(a.x, h, v.x); v.y = fmaf(a.y, h, v.y); v.z = fmaf(a.z, h, v.z);
-    p.x = fmaf(v.x, dt, p.x); p.y = fmaf(v.y, dt, p.y); p.z = fmaf(v.z, dt, p.z);
+    if (lo) {
+      float4 l = lo[i];
+      ds_add(p.x, l.x, __fmul_rn(v.x, dt));
+      ds_add(p.y, l.y, __fmul_rn(v.y, dt));
+      ds_add(p.z, l.z, __fmul_rn(v.z, dt));
+      lo[i] = l;
+    } else {
+      p.x = fmaf(v.x, dt, p.x); p.y = fmaf(v.y, dt, p.y); p.z = fmaf(v.z, dt, p.z);
+    }
     pos[i] = p;
     vel[i] = v;
   }
@@ -70,13 +91,13 @@ __global__ void __launch_bounds__(256) k_move(float4* __restrict__ pos, float4* 
                                               const float4* __restrict__ acc, int n, float dt,
                                               int* __restrict__ closing, float eps, int write,
                                               double* __restrict__ partial, unsigned* __restrict__ ticket,
-                                              double* __restrict__ energies) {
+                                              double* __restrict__ energies, float4* __restrict__ lo) {
   const float h = 0.5f * dt;
   const float hc = (*closing) ? h : 0.0f;
   const double ieps = eps > 0.f ? 1.0 / (double)eps : 0.0;
   EnergySums e;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    move_one(pos, vel, acc, i, dt, h, hc, ieps, write, e);
+    move_one(pos, vel, acc, i, dt, h, hc, ieps, write, e, lo);
   __shared__ double sh[kNE][8];
   __shared__ bool last;
   const double x = block_energy_sum(e, sh);
@@ -154,29 +175,39 @@ void launch_move_sys(float4* pos, float4* vel, const float4* acc, const int4* ch
 }
 
 void launch_move(float4* pos, float4* vel, const float4* acc, int n, float dt, int* closing, float eps, int write,
-                 double* partial, int nblocks, unsigned* ticket, double* energies, cudaStream_t s) {
-  k_move<<<nblocks, 256, 0, s>>>(pos, vel, acc, n, dt, closing, eps, write, partial, ticket, energies);
+                 double* partial, int nblocks, unsigned* ticket, double* energies, cudaStream_t s, float4* lo) {
+  k_move<<<nblocks, 256, 0, s>>>(pos, vel, acc, n, dt, closing, eps, write, partial, ticket, energies, lo);
 }
 
 // FP64 direct summation for sample particles (checker): grid (ceil(ns/256),
 // nsplit); thread = one sample, block = one slice of the sources.
 __global__ void __launch_bounds__(256) k_direct_fp64(const float4* __restrict__ pos, int n,
                                                      const int* __restrict__ sample, int ns, double eps2,
-                                                     int include_self, double* __restrict__ part) {
+                                                     int include_self, double* __restrict__ part,
+                                                     const float4* __restrict__ lo) {
   __shared__ double4 sj[256];
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   const int nsplit = gridDim.y;
   const int jb = (int)((long long)n * blockIdx.y / nsplit), je = (int)((long long)n * (blockIdx.y + 1) / nsplit);
   const int i = s < ns ? sample[s] : 0;
   const float4 pi = pos[i];
-  const double xi = pi.x, yi = pi.y, zi = pi.z;
+  double xi = pi.x, yi = pi.y, zi = pi.z;
+  if (lo) {
+    const float4 l = lo[i];
+    xi += l.x; yi += l.y; zi += l.z;
+  }
   double ax = 0, ay = 0, az = 0, ph = 0;
   for (int j0 = jb; j0 < je; j0 += 256) {
     __syncthreads();
     const int jj = j0 + threadIdx.x;
     if (jj < je) {
       const float4 p = pos[jj];
-      sj[threadIdx.x] = make_double4(p.x, p.y, p.z, p.w);
+      double4 q = make_double4(p.x, p.y, p.z, p.w);
+      if (lo) {
+        const float4 l = lo[jj];
+        q.x += l.x; q.y += l.y; q.z += l.z;
+      }
+      sj[threadIdx.x] = q;
     }
     __syncthreads();
     const int cnt = min(256, je - j0);
@@ -206,9 +237,9 @@ __global__ void k_direct_fold(const double* __restrict__ part, int ns, int nspli
 }
 
 void launch_direct_fp64(const float4* pos, int n, const int* sample, int ns, double eps2, int include_self,
-                        double* part, int nsplit, double* out, cudaStream_t s) {
+                        double* part, int nsplit, double* out, cudaStream_t s, const float4* lo) {
   dim3 grid((ns + 255) / 256, nsplit);
-  k_direct_fp64<<<grid, 256, 0, s>>>(pos, n, sample, ns, eps2, include_self, part);
+  k_direct_fp64<<<grid, 256, 0, s>>>(pos, n, sample, ns, eps2, include_self, part, lo);
   k_direct_fold<<<(4 * ns + 255) / 256, 256, 0, s>>>(part, ns, nsplit, out);
 }
 

@@ -16,6 +16,8 @@
 // (l/theta_g + s)^2.  Stored for the walk (mass-weighted, pre-scaled so the
 // force kernel needs fewer operations):  cell_q0 = (M, 3Ixx, 3Iyy, 3Izz),
 // cell_q1 = (3Ixy, 3Ixz, 3Iyz, 1.5 tr I), with I = M Q.
+// Double-single positions (jlo != nullptr): particles enter the FP64 sums as
+// hi + lo, and the COM is stored as hi (cell_open) plus lo (cell_lo).
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -23,18 +25,37 @@ namespace bonsai {
 
 __device__ __forceinline__ void store_cell(int c, const MpRec& r, float inv_theta, MpRec* __restrict__ rec,
                                            float4* __restrict__ cell_open, float4* __restrict__ cell_q0,
-                                           float4* __restrict__ cell_q1, float2* __restrict__ cell_ls) {
+                                           float4* __restrict__ cell_q1, float2* __restrict__ cell_ls,
+                                           float4* __restrict__ cell_lo) {
   rec[c] = r;
   const float cx = (float)r.cx, cy = (float)r.cy, cz = (float)r.cz;
-  const float vx = __fmul_rn(__fadd_rn(r.bmax[0], r.bmin[0]), 0.5f);
-  const float vy = __fmul_rn(__fadd_rn(r.bmax[1], r.bmin[1]), 0.5f);
-  const float vz = __fmul_rn(__fadd_rn(r.bmax[2], r.bmin[2]), 0.5f);
-  const float hx = __fmul_rn(__fsub_rn(r.bmax[0], r.bmin[0]), 0.5f);
-  const float hy = __fmul_rn(__fsub_rn(r.bmax[1], r.bmin[1]), 0.5f);
-  const float hz = __fmul_rn(__fsub_rn(r.bmax[2], r.bmin[2]), 0.5f);
-  const float dx = __fsub_rn(vx, cx), dy = __fsub_rn(vy, cy), dz = __fsub_rn(vz, cz);
-  const float s = __fsqrt_rn(__fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx))));
-  const float l = fmaxf(__fmul_rn(2.0f, fmaxf(hx, fmaxf(hy, hz))), 1.0e-6f);
+  if (cell_lo)
+    cell_lo[c] = make_float4((float)(r.cx - (double)cx), (float)(r.cy - (double)cy), (float)(r.cz - (double)cz), 0.f);
+  float s, l;
+  if (cell_lo) {
+    // double-single: extents and centre offsets from the exact box and COM
+    double v[3], hm = 0.0, d2 = 0.0;
+    const double com[3] = {r.cx, r.cy, r.cz};
+    for (int k = 0; k < 3; k++) {
+      v[k] = 0.5 * (r.bmax[k] + r.bmin[k]) - com[k];
+      hm = fmax(hm, 0.5 * (r.bmax[k] - r.bmin[k]));
+      d2 += v[k] * v[k];
+    }
+    s = (float)sqrt(d2);
+    l = fmaxf((float)(2.0 * hm), 1.0e-6f);
+  } else {
+    const float b0[3] = {(float)r.bmin[0], (float)r.bmin[1], (float)r.bmin[2]};
+    const float b1[3] = {(float)r.bmax[0], (float)r.bmax[1], (float)r.bmax[2]};
+    const float vx = __fmul_rn(__fadd_rn(b1[0], b0[0]), 0.5f);
+    const float vy = __fmul_rn(__fadd_rn(b1[1], b0[1]), 0.5f);
+    const float vz = __fmul_rn(__fadd_rn(b1[2], b0[2]), 0.5f);
+    const float hx = __fmul_rn(__fsub_rn(b1[0], b0[0]), 0.5f);
+    const float hy = __fmul_rn(__fsub_rn(b1[1], b0[1]), 0.5f);
+    const float hz = __fmul_rn(__fsub_rn(b1[2], b0[2]), 0.5f);
+    const float dx = __fsub_rn(vx, cx), dy = __fsub_rn(vy, cy), dz = __fsub_rn(vz, cz);
+    s = __fsqrt_rn(__fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx))));
+    l = fmaxf(__fmul_rn(2.0f, fmaxf(hx, fmaxf(hy, hz))), 1.0e-6f);
+  }
   const float op = __fmaf_rn(l, inv_theta, s);
   cell_open[c] = make_float4(cx, cy, cz, __fmul_rn(op, op));
   cell_ls[c] = make_float2(l, s);  // per-group opening angles recompute (l/theta_g + s)^2
@@ -50,7 +71,8 @@ __global__ void __launch_bounds__(256) k_multipoles(const int* __restrict__ leaf
                                                     MpRec* __restrict__ rec, float4* __restrict__ cell_open,
                                                     float4* __restrict__ cell_q0, float4* __restrict__ cell_q1,
                                                     float2* __restrict__ cell_ls, int* __restrict__ mp_count,
-                                                    int cell_cap) {
+                                                    int cell_cap, const float4* __restrict__ jlo,
+                                                    float4* __restrict__ cell_lo) {
   const int nleaves = info->nleaves;
   if (info->ncells > cell_cap) return;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nleaves; t += gridDim.x * blockDim.x) {
@@ -59,27 +81,37 @@ __global__ void __launch_bounds__(256) k_multipoles(const int* __restrict__ leaf
     const int b = (int)cd.z, e = (int)cd.w;
     MpRec r;
     double m = 0, sx = 0, sy = 0, sz = 0;
-    float mn[3] = {3.0e38f, 3.0e38f, 3.0e38f}, mx[3] = {-3.0e38f, -3.0e38f, -3.0e38f};
+    double mn[3] = {3.0e38, 3.0e38, 3.0e38}, mx[3] = {-3.0e38, -3.0e38, -3.0e38};
     for (int i = b; i < e; i++) {
       const float4 p = __ldg(jpos + i);
+      double px = p.x, py = p.y, pz = p.z;
+      if (jlo) {
+        const float4 l = __ldg(jlo + i);
+        px += l.x; py += l.y; pz += l.z;
+      }
       m += p.w;
-      sx += (double)p.w * p.x; sy += (double)p.w * p.y; sz += (double)p.w * p.z;
-      mn[0] = fminf(mn[0], p.x); mn[1] = fminf(mn[1], p.y); mn[2] = fminf(mn[2], p.z);
-      mx[0] = fmaxf(mx[0], p.x); mx[1] = fmaxf(mx[1], p.y); mx[2] = fmaxf(mx[2], p.z);
+      sx += (double)p.w * px; sy += (double)p.w * py; sz += (double)p.w * pz;
+      mn[0] = fmin(mn[0], px); mn[1] = fmin(mn[1], py); mn[2] = fmin(mn[2], pz);
+      mx[0] = fmax(mx[0], px); mx[1] = fmax(mx[1], py); mx[2] = fmax(mx[2], pz);
     }
     if (m > 0.0) { r.cx = sx / m; r.cy = sy / m; r.cz = sz / m; }
-    else { r.cx = 0.5 * ((double)mn[0] + mx[0]); r.cy = 0.5 * ((double)mn[1] + mx[1]); r.cz = 0.5 * ((double)mn[2] + mx[2]); }
+    else { r.cx = 0.5 * (mn[0] + mx[0]); r.cy = 0.5 * (mn[1] + mx[1]); r.cz = 0.5 * (mn[2] + mx[2]); }
     double q[6] = {0, 0, 0, 0, 0, 0};
     for (int i = b; i < e; i++) {
       const float4 p = __ldg(jpos + i);
-      const double dx = p.x - r.cx, dy = p.y - r.cy, dz = p.z - r.cz, w = p.w;
+      double px = p.x, py = p.y, pz = p.z;
+      if (jlo) {
+        const float4 l = __ldg(jlo + i);
+        px += l.x; py += l.y; pz += l.z;
+      }
+      const double dx = px - r.cx, dy = py - r.cy, dz = pz - r.cz, w = p.w;
       q[0] += w * dx * dx; q[1] += w * dy * dy; q[2] += w * dz * dz;
       q[3] += w * dx * dy; q[4] += w * dx * dz; q[5] += w * dy * dz;
     }
     r.m = m;
     r.ixx = q[0]; r.iyy = q[1]; r.izz = q[2]; r.ixy = q[3]; r.ixz = q[4]; r.iyz = q[5];
     for (int k = 0; k < 3; k++) { r.bmin[k] = mn[k]; r.bmax[k] = mx[k]; }
-    store_cell(c, r, inv_theta, rec, cell_open, cell_q0, cell_q1, cell_ls);
+    store_cell(c, r, inv_theta, rec, cell_open, cell_q0, cell_q1, cell_ls, cell_lo);
     // climb while this thread is the last child to arrive
     while (true) {
       const int p = cell_parent[c];
@@ -91,20 +123,20 @@ __global__ void __launch_bounds__(256) k_multipoles(const int* __restrict__ leaf
       if (old != nch - 1) break;
       __threadfence();
       double M = 0, X = 0, Y = 0, Z = 0;
-      float bmn[3] = {3.0e38f, 3.0e38f, 3.0e38f}, bmx[3] = {-3.0e38f, -3.0e38f, -3.0e38f};
+      double bmn[3] = {3.0e38, 3.0e38, 3.0e38}, bmx[3] = {-3.0e38, -3.0e38, -3.0e38};
       for (int k = 0; k < nch; k++) {
         const MpRec* ck = rec + first + k;
         const double mk = __ldcg(&ck->m);
         M += mk;
         X += mk * __ldcg(&ck->cx); Y += mk * __ldcg(&ck->cy); Z += mk * __ldcg(&ck->cz);
         for (int a = 0; a < 3; a++) {
-          bmn[a] = fminf(bmn[a], __ldcg(&ck->bmin[a]));
-          bmx[a] = fmaxf(bmx[a], __ldcg(&ck->bmax[a]));
+          bmn[a] = fmin(bmn[a], __ldcg(&ck->bmin[a]));
+          bmx[a] = fmax(bmx[a], __ldcg(&ck->bmax[a]));
         }
       }
       MpRec P;
       if (M > 0.0) { P.cx = X / M; P.cy = Y / M; P.cz = Z / M; }
-      else { P.cx = 0.5 * ((double)bmn[0] + bmx[0]); P.cy = 0.5 * ((double)bmn[1] + bmx[1]); P.cz = 0.5 * ((double)bmn[2] + bmx[2]); }
+      else { P.cx = 0.5 * (bmn[0] + bmx[0]); P.cy = 0.5 * (bmn[1] + bmx[1]); P.cz = 0.5 * (bmn[2] + bmx[2]); }
       double I[6] = {0, 0, 0, 0, 0, 0};
       for (int k = 0; k < nch; k++) {
         const MpRec* ck = rec + first + k;
@@ -120,7 +152,7 @@ __global__ void __launch_bounds__(256) k_multipoles(const int* __restrict__ leaf
       P.m = M;
       P.ixx = I[0]; P.iyy = I[1]; P.izz = I[2]; P.ixy = I[3]; P.ixz = I[4]; P.iyz = I[5];
       for (int a = 0; a < 3; a++) { P.bmin[a] = bmn[a]; P.bmax[a] = bmx[a]; }
-      store_cell(p, P, inv_theta, rec, cell_open, cell_q0, cell_q1, cell_ls);
+      store_cell(p, P, inv_theta, rec, cell_open, cell_q0, cell_q1, cell_ls, cell_lo);
       c = p;
     }
   }

@@ -93,6 +93,11 @@ struct Handle {
   int box_blocks = 0, move_blocks = 0;
   int cur_nleaf = 16, cur_ncrit = 64, cur_ls = 5;
   int walk_layout = 0;  // walk_variant layout: 0 half-warp pairs where nCrit <= 64, 1 full warp
+  // precision 1: positions double-single, hi in pos/jpos/cell_open, lo in
+  // plo/jlo/cell_lo (state, tree and cell order)
+  int precision = 0;
+  float4* plo[2] = {nullptr, nullptr};
+  float4 *jlo = nullptr, *cell_lo = nullptr;
   // ensemble layout (nsys > 1): system s owns particles [off[s], off[s+1]) of
   // the state; every stage works per system in the same launches
   int nsys = 1, nchunks = 0;
@@ -127,9 +132,27 @@ struct Handle {
     nchunks = 0;
   }
 
+  void release_lo() {
+    dfree(&plo[0]); dfree(&plo[1]); dfree(&jlo); dfree(&cell_lo);
+  }
+  // the low-part arrays of double-single positions (zero: exact float input)
+  int alloc_lo() {
+    release_lo();
+    if (!precision || n == 0) return 0;
+    const size_t N = (size_t)n;
+    for (int p = 0; p < 2; p++) {
+      BONSAI_CUDA_TRY(dalloc(&plo[p], N));
+      BONSAI_CUDA_TRY(cudaMemset(plo[p], 0, N * sizeof(float4)));
+    }
+    BONSAI_CUDA_TRY(dalloc(&jlo, N));
+    BONSAI_CUDA_TRY(dalloc(&cell_lo, (size_t)cap_cells));
+    return 0;
+  }
+
   void release_particles() {
     release_graphs();
     release_systems();
+    release_lo();
     for (int p = 0; p < 2; p++) { dfree(&pos[p]); dfree(&vel[p]); dfree(&id[p]); }
     dfree(&acc); dfree(&jpos); dfree(&tkey); dfree(&pkey); dfree(&kalt);
     dfree(&tperm); dfree(&pperm); dfree(&valt); dfree(&sort_counts); dfree(&bsum);
@@ -168,6 +191,8 @@ struct Handle {
     BONSAI_CUDA_TRY(dalloc(&mp_count, C));
     BONSAI_CUDA_TRY(dalloc(&rec, C));
     BONSAI_CUDA_TRY(dalloc(&cell_ls, C));
+    dfree(&cell_lo);
+    if (precision) BONSAI_CUDA_TRY(dalloc(&cell_lo, C));
     return 0;
   }
 
@@ -248,6 +273,8 @@ struct Handle {
     // nLeaf 16 uses ~0.23 N.  Grown on demand by the eager build.
     int rc = alloc_cells(prm.nleaf >= 8 ? nn / 2 + 4096 : 2 * nn + 4096);
     if (rc) return rc;
+    rc = alloc_lo();
+    if (rc) return rc;
     par = 0;
     built = mp_done = grouped = forced = moved_after_forces = false;
     ever_built = ever_mp = false;
@@ -292,7 +319,9 @@ struct Handle {
     BONSAI_CUDA_TRY(cudaMemcpy(chunks, ch.data(), ch.size() * sizeof(int4), cudaMemcpyHostToDevice));
     BONSAI_CUDA_TRY(cudaMemset(sys_energy, 0, (size_t)ns * 8 * sizeof(double)));
     BONSAI_CUDA_TRY(cudaMemset(root_beg, 0, (size_t)(ns + 1) * sizeof(int)));
-    theta_mode = 0;  // per-group angles are a single-system feature
+    theta_mode = 0;  // per-group angles and double-single positions are single-system features
+    precision = 0;
+    release_lo();
     return 0;
   }
 
@@ -323,12 +352,14 @@ struct Handle {
     }
     radix_sort_pairs(tkey, kalt, tperm, valt, nullptr, n, sort_counts, &info->status, 8, so(), nsys, st);
     k_gather_pos<<<nsm * 8, 256, 0, st>>>(tperm, n, pos[par], jpos);
+    if (precision) k_gather_pos<<<nsm * 8, 256, 0, st>>>(tperm, n, plo[par], jlo);
     build_tree(tkey, n, nleaf, cap_cells, cap_cells, dlev, chain, hist, info, cell_data, cell_parent, leaf_list,
                mp_count, so(), nsys, root_beg, st);
   }
   void enq_multipoles() {
     k_multipoles<<<nsm * 8, 256, 0, st>>>(leaf_list, info, cell_data, cell_parent, jpos, 1.0f / prm.theta, rec,
-                                          cell_open, cell_q0, cell_q1, cell_ls, mp_count, cap_cells);
+                                          cell_open, cell_q0, cell_q1, cell_ls, mp_count, cap_cells,
+                                          precision ? jlo : nullptr, precision ? cell_lo : nullptr);
   }
   void enq_groups(int ls, int ncrit) {
     radix_sort_pairs(pkey, kalt, pperm, valt, nullptr, n, sort_counts, &info->status, 8, so(), nsys, st);
@@ -342,6 +373,7 @@ struct Handle {
     }
     const int q = par ^ 1;
     k_gather_state<<<nsm * 8, 256, 0, st>>>(pperm, n, pos[par], vel[par], id[par], pos[q], vel[q], id[q]);
+    if (precision) k_gather_pos<<<nsm * 8, 256, 0, st>>>(pperm, n, plo[par], plo[q]);
     par = q;
   }
   void enq_forces(int ncrit) {
@@ -358,7 +390,7 @@ struct Handle {
     }
     launch_walk(k, walk_blocks[k], groups, info, pos[par], jpos, cell_data, cell_open, cell_q0, cell_q1, cell_ls,
                 ginv, prm.eps * prm.eps, acc, ring, kRingCap, group_counter, stats, &info->status, so(), nsys, root_beg,
-                st);
+                precision ? plo[par] : nullptr, jlo, cell_lo, st);
   }
   void enq_move(bool write) {
     launch_move_wrapper(write);
@@ -525,7 +557,7 @@ void Handle::launch_move_wrapper(bool write) {
                     chunk_energy, move_blocks, move_ticket, energies, sys_energy, st);
   else
     launch_move(pos[par], vel[par], acc, n, prm.dt, closing, prm.eps, write ? 1 : 0, move_partial, move_blocks,
-                move_ticket, energies, st);
+                move_ticket, energies, st, precision ? plo[par] : nullptr);
 }
 
 Handle* H(bonsai_handle h) { return reinterpret_cast<Handle*>(h); }
@@ -548,6 +580,9 @@ int last_cuda(void) {
 
 // Plummer initial conditions (host): plummer.cpp
 extern "C" int bonsai_plummer_impl(long n, unsigned int seed, float* pos4, float* vel4);
+// composite galaxy and clustered field (host): ics.cpp
+extern "C" int bonsai_galaxy_impl(long n, unsigned long long seed, double* pos4, float* vel4);
+extern "C" int bonsai_clustered_field_impl(long n, unsigned long long seed, int nclusters, float* pos4, float* vel4);
 
 extern "C" {
 
@@ -616,6 +651,7 @@ static int set_particles_impl(Handle* h, const float* pos4, const float* vel4, i
   BONSAI_CUDA_TRY(cudaMemcpyAsync(h->pos[h->par], pos4, bytes, kind, h->st));
   BONSAI_CUDA_TRY(cudaMemcpyAsync(h->vel[h->par], vel4, bytes, kind, h->st));
   k_iota<<<h->nsm * 4, 256, 0, h->st>>>(h->id[h->par], n);
+  if (h->precision) BONSAI_CUDA_TRY(cudaMemsetAsync(h->plo[h->par], 0, bytes, h->st));  // float input: lo = 0
   BONSAI_CUDA_TRY(cudaMemsetAsync(h->closing, 0, sizeof(int), h->st));
   h->built = h->mp_done = h->grouped = h->forced = h->moved_after_forces = false;
   return last_cuda();
@@ -821,6 +857,62 @@ int bonsai_get_system_energies(bonsai_handle hh, double* out) {
   const double* src = h->nsys > 1 ? h->sys_energy : h->energies;
   BONSAI_CUDA_TRY(cudaMemcpyAsync(out, src, (size_t)h->nsys * 8 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
   BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  return last_cuda();
+}
+
+int bonsai_set_precision(bonsai_handle hh, int mode) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (mode < 0 || mode > 1) return BONSAI_ERR_ARG;
+  if (mode && h->nsys > 1) return BONSAI_ERR_ARG;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  h->release_graphs();
+  h->precision = mode;
+  return h->alloc_lo();
+}
+
+int bonsai_set_particles_f64(bonsai_handle hh, const double* pos4, const float* vel4, int n) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (!pos4 || !vel4 || n < 1) return BONSAI_ERR_ARG;
+  const size_t N = (size_t)n;
+  std::vector<float4> hi(N), lo(N);
+  for (size_t i = 0; i < N; i++) {
+    const double x = pos4[4 * i], y = pos4[4 * i + 1], z = pos4[4 * i + 2];
+    hi[i] = make_float4((float)x, (float)y, (float)z, (float)pos4[4 * i + 3]);
+    lo[i] = make_float4((float)(x - (double)hi[i].x), (float)(y - (double)hi[i].y), (float)(z - (double)hi[i].z), 0.f);
+  }
+  int rc = set_particles_impl(h, &hi[0].x, vel4, n, cudaMemcpyHostToDevice);
+  if (rc) return rc;
+  if (h->precision)
+    BONSAI_CUDA_TRY(cudaMemcpyAsync(h->plo[h->par], lo.data(), N * sizeof(float4), cudaMemcpyHostToDevice, h->st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));  // the host staging vectors go out of scope
+  return last_cuda();
+}
+
+int bonsai_get_particles_f64(bonsai_handle hh, double* pos4, float* vel4, float* acc4) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (h->n == 0) return BONSAI_ERR_NOT_ALLOCATED;
+  int rc = get_particles_impl(h, nullptr, vel4, acc4, cudaMemcpyDeviceToHost);
+  if (rc || !pos4) return rc;
+  const size_t N = (size_t)h->n;
+  std::vector<float4> hi(N), lo(N, make_float4(0.f, 0.f, 0.f, 0.f));
+  rc = get_particles_impl(h, &hi[0].x, nullptr, nullptr, cudaMemcpyDeviceToHost);
+  if (rc) return rc;
+  if (h->precision) {
+    float4* tmp = h->pos[h->par ^ 1];
+    k_scatter_by_id<<<h->nsm * 8, 256, 0, h->st>>>(h->id[h->par], h->n, h->plo[h->par], tmp);
+    BONSAI_CUDA_TRY(cudaMemcpyAsync(lo.data(), tmp, N * sizeof(float4), cudaMemcpyDeviceToHost, h->st));
+    BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  }
+  for (size_t i = 0; i < N; i++) {
+    pos4[4 * i] = (double)hi[i].x + (double)lo[i].x;
+    pos4[4 * i + 1] = (double)hi[i].y + (double)lo[i].y;
+    pos4[4 * i + 2] = (double)hi[i].z + (double)lo[i].z;
+    pos4[4 * i + 3] = (double)hi[i].w;
+  }
   return last_cuda();
 }
 
@@ -1030,13 +1122,18 @@ int bonsai_direct_fp64(bonsai_handle hh, const int* sample, int ns, int include_
   // positions in caller order into the idle state buffer
   float4* tmp = h->pos[h->par ^ 1];
   k_scatter_by_id<<<h->nsm * 8, 256, 0, h->st>>>(h->id[h->par], h->n, h->pos[h->par], tmp);
+  float4* tmp_lo = nullptr;
+  if (h->precision) {
+    tmp_lo = h->plo[h->par ^ 1];
+    k_scatter_by_id<<<h->nsm * 8, 256, 0, h->st>>>(h->id[h->par], h->n, h->plo[h->par], tmp_lo);
+  }
   BONSAI_CUDA_TRY(cudaMemcpyAsync(h->direct_sample, sample, (size_t)ns * 4, cudaMemcpyHostToDevice, h->st));
   const double e2 = (double)h->prm.eps * (double)h->prm.eps;
   if (h->nsys > 1)
     launch_direct_fp64_sys(tmp, h->sys_off, h->nsys, h->direct_sample, ns, e2, include_self, h->direct_out, h->st);
   else
     launch_direct_fp64(tmp, h->n, h->direct_sample, ns, e2, include_self, h->direct_part, nsplit, h->direct_out,
-                       h->st);
+                       h->st, tmp_lo);
   BONSAI_CUDA_TRY(cudaMemcpyAsync(out, h->direct_out, (size_t)ns * 4 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
   BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
   return last_cuda();
@@ -1199,6 +1296,14 @@ int bonsai_mlp_predict(int device, const float* X, int S, const float* w, float 
 int bonsai_plummer(long n, unsigned int seed, float* pos4, float* vel4) {
   if (n < 1 || !pos4 || !vel4) return BONSAI_ERR_ARG;
   return bonsai_plummer_impl(n, seed, pos4, vel4);
+}
+
+int bonsai_galaxy(long n, unsigned long long seed, double* pos4, float* vel4) {
+  return bonsai_galaxy_impl(n, seed, pos4, vel4);
+}
+
+int bonsai_clustered_field(long n, unsigned long long seed, int nclusters, float* pos4, float* vel4) {
+  return bonsai_clustered_field_impl(n, seed, nclusters, pos4, vel4);
 }
 
 int bonsai_fp32_peak(int device, double* tflops) {

@@ -29,6 +29,8 @@
 //     (34 FP32 operations + 1 MUFU per interaction; the reference's
 //     formulation, counted as 64 flops by treecode.cu:149-158, is the same
 //     algebra).
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -125,7 +127,13 @@ __device__ __forceinline__ int find_src(int incl, int s) {
 // ENS: the particles form an ensemble of independent systems (sys_off); a
 // group walks from its own system's level-1 cells [root_beg[s], root_beg[s+1])
 // only, in the order the system alone would.
-template <int NI, bool SPLIT, bool PERGROUP, bool ENS>
+// DS: positions are double-single (hi in ipos/jpos/cell_open, lo in
+// ipos_lo/jpos_lo/cell_lo).  Every coordinate the group uses is taken
+// relative to the group's reference point R (its first particle's hi
+// position) as (hi - R) + lo: the subtraction is exact for nearby points, so
+// separations keep FP32 relative precision however far from the origin the
+// group lies.  The interaction loops are unchanged.
+template <int NI, bool SPLIT, bool PERGROUP, bool ENS, bool DS>
 __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
     k_walk(const int2* __restrict__ groups, const TreeInfo* __restrict__ info, const float4* __restrict__ ipos,
            const float4* __restrict__ jpos, const uint4* __restrict__ cell_data,
@@ -134,7 +142,8 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
            const float* __restrict__ group_inv_theta, float eps2, float4* __restrict__ acc,
            int* __restrict__ ring_pool, int ring_cap, unsigned* __restrict__ group_counter,
            unsigned long long* __restrict__ stats, int* __restrict__ status, const int* __restrict__ sys_off,
-           int nsys, const int* __restrict__ root_beg) {
+           int nsys, const int* __restrict__ root_beg, const float4* __restrict__ ipos_lo,
+           const float4* __restrict__ jpos_lo, const float4* __restrict__ cell_lo) {
   constexpr int STRIDE = SPLIT ? 16 : 32;
   constexpr int JSTEP = SPLIT ? 2 : 1;
   __shared__ float4 s_a0[kWalkWarps][64];
@@ -170,14 +179,27 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
     }
     IPart pi[NI];
     float4 ai[NI];
+    float3 R = make_float3(0.f, 0.f, 0.f);
+    if (DS) {
+      const float4 r0 = ipos[pbeg];
+      R = make_float3(r0.x, r0.y, r0.z);
+    }
     float mnx = 3.0e38f, mny = 3.0e38f, mnz = 3.0e38f, mxx = -3.0e38f, mxy = -3.0e38f, mxz = -3.0e38f;
 #pragma unroll
     for (int k = 0; k < NI; k++) {
-      const float4 p = ipos[pbeg + min(k * STRIDE + sub, np - 1)];
-      pi[k].x = p.x; pi[k].y = p.y; pi[k].z = p.z;
+      const int ii = pbeg + min(k * STRIDE + sub, np - 1);
+      const float4 p = ipos[ii];
+      if (DS) {
+        const float4 lo = ipos_lo[ii];
+        pi[k].x = __fadd_rn(__fsub_rn(p.x, R.x), lo.x);
+        pi[k].y = __fadd_rn(__fsub_rn(p.y, R.y), lo.y);
+        pi[k].z = __fadd_rn(__fsub_rn(p.z, R.z), lo.z);
+      } else {
+        pi[k].x = p.x; pi[k].y = p.y; pi[k].z = p.z;
+      }
       ai[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-      mnx = fminf(mnx, p.x); mny = fminf(mny, p.y); mnz = fminf(mnz, p.z);
-      mxx = fmaxf(mxx, p.x); mxy = fmaxf(mxy, p.y); mxz = fmaxf(mxz, p.z);
+      mnx = fminf(mnx, pi[k].x); mny = fminf(mny, pi[k].y); mnz = fminf(mnz, pi[k].z);
+      mxx = fmaxf(mxx, pi[k].x); mxy = fmaxf(mxy, pi[k].y); mxz = fmaxf(mxz, pi[k].z);
     }
     mnx = warp_min_f32(mnx); mny = warp_min_f32(mny); mnz = warp_min_f32(mnz);
     mxx = warp_max_f32(mxx); mxy = warp_max_f32(mxy); mxz = warp_max_f32(mxz);
@@ -204,6 +226,12 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
         if (valid) {
           cd = __ldg(cell_data + cell);
           co = __ldg(cell_open + cell);
+          if (DS) {
+            const float4 cl = __ldg(cell_lo + cell);
+            co.x = __fadd_rn(__fsub_rn(co.x, R.x), cl.x);
+            co.y = __fadd_rn(__fsub_rn(co.y, R.y), cl.y);
+            co.z = __fadd_rn(__fsub_rn(co.z, R.z), cl.z);
+          }
           if (PERGROUP) {
             const float2 ls = __ldg(cell_ls + cell);
             const float op = __fmaf_rn(ls.x, inv_theta_g, ls.y);
@@ -267,7 +295,17 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
           const int f = __shfl_sync(kFull, pb, src);
           const int e = __shfl_sync(kFull, incl2 - nb, src);
           const int cnt = min(32, tot2 - base);
-          if (lane < cnt) s_d[w][(d_head + d_cnt + lane) & 63] = __ldg(jpos + f + (s - e));
+          if (lane < cnt) {
+            const int jj = f + (s - e);
+            float4 pj = __ldg(jpos + jj);
+            if (DS) {
+              const float4 lo = __ldg(jpos_lo + jj);
+              pj.x = __fadd_rn(__fsub_rn(pj.x, R.x), lo.x);
+              pj.y = __fadd_rn(__fsub_rn(pj.y, R.y), lo.y);
+              pj.z = __fadd_rn(__fsub_rn(pj.z, R.z), lo.z);
+            }
+            s_d[w][(d_head + d_cnt + lane) & 63] = pj;
+          }
           d_cnt += cnt;
           if (d_cnt >= 32) {
             __syncwarp();
@@ -352,20 +390,22 @@ int walk_variant(int ncrit, int layout) {
   return ncrit <= 32 ? 3 : (ncrit <= 64 ? 4 : 5);
 }
 
+template <class K>
+static int occupancy(K kernel) {
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, kWalkThreads, 0) != cudaSuccess) nb = 1;
+  return nb;
+}
+
+// blocks per SM that every instantiation of the variant reaches (the level
+// lists are sized for the largest grid)
 template <int NI, bool SPLIT>
 static int occupancy_of() {
-  int nb = 0, nb2 = 0, nb3 = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_walk<NI, SPLIT, false, false>, kWalkThreads, 0) !=
-      cudaSuccess)
-    nb = 1;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb2, k_walk<NI, SPLIT, true, false>, kWalkThreads, 0) !=
-      cudaSuccess)
-    nb2 = 1;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb3, k_walk<NI, SPLIT, false, true>, kWalkThreads, 0) !=
-      cudaSuccess)
-    nb3 = 1;
-  nb = nb < nb2 ? nb : nb2;
-  nb = nb < nb3 ? nb : nb3;
+  int nb = occupancy(k_walk<NI, SPLIT, false, false, false>);
+  nb = std::min(nb, occupancy(k_walk<NI, SPLIT, true, false, false>));
+  nb = std::min(nb, occupancy(k_walk<NI, SPLIT, false, true, false>));
+  nb = std::min(nb, occupancy(k_walk<NI, SPLIT, false, false, true>));
+  nb = std::min(nb, occupancy(k_walk<NI, SPLIT, true, false, true>));
   return nb < 1 ? 1 : nb;
 }
 
@@ -386,18 +426,23 @@ void launch_walk(int variant, int nblocks, const int2* groups, const TreeInfo* i
                  const float4* jpos, const uint4* cell_data, const float4* cell_open, const float4* cell_q0,
                  const float4* cell_q1, const float2* cell_ls, const float* group_inv_theta, float eps2,
                  float4* acc, int* ring_pool, int ring_cap, unsigned* group_counter, unsigned long long* stats,
-                 int* status, const int* sys_off, int nsys, const int* root_beg, cudaStream_t s) {
+                 int* status, const int* sys_off, int nsys, const int* root_beg, const float4* ipos_lo,
+                 const float4* jpos_lo, const float4* cell_lo, cudaStream_t s) {
 #define BONSAI_WALK_ARGS                                                                                          \
   groups, info, ipos, jpos, cell_data, cell_open, cell_q0, cell_q1, cell_ls, group_inv_theta, eps2, acc, ring_pool, \
-      ring_cap, group_counter, stats, status, sys_off, nsys, root_beg
+      ring_cap, group_counter, stats, status, sys_off, nsys, root_beg, ipos_lo, jpos_lo, cell_lo
 #define BONSAI_WALK(NI, SP)                                                                \
   do {                                                                                     \
     if (nsys > 1)                                                                          \
-      k_walk<NI, SP, false, true><<<nblocks, kWalkThreads, 0, s>>>(BONSAI_WALK_ARGS);      \
+      k_walk<NI, SP, false, true, false><<<nblocks, kWalkThreads, 0, s>>>(BONSAI_WALK_ARGS); \
+    else if (ipos_lo && group_inv_theta)                                                   \
+      k_walk<NI, SP, true, false, true><<<nblocks, kWalkThreads, 0, s>>>(BONSAI_WALK_ARGS);  \
+    else if (ipos_lo)                                                                      \
+      k_walk<NI, SP, false, false, true><<<nblocks, kWalkThreads, 0, s>>>(BONSAI_WALK_ARGS); \
     else if (group_inv_theta)                                                              \
-      k_walk<NI, SP, true, false><<<nblocks, kWalkThreads, 0, s>>>(BONSAI_WALK_ARGS);      \
+      k_walk<NI, SP, true, false, false><<<nblocks, kWalkThreads, 0, s>>>(BONSAI_WALK_ARGS); \
     else                                                                                   \
-      k_walk<NI, SP, false, false><<<nblocks, kWalkThreads, 0, s>>>(BONSAI_WALK_ARGS);     \
+      k_walk<NI, SP, false, false, false><<<nblocks, kWalkThreads, 0, s>>>(BONSAI_WALK_ARGS); \
   } while (0)
   switch (variant) {
 #if BONSAI_WALK_SPLIT

@@ -58,6 +58,23 @@ def plummer(n: int, seed: int = 19810614):
     return pos, vel
 
 
+def galaxy(n: int, seed: int = 1):
+    """Composite galaxy (halo + disk + bulge), positions as (n, 4) float64
+    (x, y, z, m), velocities (n, 4) float32 (bonsai_galaxy)."""
+    pos = np.empty((n, 4), np.float64)
+    vel = np.empty((n, 4), np.float32)
+    _check(load().bonsai_galaxy(n, seed, _p(pos), _p(vel)), "bonsai_galaxy")
+    return pos, vel
+
+
+def clustered_field(n: int, seed: int = 1, nclusters: int = 64):
+    """Plummer subclusters plus a uniform background, float32 (n, 4) arrays."""
+    pos = np.empty((n, 4), np.float32)
+    vel = np.empty((n, 4), np.float32)
+    _check(load().bonsai_clustered_field(n, seed, nclusters, _p(pos), _p(vel)), "bonsai_clustered_field")
+    return pos, vel
+
+
 class Treecode:
     def __init__(self, eps: float = 0.01, theta: float = 0.75, ncrit: int = 64, nleaf: int = 16,
                  level_split: int = 5, dt: float = 1.0 / 64, device: int = 0):
@@ -155,6 +172,30 @@ class Treecode:
         e = np.empty((ns, 8), np.float64)
         _check(self._L.bonsai_get_system_energies(self._h, _p(e)), "bonsai_get_system_energies")
         return e
+
+    def set_precision(self, mode: int):
+        """1: double-single positions (hi + lo float pairs, group-relative
+        walk coordinates); 0: float positions.  Set before loading particles."""
+        _check(self._L.bonsai_set_precision(self._h, mode), "bonsai_set_precision")
+
+    def set_particles_f64(self, pos4: np.ndarray, vel4: np.ndarray):
+        """Loads (n, 4) float64 positions (x, y, z, m) and float32 velocities."""
+        p = np.ascontiguousarray(pos4, np.float64)
+        v = np.ascontiguousarray(vel4, np.float32)
+        _check(self._L.bonsai_set_particles_f64(self._h, _p(p), _p(v), p.shape[0]), "bonsai_set_particles_f64")
+        if p.shape[0] != self.nPtcl:
+            self.nPtcl = p.shape[0]
+            self.h_ptclPos = np.zeros((self.nPtcl, 4), np.float32)
+            self.h_ptclVel = np.zeros((self.nPtcl, 4), np.float32)
+
+    def get_particles_f64(self):
+        """(positions float64 hi + lo, velocities, accelerations), caller order."""
+        n = self.nPtcl
+        p = np.empty((n, 4), np.float64)
+        v = np.empty((n, 4), np.float32)
+        a = np.empty((n, 4), np.float32)
+        _check(self._L.bonsai_get_particles_f64(self._h, _p(p), _p(v), _p(a)), "bonsai_get_particles_f64")
+        return p, v, a
 
     def set_walk_layout(self, layout: int):
         """0: two half-warps per group (nCrit <= 64), 1: one warp per group."""

@@ -195,6 +195,23 @@ int bonsai_mlp_train(int device, const float *X, const float *y, int S, float *w
                      float hi, float over, double *loss);
 int bonsai_mlp_predict(int device, const float *X, int S, const float *w, float lo, float hi, float *theta);
 
+/* ---- Double-single positions (precision form) ----
+ * No counterpart in the reference (float positions throughout).  mode 1
+ * keeps every position as a float pair hi + lo: the tree, keys and groups are
+ * built from hi; multipoles sum hi + lo in FP64 and store the centre of mass
+ * as a pair; the walk takes every coordinate relative to the group's first
+ * particle, (hi - R) + lo, so separations keep FP32 relative precision far
+ * from the origin; the drift adds in double-single; the FP64 checker
+ * (bonsai_direct_fp64) uses hi + lo.  Interactions stay FP32.  Set it before
+ * loading particles (the low parts start at zero); single systems only
+ * (BONSAI_ERR_ARG for an ensemble).  mode 0 (default) = float positions. */
+int bonsai_set_precision(bonsai_handle h, int mode);
+/* bonsai_set_particles from double positions pos4 = (x, y, z, m): split into
+ * hi = (float)x and lo = (float)(x - hi) (lo dropped in mode 0) */
+int bonsai_set_particles_f64(bonsai_handle h, const double *pos4, const float *vel4, int n);
+/* bonsai_get_particles with positions returned as hi + lo in double */
+int bonsai_get_particles_f64(bonsai_handle h, double *pos4, float *vel4, float *acc4);
+
 /* ---- Ensembles of independent systems (batching) ----
  * No counterpart in the reference, which holds one tree per process (its stage
  * state lives in file-scope device globals, buildTree.cu:23-36).
@@ -237,6 +254,18 @@ int bonsai_autotune(bonsai_handle h, const int *nleaf, int n_nleaf, const int *n
  * code/plummer.h:9-138 (glibc rand(), same stream), converted to float4 like
  * treecode.cu:65-87: pos4 = (x,y,z,m), vel4 = (vx,vy,vz,m).  n >= 1. */
 int bonsai_plummer(long n, unsigned int seed, float *pos4, float *vel4);
+
+/* Composite galaxy on the host (no counterpart in the reference): 60 % NFW-like
+ * halo (r_s 10, truncated at 200), 30 % exponential disk (R_d 3, sech^2
+ * z_d 0.3), 10 % Hernquist bulge (a 0.5) by particle index; log-normal masses
+ * (sigma 0.5) normalised to 1; pos4 = (x, y, z, m) in double, vel4 = (vx, vy,
+ * vz, m).  Seeded per particle: the result is independent of thread count. */
+int bonsai_galaxy(long n, unsigned long long seed, double *pos4, float *vel4);
+/* Clustered field on the host (no counterpart in the reference): 80 % of the
+ * particles in nclusters Plummer subclusters (masses log-uniform over two
+ * decades, scale radii log-uniform in [0.01, 0.2], centres uniform in the
+ * unit cube), 20 % uniform in the unit cube; equal masses 1/n. */
+int bonsai_clustered_field(long n, unsigned long long seed, int nclusters, float *pos4, float *vel4);
 
 /* pinned host memory (host_mem<T>, cudamem.h:64-96) */
 void *bonsai_host_alloc(size_t bytes);

@@ -70,7 +70,9 @@ def test_ensemble_bit_identical_to_alone(eager):
         assert np.array_equal(p[b:e].view(np.uint32), pa.view(np.uint32)), f"positions of system {s}"
         assert np.array_equal(v[b:e].view(np.uint32), va.view(np.uint32)), f"velocities of system {s}"
         assert np.array_equal(a[b:e].view(np.uint32), aa.view(np.uint32)), f"accelerations of system {s}"
-        np.testing.assert_allclose(es[s], ea, rtol=1e-12, atol=1e-300)
+        # FP64 sums in another grouping (chunks of the ensemble vs blocks alone): equal to
+        # rounding; momentum terms are cancellations of O(1e-3) terms, hence the absolute floor
+        np.testing.assert_allclose(es[s], ea, rtol=1e-12, atol=1e-15)
         if eager:
             sum_dir += st[0] * (e - b)
             sum_app += st[2] * (e - b)
@@ -132,7 +134,8 @@ def test_autotune_restores_state_and_keeps_bit_identity():
     assert r["nleaf"] in (8, 16) and r["ncrit"] in (32, 64, 128) and r["layout"] in (0, 1)
     assert np.all(ms[1] > 0)                        # full-warp layout: every candidate ran
     assert np.all(ms[0][:, :2] > 0) and np.all(ms[0][:, 2] == -1)  # no half-warp layout above nCrit 64
-    assert ms[r["layout"]].min() == ms[ms > 0].min()
+    chosen = ms[r["layout"]]
+    assert chosen[chosen > 0].min() == ms[ms > 0].min()  # the fastest candidate was kept
     # the state was restored: stepping now equals a fresh ensemble with the chosen parameters
     t.step(2, graph=True)
     assert t.synchronize() == 0
