@@ -64,6 +64,10 @@ def parse():
     ap.add_argument("--sweep", default="0.3,0.4,0.5,0.6,0.7,0.8", help="thetas of the sweep reported beside the headline")
     ap.add_argument("--learned-target", type=float, default=1e-3,
                     help="per-group error target of the learned opening angles (0: skip the learned form)")
+    ap.add_argument("--precision-n", type=int, default=1 << 26,
+                    help="particles of the precision form (composite galaxy; 0: skip)")
+    ap.add_argument("--field-n", type=int, default=1 << 25,
+                    help="particles of the learned form's clustered field (0: skip)")
     ap.add_argument("--batch-systems", type=int, default=512,
                     help="systems of the batching form reported beside the headline (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=32)
@@ -337,6 +341,8 @@ def run_ours(a):
     sweep = theta_sweep(B, L, pos, vel, a, d.local) if (d.rank == 0 and a.sweep) else None
     learned = learned_theta(B, L, pos, vel, a, d.local, sweep) if (d.rank == 0 and a.learned_target > 0) else None
     batching = batching_form(B, L, a, d.local) if (d.rank == 0 and a.batch_systems > 0) else None
+    precision = precision_form(B, L, a, d.local) if (d.rank == 0 and a.precision_n > 0) else None
+    field = learned_field_form(B, L, a, d.local) if (d.rank == 0 and a.field_n > 0) else None
 
     cpu = None
     if d.rank == 0 and d.world == 1 and not a.no_cpu_baseline:
@@ -376,6 +382,8 @@ def run_ours(a):
             "theta_sweep": sweep,
             "learned_theta": learned,
             "batching": batching,
+            "precision_form": precision,
+            "learned_form_clustered_field": field,
         }
         if learned:
             learned["vs_fixed_headline"] = learned["value"] / value
@@ -493,7 +501,165 @@ def learned_theta(B, L, pos, vel, a, device, sweep):
     out["fixed_theta_value_at_equal_p99"] = eq_p
     out["gain_at_equal_median"] = out["value"] / eq_m if eq_m else None
     out["gain_at_equal_p99"] = out["value"] / eq_p if eq_p else None
+    # the same network driving the double-single walk
+    ds = measure(B, L, pos, vel, samp, ref, theta=a.theta, eps=a.eps, device=device, nleaf=a.nleaf, ncrit=a.ncrit,
+                 level_split=a.level_split, dt=a.dt, steps=a.steps, precision=1, weights=w)
+    if sweep:
+        e_m = at_equal(sweep, "value", "median_rel_force_err", ds["median_rel_force_err"])
+        ds["fixed_fp32_value_at_equal_median"] = e_m
+        ds["gain_at_equal_median_vs_fixed_fp32"] = ds["value"] / e_m if e_m else None
+    out["double_single"] = ds
     return out
+
+
+def measure(B, L, pos, vel, samp, ref, *, theta, eps, device, nleaf=16, ncrit=64, level_split=5, dt=1.0 / 128,
+            steps=3, precision=0, weights=None):
+    """One configuration on one system: an eager force evaluation judged at
+    the sample particles against ref (FP64 direct sum), then `steps` timed
+    graph steps from the same initial state.  pos may be float64 (loaded as
+    double-single in precision 1, rounded to float in precision 0)."""
+    from bonsai2_b200 import learned as Lr
+    from bonsai2_b200.treecode import _p
+    n = pos.shape[0]
+    t = B.Treecode(eps=eps, theta=theta, ncrit=ncrit, nleaf=nleaf, level_split=level_split, dt=dt, device=device)
+    t.set_precision(precision)
+    if weights is not None:
+        Lr.set_weights(t, weights)
+        Lr.set_theta_mode(t, 1)
+
+    def load():
+        if pos.dtype == np.float64:
+            t.set_particles_f64(pos, vel)
+        else:
+            t.alloc(n) if t.nPtcl != n else None
+            t.nPtcl = n
+            L.bonsai_set_particles(t.handle, _p(pos), _p(vel), n)
+
+    load()
+    t.buildTree(nleaf)
+    t.computeMultipoles()
+    t.makeGroups(level_split, ncrit)
+    t.computeForces(False)
+    acc = t.get_acc()[samp].astype(np.float64)
+    err = np.linalg.norm(acc[:, :3] - ref[:, :3], axis=1) / np.linalg.norm(ref[:, :3], axis=1)
+    th = Lr.group_theta(t) if weights is not None else None
+    load()
+    t.step(1, graph=True)
+    t.synchronize()
+    ph = np.zeros(4 * steps + 1, np.float32)
+    rc = L.bonsai_step_timed(t.handle, steps, _p(ph))
+    if rc:
+        raise B.BonsaiError(rc, "measure")
+    st = np.zeros(4, np.uint64)
+    L.bonsai_get_stats(t.handle, _p(st))
+    status = t.synchronize()
+    t.close()
+    walk = float(np.median(ph[:4 * steps].reshape(steps, 4)[:, 1]))
+    ms = float(ph[4 * steps]) / steps
+    out = {"theta": theta, "value": n / (ms * 1e-3) / 1e6, "ms_per_step": ms, "walk_ms": walk,
+           "walk_tflops": (20.0 * float(st[1]) + 64.0 * float(st[0])) / (walk * 1e-3) / 1e12,
+           "approx_per_particle": float(st[0]) / n, "direct_per_particle": float(st[1]) / n,
+           "median_rel_force_err": float(np.median(err)), "p99_rel_force_err": float(np.percentile(err, 99)),
+           "status": int(status)}
+    if th is not None:
+        out["theta_mean"] = float(th.mean())
+        out["theta_p10_p90"] = [float(np.percentile(th, 10)), float(np.percentile(th, 90))]
+    return out
+
+
+def at_equal(sweep, value_key, err_key, e):
+    """Fixed-angle throughput interpolated (log-log) at error e, or None."""
+    pts = sorted(((s[err_key], s[value_key]) for s in sweep), key=lambda x: x[0])
+    for (e0, v0), (e1, v1) in zip(pts, pts[1:]):
+        if e0 <= e <= e1 and e1 > e0:
+            f = (np.log(e) - np.log(e0)) / (np.log(e1) - np.log(e0))
+            return float(np.exp(np.log(v0) + f * (np.log(v1) - np.log(v0))))
+    return None
+
+
+def precision_form(B, L, a, device):
+    """The precision form: the composite galaxy (NFW-like halo, exponential
+    disk, Hernquist bulge; log-normal masses; radii ~1e-3 to 200), double-
+    single positions against float positions at the same angle, both judged
+    against the FP64 direct sum on the exact positions (8192 samples).  Then
+    the same galaxy moved to (1e4, -7e3, 5e3) at 2^22 particles: float
+    positions lose the bulge's separations there, double-single ones do not."""
+    n = a.precision_n
+    pos, vel = B.galaxy(n, seed=a.seed)
+    rng = np.random.default_rng(8192)
+    samp = np.ascontiguousarray(np.sort(rng.choice(n, 8192, replace=False)).astype(np.int32))
+    eps = 0.01
+
+    def reference(p, sm):
+        # FP64 direct sum on the exact (double) positions
+        t = B.Treecode(eps=eps, theta=a.theta, device=device)
+        t.set_precision(1)
+        t.set_particles_f64(p, vel[:p.shape[0]])
+        r = t.direct_fp64(sm, include_self=True)
+        t.close()
+        return r
+
+    ref = reference(pos, samp)
+    out = {"config": "composite galaxy N=%d (60%% NFW r_s=10 cut 200, 30%% exp. disk R_d=3 z_d=0.3, 10%% Hernquist "
+                     "a=0.5; log-normal masses sigma 0.5), theta %.2f, eps %.3f, 8192 samples" % (n, a.theta, eps)}
+    for prec, key in ((1, "double_single"), (0, "fp32")):
+        out[key] = measure(B, L, pos, vel, samp, ref, theta=a.theta, eps=eps, device=device, precision=prec)
+    out["ds_cost"] = out["fp32"]["value"] / out["double_single"]["value"]
+    m = min(n, 1 << 22)
+    small = pos[:m].copy() if m < n else pos.copy()
+    small_samp = np.ascontiguousarray(np.sort(np.random.default_rng(4096).choice(m, 4096, replace=False)).astype(np.int32))
+    small[:, :3] += np.array([1.0e4, -7.0e3, 5.0e3])
+    ref_far = reference(small, small_samp)
+    far = {}
+    for prec, key in ((1, "double_single"), (0, "fp32")):
+        r = measure(B, L, small, vel[:m], small_samp, ref_far, theta=a.theta, eps=eps, device=device, precision=prec,
+                    steps=1)
+        far[key] = {"median_rel_force_err": r["median_rel_force_err"], "p99_rel_force_err": r["p99_rel_force_err"]}
+    out["shifted_to_1e4"] = dict(far, particles=m, shift=[1.0e4, -7.0e3, 5.0e3])
+    return out
+
+
+def learned_field_form(B, L, a, device):
+    """The learned form on the clustered field (64 Plummer subclusters plus
+    a 20 % uniform background): the network is trained on a field of another
+    seed (untimed), then learned and fixed angles are timed on the bench field
+    and judged against the FP64 direct sum (2048 samples); interactions per
+    particle and throughput at equal median and p99 error."""
+    from bonsai2_b200 import learned as Lr
+    n = a.field_n
+    eps = 0.001
+    pos, vel = B.clustered_field(n, seed=a.seed)
+    t0 = time.perf_counter()
+    ptr, vtr = B.clustered_field(n, seed=a.seed + 1)
+    X, y, _ = Lr.training_set(ptr, vtr, eps=eps, target=a.learned_target, max_groups=8192, device=device)
+    w, loss = Lr.train(X, y, epochs=3000, lr=3e-3, device=device)
+    t_train = time.perf_counter() - t0
+    del ptr, vtr
+    rng = np.random.default_rng(2048)
+    samp = np.ascontiguousarray(np.sort(rng.choice(n, 2048, replace=False)).astype(np.int32))
+    t = B.Treecode(eps=eps, theta=0.5, device=device)
+    t.alloc(n)
+    t.h_ptclPos[:] = pos
+    t.h_ptclVel[:] = vel
+    t.ptcl_h2d()
+    ref = t.direct_fp64(samp, include_self=True)
+    t.close()
+    sweep = [measure(B, L, pos, vel, samp, ref, theta=th, eps=eps, device=device)
+             for th in (0.4, 0.5, 0.6, 0.7, 0.8, 0.9, 1.0)]
+    lrn = measure(B, L, pos, vel, samp, ref, theta=0.5, eps=eps, device=device, weights=w)
+    eq_m = at_equal(sweep, "value", "median_rel_force_err", lrn["median_rel_force_err"])
+    eq_p = at_equal(sweep, "value", "p99_rel_force_err", lrn["p99_rel_force_err"])
+    ip_m = at_equal(sweep, "approx_per_particle", "median_rel_force_err", lrn["median_rel_force_err"])
+    return {"config": "clustered field N=%d: 64 Plummer subclusters (masses log-uniform over 2 decades, scale radii "
+                      "log-uniform 0.01-0.2, centres uniform in the unit cube) + 20%% uniform background; eps %.3f; "
+                      "2048 samples" % (n, eps),
+            "learned": lrn, "fixed_theta_sweep": sweep,
+            "fixed_value_at_equal_median": eq_m, "fixed_value_at_equal_p99": eq_p,
+            "gain_at_equal_median": lrn["value"] / eq_m if eq_m else None,
+            "gain_at_equal_p99": lrn["value"] / eq_p if eq_p else None,
+            "fixed_approx_per_particle_at_equal_median": ip_m,
+            "training": {"system": "clustered field seed %d" % (a.seed + 1), "pairs": int(X.shape[0]),
+                         "final_loss": loss, "seconds": t_train, "target": a.learned_target}}
 
 
 def batching_form(B, L, a, device):

@@ -2,8 +2,9 @@
 
 Accuracy is judged the reference's way, against the FP64 direct sum, here on
 the exact (double) positions.  The composite galaxy is used at the origin and
-moved far from it: FP32 positions lose the bulge's small separations there,
-double-single positions must not."""
+moved to |x| ~ 1e4, where the float spacing (~1e-3) is comparable to the
+bulge's particle separations: FP32 positions lose them there, double-single
+positions must not."""
 import numpy as np
 import pytest
 
@@ -71,7 +72,7 @@ def test_galaxy_far_from_origin_keeps_accuracy():
     res = {}
     for label, shift in (("origin", 0.0), ("far", 1.0)):
         p = pos.copy()
-        p[:, :3] += shift * np.array([1000.0, -700.0, 500.0])
+        p[:, :3] += shift * np.array([1.0e4, -7.0e3, 5.0e3])
         ref = _reference(p, vel, sample)
         for prec in (0, 1):
             t, acc = _forces(p, vel, prec)
