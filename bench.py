@@ -387,6 +387,8 @@ def run_ours(a):
         }
         if learned:
             learned["vs_fixed_headline"] = learned["value"] / value
+            for k in ("fp32", "double_single"):
+                learned["calibrated"][k]["vs_fixed_headline"] = learned["calibrated"][k]["value"] / value
         print(json.dumps(line), flush=True)
     for hptr in (hp, hv, ha):
         L.bonsai_host_free(hptr)
@@ -439,9 +441,11 @@ def learned_theta(B, L, pos, vel, a, device, sweep):
     """The learned form: per-group opening angles from the MLP, trained on a
     Plummer sphere of another seed (untimed setup), then timed on the bench
     system like the headline and judged against the FP64 direct sum; compared
-    with the fixed angles of the sweep at equal median and equal p99 error."""
+    with the fixed angles of the sweep at equal median and equal p99 error.
+    Reported raw, and calibrated (one scale on the network's angles, set by
+    bisection on the training system to 0.9 x the target median error) in
+    float and double-single positions."""
     from bonsai2_b200 import learned as Lr
-    from bonsai2_b200.treecode import _p
     n = pos.shape[0]
     t0 = time.perf_counter()
     ptr, vtr = B.plummer(n, a.seed + 1)
@@ -449,71 +453,46 @@ def learned_theta(B, L, pos, vel, a, device, sweep):
                               ncrit=a.ncrit, level_split=a.level_split, device=device)
     w, loss = Lr.train(X, y, epochs=3000, lr=3e-3, device=device)
     t_train = time.perf_counter() - t0
-    t = B.Treecode(eps=a.eps, theta=a.theta, ncrit=a.ncrit, nleaf=a.nleaf, level_split=a.level_split, dt=a.dt,
-                   device=device)
-    t.alloc(n)
-    Lr.set_weights(t, w)
-    Lr.set_theta_mode(t, 1)
-    L.bonsai_set_particles(t.handle, _p(pos), _p(vel), n)
-    t.buildTree(a.nleaf)
-    t.computeMultipoles()
-    t.makeGroups(a.level_split, a.ncrit)
-    t.computeForces(False)
-    acc = t.get_acc().astype(np.float64)
-    th = Lr.group_theta(t)
+    c, lo, hi, e_cal = Lr.calibrate(ptr, vtr, w, a.eps, a.learned_target, nleaf=a.nleaf, ncrit=a.ncrit,
+                                    level_split=a.level_split, device=device)
+    del ptr, vtr
     rng = np.random.default_rng(2048)
-    samp = np.ascontiguousarray(rng.choice(n, min(2048, n), replace=False).astype(np.int32))
+    samp = np.ascontiguousarray(np.sort(rng.choice(n, min(2048, n), replace=False)).astype(np.int32))
+    t = B.Treecode(eps=a.eps, theta=a.theta, device=device)
+    t.alloc(n)
+    t.h_ptclPos[:] = pos
+    t.h_ptclVel[:] = vel
+    t.ptcl_h2d()
     ref = t.direct_fp64(samp, include_self=True)
-    err = np.linalg.norm(acc[samp, :3] - ref[:, :3], axis=1) / np.linalg.norm(ref[:, :3], axis=1)
-    L.bonsai_set_particles(t.handle, _p(pos), _p(vel), n)
-    t.step(2, graph=True)
-    t.synchronize()
-    ph = np.zeros(4 * a.steps + 1, np.float32)
-    rc = L.bonsai_step_timed(t.handle, a.steps, _p(ph))
-    if rc:
-        raise B.BonsaiError(rc, "learned steps")
-    st = np.zeros(4, np.uint64)
-    L.bonsai_get_stats(t.handle, _p(st))
     t.close()
-    ms = float(ph[4 * a.steps]) / a.steps
-    walk = float(np.median(ph[:4 * a.steps].reshape(a.steps, 4)[:, 1]))
-    flops_pp = (20.0 * float(st[1]) + 64.0 * float(st[0])) / n
-    med, p99 = float(np.median(err)), float(np.percentile(err, 99))
+    kw = dict(theta=a.theta, eps=a.eps, device=device, nleaf=a.nleaf, ncrit=a.ncrit, level_split=a.level_split,
+              dt=a.dt, steps=a.steps, weights=w)
 
-    def at_equal(key):
-        # fixed-angle throughput at the learned error, log-log between sweep points
-        pts = sorted(((s[key], s["value"]) for s in (sweep or [])), key=lambda x: x[0])
-        e = med if key == "median_rel_force_err" else p99
-        for (e0, v0), (e1, v1) in zip(pts, pts[1:]):
-            if e0 <= e <= e1 and e1 > e0:
-                f = (np.log(e) - np.log(e0)) / (np.log(e1) - np.log(e0))
-                return float(np.exp(np.log(v0) + f * (np.log(v1) - np.log(v0))))
-        return None
+    def compare(r):
+        if sweep:
+            em = at_equal(sweep, "value", "median_rel_force_err", r["median_rel_force_err"])
+            ep = at_equal(sweep, "value", "p99_rel_force_err", r["p99_rel_force_err"])
+            r["fixed_theta_value_at_equal_median"] = em
+            r["fixed_theta_value_at_equal_p99"] = ep
+            r["gain_at_equal_median"] = r["value"] / em if em else None
+            r["gain_at_equal_p99"] = r["value"] / ep if ep else None
+        return r
 
-    out = {"value": n / (ms * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": ms, "walk_ms": walk,
-           "walk_tflops": flops_pp * n / (walk * 1e-3) / 1e12, "flops_per_particle": flops_pp,
-           "median_rel_force_err": med, "p99_rel_force_err": p99, "target": a.learned_target,
-           "theta_mean": float(th.mean()), "theta_p10_p90": [float(np.percentile(th, 10)), float(np.percentile(th, 90))],
-           "training": {"system": "Plummer N=%d seed %d" % (n, a.seed + 1), "pairs": int(X.shape[0]),
-                        "final_loss": loss, "seconds": t_train}}
-    eq_m, eq_p = at_equal("median_rel_force_err"), at_equal("p99_rel_force_err")
-    out["fixed_theta_value_at_equal_median"] = eq_m
-    out["fixed_theta_value_at_equal_p99"] = eq_p
-    out["gain_at_equal_median"] = out["value"] / eq_m if eq_m else None
-    out["gain_at_equal_p99"] = out["value"] / eq_p if eq_p else None
-    # the same network driving the double-single walk
-    ds = measure(B, L, pos, vel, samp, ref, theta=a.theta, eps=a.eps, device=device, nleaf=a.nleaf, ncrit=a.ncrit,
-                 level_split=a.level_split, dt=a.dt, steps=a.steps, precision=1, weights=w)
-    if sweep:
-        e_m = at_equal(sweep, "value", "median_rel_force_err", ds["median_rel_force_err"])
-        ds["fixed_fp32_value_at_equal_median"] = e_m
-        ds["gain_at_equal_median_vs_fixed_fp32"] = ds["value"] / e_m if e_m else None
-    out["double_single"] = ds
+    out = compare(measure(B, L, pos, vel, samp, ref, **kw))
+    out["unit"] = UNIT
+    out["target"] = a.learned_target
+    out["training"] = {"system": "Plummer N=%d seed %d" % (n, a.seed + 1), "pairs": int(X.shape[0]),
+                       "final_loss": loss, "seconds": t_train}
+    out["calibrated"] = {
+        "scale": c, "theta_range": [lo, hi], "median_err_on_training_system": e_cal,
+        "fp32": compare(measure(B, L, pos, vel, samp, ref, theta_range=(lo, hi), **kw)),
+        "double_single": compare(measure(B, L, pos, vel, samp, ref, theta_range=(lo, hi), precision=1, **kw)),
+    }
     return out
 
 
 def measure(B, L, pos, vel, samp, ref, *, theta, eps, device, nleaf=16, ncrit=64, level_split=5, dt=1.0 / 128,
-            steps=3, precision=0, weights=None):
+            steps=3, precision=0, weights=None, theta_range=None):
     """One configuration on one system: an eager force evaluation judged at
     the sample particles against ref (FP64 direct sum), then `steps` timed
     graph steps from the same initial state.  pos may be float64 (loaded as
@@ -525,7 +504,7 @@ def measure(B, L, pos, vel, samp, ref, *, theta, eps, device, nleaf=16, ncrit=64
     t.set_precision(precision)
     if weights is not None:
         Lr.set_weights(t, weights)
-        Lr.set_theta_mode(t, 1)
+        Lr.set_theta_mode(t, 1, *(theta_range or (Lr.LO, Lr.HI)))
 
     def load():
         if pos.dtype == np.float64:
@@ -634,6 +613,7 @@ def learned_field_form(B, L, a, device):
     X, y, _ = Lr.training_set(ptr, vtr, eps=eps, target=a.learned_target, max_groups=8192, device=device)
     w, loss = Lr.train(X, y, epochs=3000, lr=3e-3, device=device)
     t_train = time.perf_counter() - t0
+    c, lo, hi, e_cal = Lr.calibrate(ptr, vtr, w, eps, a.learned_target, device=device)
     del ptr, vtr
     rng = np.random.default_rng(2048)
     samp = np.ascontiguousarray(np.sort(rng.choice(n, 2048, replace=False)).astype(np.int32))
@@ -647,13 +627,21 @@ def learned_field_form(B, L, a, device):
     sweep = [measure(B, L, pos, vel, samp, ref, theta=th, eps=eps, device=device)
              for th in (0.4, 0.5, 0.6, 0.7, 0.8, 0.9, 1.0)]
     lrn = measure(B, L, pos, vel, samp, ref, theta=0.5, eps=eps, device=device, weights=w)
+    cal = measure(B, L, pos, vel, samp, ref, theta=0.5, eps=eps, device=device, weights=w, theta_range=(lo, hi))
+    for r in (cal,):
+        em = at_equal(sweep, "value", "median_rel_force_err", r["median_rel_force_err"])
+        ep = at_equal(sweep, "value", "p99_rel_force_err", r["p99_rel_force_err"])
+        r["gain_at_equal_median"] = r["value"] / em if em else None
+        r["gain_at_equal_p99"] = r["value"] / ep if ep else None
+        r["scale"] = c
+        r["median_err_on_training_field"] = e_cal
     eq_m = at_equal(sweep, "value", "median_rel_force_err", lrn["median_rel_force_err"])
     eq_p = at_equal(sweep, "value", "p99_rel_force_err", lrn["p99_rel_force_err"])
     ip_m = at_equal(sweep, "approx_per_particle", "median_rel_force_err", lrn["median_rel_force_err"])
     return {"config": "clustered field N=%d: 64 Plummer subclusters (masses log-uniform over 2 decades, scale radii "
                       "log-uniform 0.01-0.2, centres uniform in the unit cube) + 20%% uniform background; eps %.3f; "
                       "2048 samples" % (n, eps),
-            "learned": lrn, "fixed_theta_sweep": sweep,
+            "learned": lrn, "learned_calibrated": cal, "fixed_theta_sweep": sweep,
             "fixed_value_at_equal_median": eq_m, "fixed_value_at_equal_p99": eq_p,
             "gain_at_equal_median": lrn["value"] / eq_m if eq_m else None,
             "gain_at_equal_p99": lrn["value"] / eq_p if eq_p else None,

@@ -158,3 +158,52 @@ def training_set(pos, vel, eps, thetas=DEFAULT_GRID, target=5e-4, samples_per_gr
         return F[gsel], label.astype(np.float32), E
     finally:
         t.close()
+
+
+def calibrate(pos, vel, w, eps, target, fraction=0.9, samples=2048, iters=10, nleaf=16, ncrit=64, level_split=5,
+              seed=0, device=0):
+    """Scale c of the network's angle range (every group's angle becomes c
+    times the network's), found by bisection on log c so that the median
+    |da|/|a| of the system (pos, vel) against the FP64 direct sum is
+    fraction * target.  Returns (c, lo * c, hi * c, median error at c).  The
+    network's raw output sits below the target by design (its loss penalises
+    too-large angles more); this one scalar moves it onto the target on a
+    training system."""
+    n = pos.shape[0]
+    t = Treecode(eps=eps, theta=0.5, ncrit=ncrit, nleaf=nleaf, level_split=level_split, device=device)
+    try:
+        t.alloc(n)
+        t.h_ptclPos[:] = pos
+        t.h_ptclVel[:] = vel
+        t.ptcl_h2d()
+        rng = np.random.default_rng(seed)
+        samp = np.ascontiguousarray(np.sort(rng.choice(n, min(samples, n), replace=False)).astype(np.int32))
+        ref = t.direct_fp64(samp, include_self=True)
+        refn = np.linalg.norm(ref[:, :3], axis=1)
+        set_weights(t, w)
+        t.buildTree(nleaf)
+        t.computeMultipoles()
+        t.makeGroups(level_split, ncrit)
+
+        def median_err(c):
+            set_theta_mode(t, 1, LO * c, HI * c)
+            t.computeForces(False)
+            acc = t.get_acc()[samp].astype(np.float64)
+            return float(np.median(np.linalg.norm(acc[:, :3] - ref[:, :3], axis=1) / refn))
+
+        goal = fraction * target
+        lo_c, hi_c = 0.5, 2.0
+        e_lo, e_hi = median_err(lo_c), median_err(hi_c)
+        if e_lo > goal:
+            return lo_c, LO * lo_c, HI * lo_c, e_lo
+        if e_hi < goal:
+            return hi_c, LO * hi_c, HI * hi_c, e_hi
+        for _ in range(iters):
+            mid = float(np.sqrt(lo_c * hi_c))
+            if median_err(mid) > goal:
+                hi_c = mid
+            else:
+                lo_c = mid
+        return lo_c, LO * lo_c, HI * lo_c, median_err(lo_c)
+    finally:
+        t.close()
