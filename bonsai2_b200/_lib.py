@@ -65,6 +65,7 @@ SIGNATURES = {
     "bonsai_set_group_theta": (I, [P, P, I]),
     "bonsai_get_group_features": (I, [P, P, P]),
     "bonsai_get_group_theta": (I, [P, P]),
+    "bonsai_get_group_interactions": (I, [P, P]),
     "bonsai_mlp_loss_grad": (I, [I, P, P, I, P, ctypes.c_float, ctypes.c_float, ctypes.c_float, P, P]),
     "bonsai_mlp_train": (I, [I, P, P, I, P, I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, P]),
     "bonsai_mlp_predict": (I, [I, P, I, P, ctypes.c_float, ctypes.c_float, P]),

@@ -76,7 +76,7 @@ void launch_walk(int variant, int nblocks, const int2* groups, const TreeInfo* i
                  const float2* cell_ls, const float* group_inv_theta, float eps2, float4* acc, int* ring_pool,
                  int ring_cap, unsigned* group_counter, unsigned long long* stats, int* status, const int* sys_off,
                  int nsys, const int* root_beg, const float4* ipos_lo, const float4* jpos_lo, const float4* cell_lo,
-                 cudaStream_t s);
+                 uint2* group_counts, cudaStream_t s);
 
 // move.cu
 // lo (nullable): double-single position low parts, drifted with the high parts

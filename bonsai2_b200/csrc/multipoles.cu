@@ -4,11 +4,11 @@
 // The reference (computeCellMultipoles, computeMultipoles.cu:81-190) gives a
 // warp to every cell and rescans all of that cell's particles, O(N * depth)
 // particle reads, with float products summed in double.  Here each leaf is
-// reduced from its own particles (one half-warp per leaf, FP64, two passes:
+// reduced from its own particles (one thread per leaf, FP64, two passes:
 // centre of mass, then central moments), and every node is combined from its
 // children with the parallel-axis theorem by the child that finishes last
-// (an acquire-release arrival counter per cell; no thread waits on another).
-// Each particle is read once from HBM.  The quantities match the reference's definitions:
+// (an arrival counter per cell; no thread waits on another).
+// Each particle is read once.  The quantities match the reference's definitions:
 //   M, COM; Q = second moment about the COM per unit mass (:148-158);
 //   particle bounding box -> l = max(2 max h, 1e-6), s = |cvec - COM|,
 //   cellOp = l/theta + s, stored squared (:168-177).
@@ -64,30 +64,16 @@ __device__ __forceinline__ void store_cell(int c, const MpRec& r, float inv_thet
   cell_q1[c] = make_float4((float)(3.0 * r.ixy), (float)(3.0 * r.ixz), (float)(3.0 * r.iyz), (float)(1.5 * tr));
 }
 
-// Arrival on a parent's counter with acquire-release semantics: the
-// arriving child's record stores are released to, and the last arriver
-// acquires every sibling's, without separate fences.
-__device__ __forceinline__ int arrive_acq_rel(int* p) {
-  int old;
-  asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;" : "=r"(old) : "l"(p) : "memory");
-  return old;
-}
-
-// fixed-order reductions over the 16 lanes of a half-warp
-__device__ __forceinline__ double half_sum(double v, unsigned mask) {
-#pragma unroll
-  for (int o = 8; o >= 1; o >>= 1) v += __shfl_xor_sync(mask, v, o, 16);
-  return v;
-}
-__device__ __forceinline__ double half_min(double v, unsigned mask) {
-#pragma unroll
-  for (int o = 8; o >= 1; o >>= 1) v = fmin(v, __shfl_xor_sync(mask, v, o, 16));
-  return v;
-}
-__device__ __forceinline__ double half_max(double v, unsigned mask) {
-#pragma unroll
-  for (int o = 8; o >= 1; o >>= 1) v = fmax(v, __shfl_xor_sync(mask, v, o, 16));
-  return v;
+// Arrival on a parent's counter: a fence publishes this child's record, a
+// relaxed atomic counts it, and only the last arriver fences again before it
+// reads its siblings' records (through L2).  (An acquire-release atomic per
+// arrival was measured 16x slower here: a GPU-scope acquire invalidates the
+// SM's L1, which the leaf loads of every other warp depend on.)
+__device__ __forceinline__ bool arrive_last(int* p, int nch) {
+  __threadfence();
+  if (atomicAdd(p, 1) != nch - 1) return false;
+  __threadfence();
+  return true;
 }
 
 __device__ __forceinline__ void particle_ds(const float4* __restrict__ jpos, const float4* __restrict__ jlo, int i,
@@ -110,7 +96,7 @@ __device__ void climb(int c, const uint4* __restrict__ cell_data, const int* __r
     if (p < 0) break;
     const unsigned y = cell_data[p].y;
     const int first = (int)(y & 0x1FFFFFFFu), nch = (int)(y >> 29) + 1;
-    if (arrive_acq_rel(mp_count + p) != nch - 1) break;
+    if (!arrive_last(mp_count + p, nch)) break;
     double M = 0, X = 0, Y = 0, Z = 0;
     double bmn[3] = {3.0e38, 3.0e38, 3.0e38}, bmx[3] = {-3.0e38, -3.0e38, -3.0e38};
     for (int k = 0; k < nch; k++) {
@@ -146,9 +132,9 @@ __device__ void climb(int c, const uint4* __restrict__ cell_data, const int* __r
   }
 }
 
-// One half-warp per leaf: its lanes read the leaf's particles coalesced (16
-// at a time, larger leaves loop), the FP64 sums are fixed-order xor trees over
-// the half, and lane 0 stores the leaf and climbs.
+// One thread per leaf: two passes over the leaf's particles (COM, then
+// central moments), then the bottom-up climb.  (Half-warp-cooperative leaves
+// with shuffle reductions were measured 16x slower on the B200.)
 __global__ void __launch_bounds__(256) k_multipoles(const int* __restrict__ leaf_list, const TreeInfo* __restrict__ info,
                                                     const uint4* __restrict__ cell_data,
                                                     const int* __restrict__ cell_parent,
@@ -160,16 +146,14 @@ __global__ void __launch_bounds__(256) k_multipoles(const int* __restrict__ leaf
                                                     float4* __restrict__ cell_lo) {
   const int nleaves = info->nleaves;
   if (info->ncells > cell_cap) return;
-  const int sub = threadIdx.x & 15;
-  const unsigned hmask = (threadIdx.x & 16) ? 0xFFFF0000u : 0x0000FFFFu;
-  const int nh = (gridDim.x * blockDim.x) >> 4;
-  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 4; t < nleaves; t += nh) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nleaves; t += gridDim.x * blockDim.x) {
     const int c = leaf_list[t];
     const uint4 cd = cell_data[c];
     const int b = (int)cd.z, e = (int)cd.w;
+    MpRec r;
     double m = 0, sx = 0, sy = 0, sz = 0;
     double mn[3] = {3.0e38, 3.0e38, 3.0e38}, mx[3] = {-3.0e38, -3.0e38, -3.0e38};
-    for (int i = b + sub; i < e; i += 16) {
+    for (int i = b; i < e; i++) {
       double px, py, pz, w;
       particle_ds(jpos, jlo, i, px, py, pz, w);
       m += w;
@@ -177,28 +161,21 @@ __global__ void __launch_bounds__(256) k_multipoles(const int* __restrict__ leaf
       mn[0] = fmin(mn[0], px); mn[1] = fmin(mn[1], py); mn[2] = fmin(mn[2], pz);
       mx[0] = fmax(mx[0], px); mx[1] = fmax(mx[1], py); mx[2] = fmax(mx[2], pz);
     }
-    m = half_sum(m, hmask);
-    sx = half_sum(sx, hmask); sy = half_sum(sy, hmask); sz = half_sum(sz, hmask);
-    for (int k = 0; k < 3; k++) { mn[k] = half_min(mn[k], hmask); mx[k] = half_max(mx[k], hmask); }
-    MpRec r;
     if (m > 0.0) { r.cx = sx / m; r.cy = sy / m; r.cz = sz / m; }
     else { r.cx = 0.5 * (mn[0] + mx[0]); r.cy = 0.5 * (mn[1] + mx[1]); r.cz = 0.5 * (mn[2] + mx[2]); }
     double q[6] = {0, 0, 0, 0, 0, 0};
-    for (int i = b + sub; i < e; i += 16) {
+    for (int i = b; i < e; i++) {
       double px, py, pz, w;
       particle_ds(jpos, jlo, i, px, py, pz, w);
       const double dx = px - r.cx, dy = py - r.cy, dz = pz - r.cz;
       q[0] += w * dx * dx; q[1] += w * dy * dy; q[2] += w * dz * dz;
       q[3] += w * dx * dy; q[4] += w * dx * dz; q[5] += w * dy * dz;
     }
-    for (int k = 0; k < 6; k++) q[k] = half_sum(q[k], hmask);
-    if (sub == 0) {
-      r.m = m;
-      r.ixx = q[0]; r.iyy = q[1]; r.izz = q[2]; r.ixy = q[3]; r.ixz = q[4]; r.iyz = q[5];
-      for (int k = 0; k < 3; k++) { r.bmin[k] = mn[k]; r.bmax[k] = mx[k]; }
-      store_cell(c, r, inv_theta, rec, cell_open, cell_q0, cell_q1, cell_ls, cell_lo);
-      climb(c, cell_data, cell_parent, inv_theta, rec, cell_open, cell_q0, cell_q1, cell_ls, mp_count, cell_lo);
-    }
+    r.m = m;
+    r.ixx = q[0]; r.iyy = q[1]; r.izz = q[2]; r.ixy = q[3]; r.ixz = q[4]; r.iyz = q[5];
+    for (int k = 0; k < 3; k++) { r.bmin[k] = mn[k]; r.bmax[k] = mx[k]; }
+    store_cell(c, r, inv_theta, rec, cell_open, cell_q0, cell_q1, cell_ls, cell_lo);
+    climb(c, cell_data, cell_parent, inv_theta, rec, cell_open, cell_q0, cell_q1, cell_ls, mp_count, cell_lo);
   }
 }
 

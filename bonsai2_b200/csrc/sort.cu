@@ -7,7 +7,10 @@
 // 8 passes of 8 bits, one-sweep (below): keys are ranked stably inside each
 // 4096-key tile with warp match_any and per-warp digit counters in shared
 // memory, tile offsets come from a decoupled look-back, and tiles are written
-// out through shared memory in contiguous digit runs.
+// out through shared memory in contiguous digit runs.  A thread keeps only the
+// 16 ranks and packed digits of its keys across the look-back (the keys are
+// re-read from L2 for staging): 80 registers, 3 blocks per SM (keeping the
+// keys, 127 registers and 2 blocks per SM, was 16 % slower per sort).
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -155,7 +158,7 @@ __global__ void __launch_bounds__(256) k_sort_hist_scan(unsigned* __restrict__ g
 // value, the element's position in the sort's input order), not of its key:
 // the passes that make an ensemble sort stable-partition by system last.
 template <bool SYSD>
-__global__ void __launch_bounds__(kSortThreads) k_sort_onesweep(
+__global__ void __launch_bounds__(kSortThreads, 3) k_sort_onesweep(
     const unsigned long long* __restrict__ keys_in, const int* __restrict__ vals_in, int n, int shift,
     const unsigned* __restrict__ gbase, unsigned* __restrict__ status, unsigned* __restrict__ tile_counter,
     unsigned long long* __restrict__ keys_out, int* __restrict__ vals_out, int* __restrict__ err,
@@ -164,7 +167,7 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_onesweep(
   __shared__ unsigned tile_off[256];
   __shared__ unsigned dstart[256];
   __shared__ unsigned long long stage[kSortTile];  // keys, then values (as 32-bit) in digit order
-  __shared__ unsigned char sdig[SYSD ? kSortTile : 1];
+  __shared__ unsigned char sdig[kSortTile];
   __shared__ unsigned sh[32];
   __shared__ int tile_sh;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -173,22 +176,20 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_onesweep(
   __syncthreads();
   const int tile = tile_sh;
   const int base = tile * kSortTile + w * (32 * kSortItems);
-  unsigned long long key[kSortItems];
   unsigned rank[kSortItems];
-  unsigned dpack[SYSD ? kSortItems / 4 : 1];
+  unsigned dpack[kSortItems / 4];
 #pragma unroll
   for (int k = 0; k < kSortItems; k++) {
     const int i = base + k * 32 + lane;
     const bool ok = i < n;
-    key[k] = ok ? keys_in[i] : 0ull;
     unsigned d;
     if constexpr (SYSD) {
       d = ok ? (((unsigned)sys_of(sys_off, nsys, vals_in ? vals_in[i] : i) >> shift) & 255u) : 256u;
-      if ((k & 3) == 0) dpack[k >> 2] = 0u;
-      dpack[k >> 2] |= (d & 255u) << (8 * (k & 3));
     } else {
-      d = ok ? ((unsigned)(key[k] >> shift) & 255u) : 256u;
+      d = ok ? ((unsigned)(keys_in[i] >> shift) & 255u) : 256u;
     }
+    if ((k & 3) == 0) dpack[k >> 2] = 0u;
+    dpack[k >> 2] |= (d & 255u) << (8 * (k & 3));
     const unsigned peers = __match_any_sync(kFull, d);
     const unsigned before = (unsigned)__popc(peers & lanemask_lt());
     const unsigned cur = ok ? wcnt[w][d] : 0u;
@@ -235,43 +236,35 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_onesweep(
     dstart[d] = gbase[d] + excl;
   }
   __syncthreads();
-  // stage keys in digit order, write contiguous runs
+  // stage keys in digit order (re-read from L2), write contiguous runs
   const int tile_n = min(kSortTile, n - tile * kSortTile);
   unsigned lpos[kSortItems];
 #pragma unroll
   for (int k = 0; k < kSortItems; k++) {
     const int i = base + k * 32 + lane;
     if (i < n) {
-      unsigned dd;
-      if constexpr (SYSD) dd = (dpack[k >> 2] >> (8 * (k & 3))) & 255u;
-      else dd = (unsigned)(key[k] >> shift) & 255u;
+      const unsigned dd = (dpack[k >> 2] >> (8 * (k & 3))) & 255u;
       lpos[k] = tile_off[dd] + wcnt[w][dd] + rank[k];
-      stage[lpos[k]] = key[k];
-      if constexpr (SYSD) sdig[lpos[k]] = (unsigned char)dd;
+      stage[lpos[k]] = keys_in[i];
+      sdig[lpos[k]] = (unsigned char)dd;
     }
   }
   __syncthreads();
   for (int j = threadIdx.x; j < tile_n; j += kSortThreads) {
     const unsigned long long kk = stage[j];
-    unsigned dd;
-    if constexpr (SYSD) dd = sdig[j];
-    else dd = (unsigned)(kk >> shift) & 255u;
+    const unsigned dd = sdig[j];
     keys_out[dstart[dd] + (unsigned)j - tile_off[dd]] = kk;
   }
   __syncthreads();
   unsigned* stage32 = reinterpret_cast<unsigned*>(stage);
-  unsigned char* digit_of = SYSD ? sdig : reinterpret_cast<unsigned char*>(stage32 + kSortTile);
 #pragma unroll
   for (int k = 0; k < kSortItems; k++) {
     const int i = base + k * 32 + lane;
-    if (i < n) {
-      stage32[lpos[k]] = (unsigned)(vals_in ? vals_in[i] : i);
-      if constexpr (!SYSD) digit_of[lpos[k]] = (unsigned char)((unsigned)(key[k] >> shift) & 255u);
-    }
+    if (i < n) stage32[lpos[k]] = (unsigned)(vals_in ? vals_in[i] : i);
   }
   __syncthreads();
   for (int j = threadIdx.x; j < tile_n; j += kSortThreads) {
-    const unsigned dd = digit_of[j];
+    const unsigned dd = sdig[j];
     vals_out[dstart[dd] + (unsigned)j - tile_off[dd]] = (int)stage32[j];
   }
 }

@@ -71,6 +71,7 @@ struct Handle {
   int gcap = 0;
   float* group_inv = nullptr;
   float* group_feat = nullptr;
+  uint2* group_counts = nullptr;  // per-group (approx, direct) counts of the per-group angle walk
   float* mlp_w = nullptr;
   void* mlp_wh = nullptr;
   bool mlp_loaded = false;
@@ -157,6 +158,7 @@ struct Handle {
     dfree(&acc); dfree(&jpos); dfree(&tkey); dfree(&pkey); dfree(&kalt);
     dfree(&tperm); dfree(&pperm); dfree(&valt); dfree(&sort_counts); dfree(&bsum);
     dfree(&dlev); dfree(&chain); dfree(&hist); dfree(&groups); dfree(&group_inv); dfree(&group_feat);
+    dfree(&group_counts);
     release_cells();
     n = 0;
   }
@@ -269,6 +271,7 @@ struct Handle {
     gcap = (int)std::min<long long>(N, (long long)N / std::max(1, prm.ncrit) + (1ll << (3 * kMaxLevelSplit)) + 1);
     BONSAI_CUDA_TRY(dalloc(&group_inv, (size_t)gcap));
     BONSAI_CUDA_TRY(dalloc(&group_feat, (size_t)gcap * kMlpFeatures));
+    BONSAI_CUDA_TRY(dalloc(&group_counts, (size_t)gcap));
     // the reference reserves nPtcl cells (Treecode.h:192); a Plummer tree at
     // nLeaf 16 uses ~0.23 N.  Grown on demand by the eager build.
     int rc = alloc_cells(prm.nleaf >= 8 ? nn / 2 + 4096 : 2 * nn + 4096);
@@ -390,7 +393,7 @@ struct Handle {
     }
     launch_walk(k, walk_blocks[k], groups, info, pos[par], jpos, cell_data, cell_open, cell_q0, cell_q1, cell_ls,
                 ginv, prm.eps * prm.eps, acc, ring, kRingCap, group_counter, stats, &info->status, so(), nsys, root_beg,
-                precision ? plo[par] : nullptr, jlo, cell_lo, st);
+                precision ? plo[par] : nullptr, jlo, cell_lo, ginv ? group_counts : nullptr, st);
   }
   void enq_move(bool write) {
     launch_move_wrapper(write);
@@ -1199,6 +1202,21 @@ int bonsai_get_group_features(bonsai_handle hh, float* out, int* ngroups) {
   BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
   *ngroups = ng;
   return last_cuda();
+}
+
+int bonsai_get_group_interactions(bonsai_handle hh, unsigned* out) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (!out) return BONSAI_ERR_ARG;
+  if (h->theta_mode == 0 || !h->forced) return BONSAI_ERR_ORDER;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  int ng = 0;
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(&ng, &h->info->ngroups, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  if (ng > h->gcap) return BONSAI_STATUS_GROUP_CAPACITY;
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(out, h->group_counts, (size_t)ng * 8, cudaMemcpyDeviceToHost, h->st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  return 0;
 }
 
 int bonsai_get_group_theta(bonsai_handle hh, float* out) {

@@ -143,7 +143,8 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
            int* __restrict__ ring_pool, int ring_cap, unsigned* __restrict__ group_counter,
            unsigned long long* __restrict__ stats, int* __restrict__ status, const int* __restrict__ sys_off,
            int nsys, const int* __restrict__ root_beg, const float4* __restrict__ ipos_lo,
-           const float4* __restrict__ jpos_lo, const float4* __restrict__ cell_lo) {
+           const float4* __restrict__ jpos_lo, const float4* __restrict__ cell_lo,
+           uint2* __restrict__ group_counts) {
   constexpr int STRIDE = SPLIT ? 16 : 32;
   constexpr int JSTEP = SPLIT ? 2 : 1;
   __shared__ float4 s_a0[kWalkWarps][64];
@@ -367,6 +368,8 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
         if (idx < np) acc[pbeg + idx] = ai[k];
       }
     }
+    // per-group (approximate, direct) interaction counts, for the per-group angle variant
+    if (PERGROUP && group_counts && lane == 0) group_counts[g] = make_uint2(n_app, n_dir);
     sum_app += (unsigned long long)n_app * (unsigned long long)np;
     sum_dir += (unsigned long long)n_dir * (unsigned long long)np;
     max_app = max(max_app, n_app);
@@ -427,10 +430,10 @@ void launch_walk(int variant, int nblocks, const int2* groups, const TreeInfo* i
                  const float4* cell_q1, const float2* cell_ls, const float* group_inv_theta, float eps2,
                  float4* acc, int* ring_pool, int ring_cap, unsigned* group_counter, unsigned long long* stats,
                  int* status, const int* sys_off, int nsys, const int* root_beg, const float4* ipos_lo,
-                 const float4* jpos_lo, const float4* cell_lo, cudaStream_t s) {
+                 const float4* jpos_lo, const float4* cell_lo, uint2* group_counts, cudaStream_t s) {
 #define BONSAI_WALK_ARGS                                                                                          \
   groups, info, ipos, jpos, cell_data, cell_open, cell_q0, cell_q1, cell_ls, group_inv_theta, eps2, acc, ring_pool, \
-      ring_cap, group_counter, stats, status, sys_off, nsys, root_beg, ipos_lo, jpos_lo, cell_lo
+      ring_cap, group_counter, stats, status, sys_off, nsys, root_beg, ipos_lo, jpos_lo, cell_lo, group_counts
 #define BONSAI_WALK(NI, SP)                                                                \
   do {                                                                                     \
     if (nsys > 1)                                                                          \

@@ -94,14 +94,22 @@ def group_theta(t: Treecode) -> np.ndarray:
 DEFAULT_GRID = tuple(np.round(np.arange(0.30, 1.2501, 0.05), 2))
 
 
-def training_set(pos, vel, eps, thetas=DEFAULT_GRID, target=5e-4, samples_per_group=8, max_groups=8192, seed=0,
-                 nleaf=16, ncrit=64, level_split=5, device=0):
-    """(features, label theta, error table) for a random subset of groups.
+def group_interactions(t: Treecode) -> np.ndarray:
+    """(G, 2) approximate and direct interaction counts per group of the last
+    walk with per-group angles."""
+    G = t.tree_info()["ngroups"]
+    out = np.empty((max(G, 1), 2), np.uint32)
+    _check(t._L.bonsai_get_group_interactions(t.handle, _p(out)), "get_group_interactions")
+    return out[:G]
 
-    The label is the angle at which the group's error (geometric mean over its
-    sampled particles of |da|/|a| against the FP64 direct sum) crosses the
-    target, interpolated linearly in log error between grid angles; clipped to
-    the grid's ends."""
+
+def training_tables(pos, vel, eps, thetas=DEFAULT_GRID, samples_per_group=8, max_groups=8192, seed=0, nleaf=16,
+                    ncrit=64, level_split=5, device=0):
+    """For a random subset of groups: features F (g, 16); error table E (g, k)
+    = geometric mean over the group's sampled particles of |da|/|a| against
+    the FP64 direct sum with every group at angle thetas[k]; cost table C
+    (g, k) = 64 n_approx + 20 n_direct of the group's warp (the walk's model
+    flops; a warp evaluates all its particle slots); group sizes (g,)."""
     n = pos.shape[0]
     t = Treecode(eps=eps, theta=0.5, ncrit=ncrit, nleaf=nleaf, level_split=level_split, device=device)
     try:
@@ -131,6 +139,7 @@ def training_set(pos, vel, eps, thetas=DEFAULT_GRID, target=5e-4, samples_per_gr
         refn = np.linalg.norm(ref[:, :3], axis=1)
         set_theta_mode(t, 2)
         E = np.zeros((gsel.shape[0], len(thetas)))
+        C = np.zeros((gsel.shape[0], len(thetas)))
         for j, th in enumerate(thetas):
             set_group_theta(t, np.full(G, th, np.float32))
             t.computeForces(False)
@@ -139,25 +148,101 @@ def training_set(pos, vel, eps, thetas=DEFAULT_GRID, target=5e-4, samples_per_gr
             le = np.log(np.maximum(err, 1e-30))
             E[:, j] = np.exp(np.bincount(owner, weights=le, minlength=gsel.shape[0]) /
                              np.bincount(owner, minlength=gsel.shape[0]))
-        th = np.asarray(thetas, np.float64)
-        lt = np.log(target)
-        logE = np.log(np.maximum(E, 1e-30))
-        label = np.full(gsel.shape[0], th[0])
-        for g in range(gsel.shape[0]):
-            above = np.nonzero(logE[g] > lt)[0]
-            if above.size == 0:
-                label[g] = th[-1]
-                continue
-            j = above[0]
-            if j == 0:
-                label[g] = th[0]
-                continue
-            e0, e1 = logE[g, j - 1], logE[g, j]
-            f = (lt - e0) / (e1 - e0) if e1 > e0 else 0.0
-            label[g] = th[j - 1] + f * (th[j] - th[j - 1])
-        return F[gsel], label.astype(np.float32), E
+            cnt = group_interactions(t)[gsel].astype(np.float64)
+            C[:, j] = 64.0 * cnt[:, 0] + 20.0 * cnt[:, 1]
+        return F[gsel], E, C, groups[gsel, 1].astype(np.float64)
     finally:
         t.close()
+
+
+def crossing_labels(E, thetas, target):
+    """Per group, the angle at which its error crosses the target
+    (interpolated linearly in log error between grid angles, clipped to the
+    grid's ends): every group made equally accurate."""
+    th = np.asarray(thetas, np.float64)
+    lt = np.log(target)
+    logE = np.log(np.maximum(E, 1e-30))
+    label = np.full(E.shape[0], th[0])
+    for g in range(E.shape[0]):
+        above = np.nonzero(logE[g] > lt)[0]
+        if above.size == 0:
+            label[g] = th[-1]
+            continue
+        j = above[0]
+        if j == 0:
+            label[g] = th[0]
+            continue
+        e0, e1 = logE[g, j - 1], logE[g, j]
+        f = (lt - e0) / (e1 - e0) if e1 > e0 else 0.0
+        label[g] = th[j - 1] + f * (th[j] - th[j - 1])
+    return label.astype(np.float32)
+
+
+def _wmedian(x, w):
+    o = np.argsort(x)
+    cw = np.cumsum(w[o])
+    return float(x[o][np.searchsorted(cw, 0.5 * cw[-1])])
+
+
+def allocation_labels(E, C, sizes, thetas, target, fraction=0.9):
+    """Per-group angles that minimise total walk cost for a given error
+    budget: group g takes argmin_k C[g,k]/mean(C) + lam * log E[g,k] (a
+    Lagrangian relaxation; groups whose error grows slowly with the angle get
+    larger angles), lam bisected so that the particle-weighted geometric mean
+    of the groups' errors is fraction * target.  (The budget is the geometric
+    mean, not the median: a median budget is met by the easier half of the
+    groups alone, and its optimum leaves the other half arbitrarily wrong.)
+    Returns (labels, info); info compares the allocation's cost with the fixed
+    angle of equal median on the same groups: the bound a per-group angle
+    model can reach there."""
+    th = np.asarray(thetas, np.float64)
+    logE = np.log(np.maximum(E, 1e-30))
+    Cn = C / C.mean()
+    wts = sizes / sizes.sum()
+    goal = np.log(fraction * target)
+    rows = np.arange(E.shape[0])
+
+    def alloc(lam):
+        j = np.argmin(Cn + lam * logE, axis=1)
+        return j, float((wts * logE[rows, j]).sum())
+
+    lo, hi = 1e-4, 1e3
+    for _ in range(60):
+        mid = np.sqrt(lo * hi)
+        if alloc(mid)[1] > goal:
+            lo = mid
+        else:
+            hi = mid
+    j, _ = alloc(hi)
+    med = _wmedian(E[rows, j], sizes)
+    cost = float(C[rows, j].sum())
+    fixed_med = np.array([_wmedian(E[:, k], sizes) for k in range(len(th))])
+    fixed_cost = C.sum(axis=0)
+    # fixed angle cost at the allocation's median, log-log between grid angles
+    fc = None
+    o = np.argsort(fixed_med)
+    fm, fcs = fixed_med[o], fixed_cost[o]
+    for a in range(len(fm) - 1):
+        if fm[a] <= med <= fm[a + 1] and fm[a + 1] > fm[a]:
+            f = (np.log(med) - np.log(fm[a])) / (np.log(fm[a + 1]) - np.log(fm[a]))
+            fc = float(np.exp(np.log(fcs[a]) + f * (np.log(fcs[a + 1]) - np.log(fcs[a]))))
+    info = {"lambda": float(hi), "median": med, "p99": float(np.percentile(E[rows, j], 99)), "cost": cost,
+            "fixed_cost_at_equal_median": fc, "bound_gain": (fc / cost) if fc else None}
+    return th[j].astype(np.float32), info
+
+
+def training_set(pos, vel, eps, thetas=DEFAULT_GRID, target=5e-4, samples_per_group=8, max_groups=8192, seed=0,
+                 nleaf=16, ncrit=64, level_split=5, device=0, labels="crossing"):
+    """(features, label theta, error table) for a random subset of groups.
+    labels = "crossing": the angle at which the group's error reaches the
+    target; "allocation": the cost-optimal allocation (allocation_labels)."""
+    F, E, C, sizes = training_tables(pos, vel, eps, thetas, samples_per_group, max_groups, seed, nleaf, ncrit,
+                                     level_split, device)
+    if labels == "allocation":
+        y, _ = allocation_labels(E, C, sizes, thetas, target)
+    else:
+        y = crossing_labels(E, thetas, target)
+    return F, y, E
 
 
 def calibrate(pos, vel, w, eps, target, fraction=0.9, samples=2048, iters=10, nleaf=16, ncrit=64, level_split=5,

@@ -186,6 +186,10 @@ int bonsai_set_group_theta(bonsai_handle h, const float *theta, int ngroups);
 int bonsai_get_group_features(bonsai_handle h, float *out, int *ngroups);
 /* angles used by the last walk in mode 1 or 2, host float[ngroups] */
 int bonsai_get_group_theta(bonsai_handle h, float *out);
+/* per-group interaction counts of the last walk with per-group angles (theta
+ * mode 1 or 2): out[2g] = approximate (cell) and out[2g+1] = direct (particle)
+ * interactions of group g (the per-group form of computeForces.cu:568-609) */
+int bonsai_get_group_interactions(bonsai_handle h, unsigned *out);
 /* MLP on the GPU, host arrays: loss (mean of 0.5 (theta - y)^2 (1 + over [theta > y]))
  * and its gradient; Adam training for `epochs` full-batch steps (w in/out);
  * prediction of theta for S feature rows. */
