@@ -38,6 +38,8 @@ SIGNATURES = {
     "bonsai_set_particles_device": (I, [P, P, P, I]),
     "bonsai_get_particles": (I, [P, P, P, P]),
     "bonsai_get_particles_device": (I, [P, P, P, P]),
+    "bonsai_set_particles_async": (I, [P, P, P, I]),
+    "bonsai_get_particles_async": (I, [P, P, P, P]),
     "bonsai_build_tree": (I, [P, I]),
     "bonsai_compute_multipoles": (I, [P]),
     "bonsai_make_groups": (I, [P, I, I]),
@@ -51,6 +53,7 @@ SIGNATURES = {
     "bonsai_fp32_peak": (I, [I, P]),
     "bonsai_synchronize": (I, [P]),
     "bonsai_stream": (P, [P]),
+    "bonsai_copy_streams": (I, [P, P, P]),
     "bonsai_error_string": (ctypes.c_char_p, [I]),
     "bonsai_get_tree_info": (I, [P, P]),
     "bonsai_get_box": (I, [P, P]),

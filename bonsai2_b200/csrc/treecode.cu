@@ -101,6 +101,15 @@ struct Handle {
   float4 *jlo = nullptr, *cell_lo = nullptr;
   // ensemble layout (nsys > 1): system s owns particles [off[s], off[s+1]) of
   // the state; every stage works per system in the same launches
+  // asynchronous host copies: uploads on st_h2d into staging (in_pos,
+  // in_vel), consumed by the handle's stream; downloads of results from two
+  // staging slots on st_d2h.  Events order the three streams.
+  cudaStream_t st_h2d = nullptr, st_d2h = nullptr;
+  float4 *in_pos = nullptr, *in_vel = nullptr;
+  float4* out_buf[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};  // slot x (pos, vel, acc)
+  int out_slot = 0;
+  cudaEvent_t ev_in_copied = nullptr, ev_in_consumed = nullptr, ev_out_ready[2] = {nullptr, nullptr},
+              ev_out_done[2] = {nullptr, nullptr};
   int nsys = 1, nchunks = 0;
   int *sys_off = nullptr, *chunk_beg = nullptr, *root_beg = nullptr;
   int4* chunks = nullptr;
@@ -150,8 +159,17 @@ struct Handle {
     return 0;
   }
 
+  void release_staging() {
+    if (st_h2d) cudaStreamSynchronize(st_h2d);
+    if (st_d2h) cudaStreamSynchronize(st_d2h);
+    dfree(&in_pos); dfree(&in_vel);
+    for (int k = 0; k < 2; k++)
+      for (int a = 0; a < 3; a++) dfree(&out_buf[k][a]);
+  }
+
   void release_particles() {
     release_graphs();
+    release_staging();
     release_systems();
     release_lo();
     for (int p = 0; p < 2; p++) { dfree(&pos[p]); dfree(&vel[p]); dfree(&id[p]); }
@@ -176,6 +194,12 @@ struct Handle {
     dfree(&ph_table); dfree(&direct_part); dfree(&direct_out); dfree(&direct_sample);
     dfree(&mlp_w);
     if (mlp_wh) { cudaFree(mlp_wh); mlp_wh = nullptr; }
+    if (st_h2d) { cudaStreamDestroy(st_h2d); st_h2d = nullptr; }
+    if (st_d2h) { cudaStreamDestroy(st_d2h); st_d2h = nullptr; }
+    cudaEvent_t* evs[6] = {&ev_in_copied, &ev_in_consumed, &ev_out_ready[0], &ev_out_ready[1], &ev_out_done[0],
+                           &ev_out_done[1]};
+    for (cudaEvent_t* e : evs)
+      if (*e) { cudaEventDestroy(*e); *e = nullptr; }
     if (st) { cudaStreamDestroy(st); st = nullptr; }
   }
 
@@ -207,6 +231,13 @@ struct Handle {
     BONSAI_CUDA_TRY(cudaSetDevice(dev));
     BONSAI_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     BONSAI_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    BONSAI_CUDA_TRY(cudaStreamCreateWithFlags(&st_h2d, cudaStreamNonBlocking));
+    BONSAI_CUDA_TRY(cudaStreamCreateWithFlags(&st_d2h, cudaStreamNonBlocking));
+    {
+      cudaEvent_t* evs[6] = {&ev_in_copied, &ev_in_consumed, &ev_out_ready[0], &ev_out_ready[1], &ev_out_done[0],
+                             &ev_out_done[1]};
+      for (cudaEvent_t* e : evs) BONSAI_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    }
     box_blocks = nsm * 4;
     move_blocks = nsm * 4;
     BONSAI_CUDA_TRY(dalloc(&info, 1));
@@ -692,6 +723,61 @@ int bonsai_get_particles_device(bonsai_handle hh, float* pos4, float* vel4, floa
   return get_particles_impl(H(hh), pos4, vel4, acc4, cudaMemcpyDeviceToDevice);
 }
 
+int bonsai_set_particles_async(bonsai_handle hh, const float* pos4, const float* vel4, int n) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (!pos4 || !vel4 || n < 1) return BONSAI_ERR_ARG;
+  if (h->n == 0) return BONSAI_ERR_NOT_ALLOCATED;
+  if (n != h->n) return BONSAI_ERR_ARG;  // no reallocation on the asynchronous path
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  const size_t bytes = (size_t)n * sizeof(float4);
+  if (!h->in_pos) {
+    BONSAI_CUDA_TRY(dalloc(&h->in_pos, (size_t)n));
+    BONSAI_CUDA_TRY(dalloc(&h->in_vel, (size_t)n));
+  }
+  // upload once the previous upload has been consumed
+  BONSAI_CUDA_TRY(cudaStreamWaitEvent(h->st_h2d, h->ev_in_consumed, 0));
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(h->in_pos, pos4, bytes, cudaMemcpyHostToDevice, h->st_h2d));
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(h->in_vel, vel4, bytes, cudaMemcpyHostToDevice, h->st_h2d));
+  BONSAI_CUDA_TRY(cudaEventRecord(h->ev_in_copied, h->st_h2d));
+  // the handle's stream takes the particles over when they have landed
+  BONSAI_CUDA_TRY(cudaStreamWaitEvent(h->st, h->ev_in_copied, 0));
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(h->pos[h->par], h->in_pos, bytes, cudaMemcpyDeviceToDevice, h->st));
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(h->vel[h->par], h->in_vel, bytes, cudaMemcpyDeviceToDevice, h->st));
+  BONSAI_CUDA_TRY(cudaEventRecord(h->ev_in_consumed, h->st));
+  k_iota<<<h->nsm * 4, 256, 0, h->st>>>(h->id[h->par], n);
+  if (h->precision) BONSAI_CUDA_TRY(cudaMemsetAsync(h->plo[h->par], 0, bytes, h->st));
+  BONSAI_CUDA_TRY(cudaMemsetAsync(h->closing, 0, sizeof(int), h->st));
+  h->built = h->mp_done = h->grouped = h->forced = h->moved_after_forces = false;
+  return last_cuda();
+}
+
+int bonsai_get_particles_async(bonsai_handle hh, float* pos4, float* vel4, float* acc4) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (h->n == 0) return BONSAI_ERR_NOT_ALLOCATED;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  const int n = h->n;
+  const size_t bytes = (size_t)n * sizeof(float4);
+  const int slot = h->out_slot;
+  h->out_slot ^= 1;
+  const float4* src[3] = {h->pos[h->par], h->vel[h->par], h->acc};
+  float* dst[3] = {pos4, vel4, acc4};
+  // the slot is free once its previous download has finished
+  BONSAI_CUDA_TRY(cudaStreamWaitEvent(h->st, h->ev_out_done[slot], 0));
+  for (int a = 0; a < 3; a++) {
+    if (!dst[a]) continue;
+    if (!h->out_buf[slot][a]) BONSAI_CUDA_TRY(dalloc(&h->out_buf[slot][a], (size_t)n));
+    k_scatter_by_id<<<h->nsm * 8, 256, 0, h->st>>>(h->id[h->par], n, src[a], h->out_buf[slot][a]);
+  }
+  BONSAI_CUDA_TRY(cudaEventRecord(h->ev_out_ready[slot], h->st));
+  BONSAI_CUDA_TRY(cudaStreamWaitEvent(h->st_d2h, h->ev_out_ready[slot], 0));
+  for (int a = 0; a < 3; a++)
+    if (dst[a]) BONSAI_CUDA_TRY(cudaMemcpyAsync(dst[a], h->out_buf[slot][a], bytes, cudaMemcpyDeviceToHost, h->st_d2h));
+  BONSAI_CUDA_TRY(cudaEventRecord(h->ev_out_done[slot], h->st_d2h));
+  return last_cuda();
+}
+
 int bonsai_build_tree(bonsai_handle hh, int nleaf) {
   Handle* h = H(hh);
   if (!h) return BONSAI_ERR_HANDLE;
@@ -964,9 +1050,19 @@ int bonsai_synchronize(bonsai_handle hh) {
   Handle* h = H(hh);
   if (!h) return BONSAI_ERR_HANDLE;
   BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st_h2d));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st_d2h));
   const int c = last_cuda();
   if (c) return c;
   return h->read_status(true);
+}
+
+int bonsai_copy_streams(bonsai_handle hh, void** h2d, void** d2h) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (h2d) *h2d = (void*)h->st_h2d;
+  if (d2h) *d2h = (void*)h->st_d2h;
+  return 0;
 }
 
 void* bonsai_stream(bonsai_handle hh) {

@@ -87,6 +87,19 @@ int bonsai_set_particles_device(bonsai_handle h, const float *d_pos4, const floa
  * computeForces.cu:611-617); caller order; any pointer may be NULL. */
 int bonsai_get_particles(bonsai_handle h, float *pos4, float *vel4, float *acc4);
 int bonsai_get_particles_device(bonsai_handle h, float *d_pos4, float *d_vel4, float *d_acc4);
+/* Asynchronous forms (no counterpart in the reference, whose copies are
+ * synchronous): they return at once, so one step's uploads and downloads can
+ * overlap other steps' compute.  bonsai_set_particles_async uploads on a copy
+ * stream into device staging and the handle's stream takes the particles over
+ * when they have landed (n must equal the allocated n; the host arrays must
+ * stay unchanged until the next bonsai_synchronize).  bonsai_get_particles_async
+ * captures the current state on the handle's stream into one of two staging
+ * slots and downloads it on a second copy stream; the host arrays hold the
+ * result after bonsai_synchronize (at most two downloads in flight; a third
+ * waits for the first).  Pinned host memory (bonsai_host_alloc) is needed for
+ * real overlap. */
+int bonsai_set_particles_async(bonsai_handle h, const float *pos4, const float *vel4, int n);
+int bonsai_get_particles_async(bonsai_handle h, float *pos4, float *vel4, float *acc4);
 
 /* Treecode::buildTree(nLeaf) -- Treecode.h:216, buildTree.cu:845-1108 (box, tree, level order, leaves) */
 int bonsai_build_tree(bonsai_handle h, int nleaf);
@@ -125,8 +138,12 @@ int bonsai_graph_kernel_count(bonsai_handle h);
 int bonsai_get_stats(bonsai_handle h, unsigned long long *out4);
 /* measured FP32 FMA throughput of the device (TFLOP/s): the walk's roofline */
 int bonsai_fp32_peak(int device, double *tflops);
-/* Wait for the handle's stream; returns the sticky device status (and clears it). */
+/* Wait for the handle's stream and its copy streams; returns the sticky device
+ * status (and clears it). */
 int bonsai_synchronize(bonsai_handle h);
+/* the copy streams (cudaStream_t) of the asynchronous set / get, for callers
+ * that order their own work or events after them */
+int bonsai_copy_streams(bonsai_handle h, void **h2d, void **d2h);
 /* the handle's CUDA stream (cudaStream_t) */
 void *bonsai_stream(bonsai_handle h);
 const char *bonsai_error_string(int code);
