@@ -48,9 +48,10 @@ if ROOT not in sys.path:
 
 METRIC = "Mparticles/s per full step at N=2^24, median |δa|/|a|≤1e-3; learned-θ vs fixed-θ"
 UNIT = "Mparticles/s"
-# the walk's traffic per launch measured by ncu on this workload (see profiles/);
-# None until a capture exists
-WALK_DRAM_BYTES_PER_LAUNCH = None
+# the walk's DRAM traffic (read + write) per launch from one ncu capture of the
+# same workload at N = 2^22, theta 0.6 (profiles/walk_k_walk_plummer_4M.md);
+# scaled by the particle count for other N (the walk's misses grow with N)
+WALK_DRAM_BYTES_2P22 = 233.3e6 + 82.3e6
 
 
 def parse():
@@ -369,7 +370,10 @@ def run_ours(a):
             "config": {"workload": workload(a), "n_per_gpu": n, "parallelism": "replicas x%d" % d.world,
                        "l2": "no flush: particle state 1.3 GB > 126 MB L2", "graph": "captured CUDA graphs"},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": float(peak.value), "unit": "TFLOP/s",
-                         "frac": achieved / float(peak.value), "traffic": WALK_DRAM_BYTES_PER_LAUNCH,
+                         "frac": achieved / float(peak.value),
+                         "traffic": WALK_DRAM_BYTES_2P22 * n / 4194304 if abs(a.theta - 0.6) < 1e-6 else None,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of k_walk at N=2^22, "
+                                           "theta 0.6, scaled by N",
                          "kernel": "k_walk", "peak_source": "measured FP32 FMA probe (bonsai_fp32_peak)",
                          "flops_per_launch": flops},
             "cpu_baseline": cpu,
