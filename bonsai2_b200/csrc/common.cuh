@@ -45,13 +45,11 @@ struct TreeInfo {
   int level_end[kLevels];
 };
 
-// Per-cell FP64 record used by the bottom-up multipole pass.  The particle
-// bounding box is kept in double so that double-single positions keep exact
-// cell extents (float positions convert to it exactly).
+// Per-cell FP64 record used by the bottom-up multipole pass (the particle
+// bounding box is a separate array, float or double with the positions).
 struct MpRec {
   double m, cx, cy, cz;
   double ixx, iyy, izz, ixy, ixz, iyz;
-  double bmin[3], bmax[3];
 };
 
 struct Box {

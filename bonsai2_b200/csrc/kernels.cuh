@@ -42,12 +42,12 @@ void build_tree(const unsigned long long* sorted_keys, int n, int nleaf, int cel
                 int* mp_count, const int* sys_off, int nsys, int* root_beg, cudaStream_t s);
 
 // multipoles.cu
-__global__ void k_multipoles(const int* __restrict__ leaf_list, const TreeInfo* __restrict__ info,
-                             const uint4* __restrict__ cell_data, const int* __restrict__ cell_parent,
-                             const float4* __restrict__ jpos, float inv_theta, MpRec* __restrict__ rec,
-                             float4* __restrict__ cell_open, float4* __restrict__ cell_q0,
-                             float4* __restrict__ cell_q1, float2* __restrict__ cell_ls, int* __restrict__ mp_count,
-                             int cell_cap, const float4* __restrict__ jlo, float4* __restrict__ cell_lo);
+// box: 6 floats per cell (float positions) or 6 doubles (jlo != nullptr:
+// double-single positions)
+void launch_multipoles(const int* leaf_list, const TreeInfo* info, const uint4* cell_data, const int* cell_parent,
+                       const float4* jpos, float inv_theta, MpRec* rec, void* box, float4* cell_open,
+                       float4* cell_q0, float4* cell_q1, float2* cell_ls, int* mp_count, int cell_cap,
+                       const float4* jlo, float4* cell_lo, int nblocks, cudaStream_t s);
 __global__ void k_multipoles_ref_layout(const TreeInfo* __restrict__ info, const float4* __restrict__ cell_open,
                                         const MpRec* __restrict__ rec, float4* __restrict__ size,
                                         float4* __restrict__ mono, float4* __restrict__ quad0,

@@ -16,42 +16,53 @@
 // (l/theta_g + s)^2.  Stored for the walk (mass-weighted, pre-scaled so the
 // force kernel needs fewer operations):  cell_q0 = (M, 3Ixx, 3Iyy, 3Izz),
 // cell_q1 = (3Ixy, 3Ixz, 3Iyz, 1.5 tr I), with I = M Q.
-// Double-single positions (jlo != nullptr): particles enter the FP64 sums as
-// hi + lo, and the COM is stored as hi (cell_open) plus lo (cell_lo).
+// The FP64 record (MpRec) holds M, COM and the moments; the particle bounding
+// box is a separate array, float for float positions and double (DS) for
+// double-single positions, where particles enter the FP64 sums as hi + lo,
+// extents are exact, and the COM is stored as hi (cell_open) plus lo (cell_lo).
 #include "common.cuh"
 #include "kernels.cuh"
 
 namespace bonsai {
 
-__device__ __forceinline__ void store_cell(int c, const MpRec& r, float inv_theta, MpRec* __restrict__ rec,
-                                           float4* __restrict__ cell_open, float4* __restrict__ cell_q0,
-                                           float4* __restrict__ cell_q1, float2* __restrict__ cell_ls,
-                                           float4* __restrict__ cell_lo) {
+template <bool DS>
+struct BoxOf {
+  typedef float T;
+};
+template <>
+struct BoxOf<true> {
+  typedef double T;
+};
+
+template <bool DS>
+__device__ __forceinline__ void store_cell(int c, const MpRec& r, const typename BoxOf<DS>::T* bmin,
+                                           const typename BoxOf<DS>::T* bmax, float inv_theta, MpRec* __restrict__ rec,
+                                           typename BoxOf<DS>::T* __restrict__ box, float4* __restrict__ cell_open,
+                                           float4* __restrict__ cell_q0, float4* __restrict__ cell_q1,
+                                           float2* __restrict__ cell_ls, float4* __restrict__ cell_lo) {
   rec[c] = r;
+  for (int k = 0; k < 3; k++) { box[6 * (size_t)c + k] = bmin[k]; box[6 * (size_t)c + 3 + k] = bmax[k]; }
   const float cx = (float)r.cx, cy = (float)r.cy, cz = (float)r.cz;
-  if (cell_lo)
-    cell_lo[c] = make_float4((float)(r.cx - (double)cx), (float)(r.cy - (double)cy), (float)(r.cz - (double)cz), 0.f);
   float s, l;
-  if (cell_lo) {
-    // double-single: extents and centre offsets from the exact box and COM
-    double v[3], hm = 0.0, d2 = 0.0;
+  if (DS) {
+    cell_lo[c] = make_float4((float)(r.cx - (double)cx), (float)(r.cy - (double)cy), (float)(r.cz - (double)cz), 0.f);
+    // extents and centre offsets from the exact box and COM
+    double hm = 0.0, d2 = 0.0;
     const double com[3] = {r.cx, r.cy, r.cz};
     for (int k = 0; k < 3; k++) {
-      v[k] = 0.5 * (r.bmax[k] + r.bmin[k]) - com[k];
-      hm = fmax(hm, 0.5 * (r.bmax[k] - r.bmin[k]));
-      d2 += v[k] * v[k];
+      const double v = 0.5 * ((double)bmax[k] + (double)bmin[k]) - com[k];
+      hm = fmax(hm, 0.5 * ((double)bmax[k] - (double)bmin[k]));
+      d2 += v * v;
     }
     s = (float)sqrt(d2);
     l = fmaxf((float)(2.0 * hm), 1.0e-6f);
   } else {
-    const float b0[3] = {(float)r.bmin[0], (float)r.bmin[1], (float)r.bmin[2]};
-    const float b1[3] = {(float)r.bmax[0], (float)r.bmax[1], (float)r.bmax[2]};
-    const float vx = __fmul_rn(__fadd_rn(b1[0], b0[0]), 0.5f);
-    const float vy = __fmul_rn(__fadd_rn(b1[1], b0[1]), 0.5f);
-    const float vz = __fmul_rn(__fadd_rn(b1[2], b0[2]), 0.5f);
-    const float hx = __fmul_rn(__fsub_rn(b1[0], b0[0]), 0.5f);
-    const float hy = __fmul_rn(__fsub_rn(b1[1], b0[1]), 0.5f);
-    const float hz = __fmul_rn(__fsub_rn(b1[2], b0[2]), 0.5f);
+    const float vx = __fmul_rn(__fadd_rn((float)bmax[0], (float)bmin[0]), 0.5f);
+    const float vy = __fmul_rn(__fadd_rn((float)bmax[1], (float)bmin[1]), 0.5f);
+    const float vz = __fmul_rn(__fadd_rn((float)bmax[2], (float)bmin[2]), 0.5f);
+    const float hx = __fmul_rn(__fsub_rn((float)bmax[0], (float)bmin[0]), 0.5f);
+    const float hy = __fmul_rn(__fsub_rn((float)bmax[1], (float)bmin[1]), 0.5f);
+    const float hz = __fmul_rn(__fsub_rn((float)bmax[2], (float)bmin[2]), 0.5f);
     const float dx = __fsub_rn(vx, cx), dy = __fsub_rn(vy, cy), dz = __fsub_rn(vz, cz);
     s = __fsqrt_rn(__fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx))));
     l = fmaxf(__fmul_rn(2.0f, fmaxf(hx, fmaxf(hy, hz))), 1.0e-6f);
@@ -66,9 +77,7 @@ __device__ __forceinline__ void store_cell(int c, const MpRec& r, float inv_thet
 
 // Arrival on a parent's counter: a fence publishes this child's record, a
 // relaxed atomic counts it, and only the last arriver fences again before it
-// reads its siblings' records (through L2).  (An acquire-release atomic per
-// arrival was measured 16x slower here: a GPU-scope acquire invalidates the
-// SM's L1, which the leaf loads of every other warp depend on.)
+// reads its siblings' records (through L2).
 __device__ __forceinline__ bool arrive_last(int* p, int nch) {
   __threadfence();
   if (atomicAdd(p, 1) != nch - 1) return false;
@@ -76,21 +85,13 @@ __device__ __forceinline__ bool arrive_last(int* p, int nch) {
   return true;
 }
 
-__device__ __forceinline__ void particle_ds(const float4* __restrict__ jpos, const float4* __restrict__ jlo, int i,
-                                            double& x, double& y, double& z, double& w) {
-  const float4 p = __ldg(jpos + i);
-  x = p.x; y = p.y; z = p.z; w = p.w;
-  if (jlo) {
-    const float4 l = __ldg(jlo + i);
-    x += l.x; y += l.y; z += l.z;
-  }
-}
-
 // Combines parents bottom-up while this thread is the last child to arrive.
+template <bool DS>
 __device__ void climb(int c, const uint4* __restrict__ cell_data, const int* __restrict__ cell_parent,
-                      float inv_theta, MpRec* __restrict__ rec, float4* __restrict__ cell_open,
-                      float4* __restrict__ cell_q0, float4* __restrict__ cell_q1, float2* __restrict__ cell_ls,
-                      int* __restrict__ mp_count, float4* __restrict__ cell_lo) {
+                      float inv_theta, MpRec* __restrict__ rec, typename BoxOf<DS>::T* __restrict__ box,
+                      float4* __restrict__ cell_open, float4* __restrict__ cell_q0, float4* __restrict__ cell_q1,
+                      float2* __restrict__ cell_ls, int* __restrict__ mp_count, float4* __restrict__ cell_lo) {
+  typedef typename BoxOf<DS>::T B;
   while (true) {
     const int p = cell_parent[c];
     if (p < 0) break;
@@ -98,20 +99,25 @@ __device__ void climb(int c, const uint4* __restrict__ cell_data, const int* __r
     const int first = (int)(y & 0x1FFFFFFFu), nch = (int)(y >> 29) + 1;
     if (!arrive_last(mp_count + p, nch)) break;
     double M = 0, X = 0, Y = 0, Z = 0;
-    double bmn[3] = {3.0e38, 3.0e38, 3.0e38}, bmx[3] = {-3.0e38, -3.0e38, -3.0e38};
+    B bmn[3] = {(B)3.0e38, (B)3.0e38, (B)3.0e38}, bmx[3] = {(B)-3.0e38, (B)-3.0e38, (B)-3.0e38};
     for (int k = 0; k < nch; k++) {
       const MpRec* ck = rec + first + k;
       const double mk = __ldcg(&ck->m);
       M += mk;
       X += mk * __ldcg(&ck->cx); Y += mk * __ldcg(&ck->cy); Z += mk * __ldcg(&ck->cz);
+      const B* bk = box + 6 * (size_t)(first + k);
       for (int a = 0; a < 3; a++) {
-        bmn[a] = fmin(bmn[a], __ldcg(&ck->bmin[a]));
-        bmx[a] = fmax(bmx[a], __ldcg(&ck->bmax[a]));
+        bmn[a] = DS ? (B)fmin((double)bmn[a], (double)__ldcg(bk + a)) : (B)fminf((float)bmn[a], (float)__ldcg(bk + a));
+        bmx[a] = DS ? (B)fmax((double)bmx[a], (double)__ldcg(bk + 3 + a))
+                    : (B)fmaxf((float)bmx[a], (float)__ldcg(bk + 3 + a));
       }
     }
     MpRec P;
     if (M > 0.0) { P.cx = X / M; P.cy = Y / M; P.cz = Z / M; }
-    else { P.cx = 0.5 * (bmn[0] + bmx[0]); P.cy = 0.5 * (bmn[1] + bmx[1]); P.cz = 0.5 * (bmn[2] + bmx[2]); }
+    else {
+      P.cx = 0.5 * ((double)bmn[0] + bmx[0]); P.cy = 0.5 * ((double)bmn[1] + bmx[1]);
+      P.cz = 0.5 * ((double)bmn[2] + bmx[2]);
+    }
     double I[6] = {0, 0, 0, 0, 0, 0};
     for (int k = 0; k < nch; k++) {
       const MpRec* ck = rec + first + k;
@@ -126,24 +132,25 @@ __device__ void climb(int c, const uint4* __restrict__ cell_data, const int* __r
     }
     P.m = M;
     P.ixx = I[0]; P.iyy = I[1]; P.izz = I[2]; P.ixy = I[3]; P.ixz = I[4]; P.iyz = I[5];
-    for (int a = 0; a < 3; a++) { P.bmin[a] = bmn[a]; P.bmax[a] = bmx[a]; }
-    store_cell(p, P, inv_theta, rec, cell_open, cell_q0, cell_q1, cell_ls, cell_lo);
+    store_cell<DS>(p, P, bmn, bmx, inv_theta, rec, box, cell_open, cell_q0, cell_q1, cell_ls, cell_lo);
     c = p;
   }
 }
 
 // One thread per leaf: two passes over the leaf's particles (COM, then
 // central moments), then the bottom-up climb.  (Half-warp-cooperative leaves
-// with shuffle reductions were measured 16x slower on the B200.)
+// with shuffle reductions were measured 13x slower on the B200.)
+template <bool DS>
 __global__ void __launch_bounds__(256) k_multipoles(const int* __restrict__ leaf_list, const TreeInfo* __restrict__ info,
                                                     const uint4* __restrict__ cell_data,
                                                     const int* __restrict__ cell_parent,
                                                     const float4* __restrict__ jpos, float inv_theta,
-                                                    MpRec* __restrict__ rec, float4* __restrict__ cell_open,
-                                                    float4* __restrict__ cell_q0, float4* __restrict__ cell_q1,
-                                                    float2* __restrict__ cell_ls, int* __restrict__ mp_count,
-                                                    int cell_cap, const float4* __restrict__ jlo,
-                                                    float4* __restrict__ cell_lo) {
+                                                    MpRec* __restrict__ rec, typename BoxOf<DS>::T* __restrict__ box,
+                                                    float4* __restrict__ cell_open, float4* __restrict__ cell_q0,
+                                                    float4* __restrict__ cell_q1, float2* __restrict__ cell_ls,
+                                                    int* __restrict__ mp_count, int cell_cap,
+                                                    const float4* __restrict__ jlo, float4* __restrict__ cell_lo) {
+  typedef typename BoxOf<DS>::T B;
   const int nleaves = info->nleaves;
   if (info->ncells > cell_cap) return;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nleaves; t += gridDim.x * blockDim.x) {
@@ -152,31 +159,57 @@ __global__ void __launch_bounds__(256) k_multipoles(const int* __restrict__ leaf
     const int b = (int)cd.z, e = (int)cd.w;
     MpRec r;
     double m = 0, sx = 0, sy = 0, sz = 0;
-    double mn[3] = {3.0e38, 3.0e38, 3.0e38}, mx[3] = {-3.0e38, -3.0e38, -3.0e38};
+    B mn[3] = {(B)3.0e38, (B)3.0e38, (B)3.0e38}, mx[3] = {(B)-3.0e38, (B)-3.0e38, (B)-3.0e38};
     for (int i = b; i < e; i++) {
-      double px, py, pz, w;
-      particle_ds(jpos, jlo, i, px, py, pz, w);
-      m += w;
-      sx += w * px; sy += w * py; sz += w * pz;
-      mn[0] = fmin(mn[0], px); mn[1] = fmin(mn[1], py); mn[2] = fmin(mn[2], pz);
-      mx[0] = fmax(mx[0], px); mx[1] = fmax(mx[1], py); mx[2] = fmax(mx[2], pz);
+      const float4 p = __ldg(jpos + i);
+      double px = p.x, py = p.y, pz = p.z;
+      if (DS) {
+        const float4 l = __ldg(jlo + i);
+        px += l.x; py += l.y; pz += l.z;
+        mn[0] = (B)fmin((double)mn[0], px); mn[1] = (B)fmin((double)mn[1], py); mn[2] = (B)fmin((double)mn[2], pz);
+        mx[0] = (B)fmax((double)mx[0], px); mx[1] = (B)fmax((double)mx[1], py); mx[2] = (B)fmax((double)mx[2], pz);
+      } else {
+        mn[0] = (B)fminf((float)mn[0], p.x); mn[1] = (B)fminf((float)mn[1], p.y); mn[2] = (B)fminf((float)mn[2], p.z);
+        mx[0] = (B)fmaxf((float)mx[0], p.x); mx[1] = (B)fmaxf((float)mx[1], p.y); mx[2] = (B)fmaxf((float)mx[2], p.z);
+      }
+      m += p.w;
+      sx += (double)p.w * px; sy += (double)p.w * py; sz += (double)p.w * pz;
     }
     if (m > 0.0) { r.cx = sx / m; r.cy = sy / m; r.cz = sz / m; }
-    else { r.cx = 0.5 * (mn[0] + mx[0]); r.cy = 0.5 * (mn[1] + mx[1]); r.cz = 0.5 * (mn[2] + mx[2]); }
+    else {
+      r.cx = 0.5 * ((double)mn[0] + mx[0]); r.cy = 0.5 * ((double)mn[1] + mx[1]); r.cz = 0.5 * ((double)mn[2] + mx[2]);
+    }
     double q[6] = {0, 0, 0, 0, 0, 0};
     for (int i = b; i < e; i++) {
-      double px, py, pz, w;
-      particle_ds(jpos, jlo, i, px, py, pz, w);
-      const double dx = px - r.cx, dy = py - r.cy, dz = pz - r.cz;
+      const float4 p = __ldg(jpos + i);
+      double px = p.x, py = p.y, pz = p.z;
+      if (DS) {
+        const float4 l = __ldg(jlo + i);
+        px += l.x; py += l.y; pz += l.z;
+      }
+      const double dx = px - r.cx, dy = py - r.cy, dz = pz - r.cz, w = p.w;
       q[0] += w * dx * dx; q[1] += w * dy * dy; q[2] += w * dz * dz;
       q[3] += w * dx * dy; q[4] += w * dx * dz; q[5] += w * dy * dz;
     }
     r.m = m;
     r.ixx = q[0]; r.iyy = q[1]; r.izz = q[2]; r.ixy = q[3]; r.ixz = q[4]; r.iyz = q[5];
-    for (int k = 0; k < 3; k++) { r.bmin[k] = mn[k]; r.bmax[k] = mx[k]; }
-    store_cell(c, r, inv_theta, rec, cell_open, cell_q0, cell_q1, cell_ls, cell_lo);
-    climb(c, cell_data, cell_parent, inv_theta, rec, cell_open, cell_q0, cell_q1, cell_ls, mp_count, cell_lo);
+    store_cell<DS>(c, r, mn, mx, inv_theta, rec, box, cell_open, cell_q0, cell_q1, cell_ls, cell_lo);
+    climb<DS>(c, cell_data, cell_parent, inv_theta, rec, box, cell_open, cell_q0, cell_q1, cell_ls, mp_count, cell_lo);
   }
+}
+
+void launch_multipoles(const int* leaf_list, const TreeInfo* info, const uint4* cell_data, const int* cell_parent,
+                       const float4* jpos, float inv_theta, MpRec* rec, void* box, float4* cell_open,
+                       float4* cell_q0, float4* cell_q1, float2* cell_ls, int* mp_count, int cell_cap,
+                       const float4* jlo, float4* cell_lo, int nblocks, cudaStream_t s) {
+  if (jlo)
+    k_multipoles<true><<<nblocks, 256, 0, s>>>(leaf_list, info, cell_data, cell_parent, jpos, inv_theta, rec,
+                                               static_cast<double*>(box), cell_open, cell_q0, cell_q1, cell_ls,
+                                               mp_count, cell_cap, jlo, cell_lo);
+  else
+    k_multipoles<false><<<nblocks, 256, 0, s>>>(leaf_list, info, cell_data, cell_parent, jpos, inv_theta, rec,
+                                                static_cast<float*>(box), cell_open, cell_q0, cell_q1, cell_ls,
+                                                mp_count, cell_cap, nullptr, nullptr);
 }
 
 // Reference-layout view of the multipoles (debug/parity getter):

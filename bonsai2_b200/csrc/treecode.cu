@@ -64,6 +64,7 @@ struct Handle {
   float4 *cell_open = nullptr, *cell_q0 = nullptr, *cell_q1 = nullptr;
   int *cell_parent = nullptr, *leaf_list = nullptr, *mp_count = nullptr;
   MpRec* rec = nullptr;
+  double* cell_box = nullptr;  // 6 per cell: floats (float positions) or doubles (double-single)
   float2* cell_ls = nullptr;
   // per-group opening angles (theta mode 1: MLP, 2: caller's array)
   int theta_mode = 0;
@@ -183,6 +184,7 @@ struct Handle {
   void release_cells() {
     dfree(&cell_data); dfree(&cell_open); dfree(&cell_q0); dfree(&cell_q1);
     dfree(&cell_parent); dfree(&leaf_list); dfree(&mp_count); dfree(&rec); dfree(&cell_ls);
+    dfree(&cell_box);
     cap_cells = 0;
   }
   void release() {
@@ -216,6 +218,7 @@ struct Handle {
     BONSAI_CUDA_TRY(dalloc(&leaf_list, C));
     BONSAI_CUDA_TRY(dalloc(&mp_count, C));
     BONSAI_CUDA_TRY(dalloc(&rec, C));
+    BONSAI_CUDA_TRY(dalloc(&cell_box, 6 * C));
     BONSAI_CUDA_TRY(dalloc(&cell_ls, C));
     dfree(&cell_lo);
     if (precision) BONSAI_CUDA_TRY(dalloc(&cell_lo, C));
@@ -391,9 +394,9 @@ struct Handle {
                mp_count, so(), nsys, root_beg, st);
   }
   void enq_multipoles() {
-    k_multipoles<<<nsm * 8, 256, 0, st>>>(leaf_list, info, cell_data, cell_parent, jpos, 1.0f / prm.theta, rec,
-                                          cell_open, cell_q0, cell_q1, cell_ls, mp_count, cap_cells,
-                                          precision ? jlo : nullptr, precision ? cell_lo : nullptr);
+    launch_multipoles(leaf_list, info, cell_data, cell_parent, jpos, 1.0f / prm.theta, rec, cell_box, cell_open,
+                      cell_q0, cell_q1, cell_ls, mp_count, cap_cells, precision ? jlo : nullptr,
+                      precision ? cell_lo : nullptr, nsm * 8, st);
   }
   void enq_groups(int ls, int ncrit) {
     radix_sort_pairs(pkey, kalt, pperm, valt, nullptr, n, sort_counts, &info->status, 8, so(), nsys, st);
