@@ -81,6 +81,9 @@ SIGNATURES = {
     "bonsai_autotune": (I, [P, P, I, P, I, I, P, P]),
     "bonsai_plummer": (I, [ctypes.c_long, ctypes.c_uint, P, P]),
     "bonsai_galaxy": (I, [ctypes.c_long, ctypes.c_ulonglong, P, P]),
+    "bonsai_read_tipsy": (I, [ctypes.c_char_p, P, P, P, P, P]),
+    "bonsai_write_tipsy": (I, [ctypes.c_char_p, ctypes.c_double, I, I, P, P, P]),
+    "bonsai_sync_velocities": (I, [P]),
     "bonsai_clustered_field": (I, [ctypes.c_long, ctypes.c_ulonglong, I, P, P]),
     "bonsai_host_alloc": (P, [ctypes.c_size_t]),
     "bonsai_host_free": (None, [P]),

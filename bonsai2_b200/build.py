@@ -26,7 +26,7 @@ EXTRA = os.environ.get("BONSAI_NVCC_DEFINES", "").split()
 PER_FILE = {"walk.cu": ["-ftz=true"]}
 SOURCES = ["keys.cu", "sort.cu", "tree.cu", "multipoles.cu", "groups.cu", "walk.cu", "move.cu", "treecode.cu",
            "noalloc.cu", "learned.cu"]
-HOST_SOURCES = ["plummer.cpp", "ics.cpp"]
+HOST_SOURCES = ["plummer.cpp", "ics.cpp", "tipsy.cpp"]
 
 
 def _deps():

@@ -87,6 +87,8 @@ void launch_move(float4* pos, float4* vel, const float4* acc, int n, float dt, i
 void launch_move_sys(float4* pos, float4* vel, const float4* acc, const int4* chunks, int nchunks,
                      const int* chunk_beg, int nsys, float dt, int* closing, float eps, int write, double* chunk_part,
                      int nblocks, unsigned* ticket, double* energies, double* sys_energies, cudaStream_t s);
+// pending closing kick applied in place, then the closing flag cleared
+void launch_closing_kick(float4* vel, const float4* acc, int n, float dt, int* closing, int nblocks, cudaStream_t s);
 // FP64 direct sum inside each sample's own system (one block per sample)
 void launch_direct_fp64_sys(const float4* pos, const int* sys_off, int nsys, const int* sample, int ns, double eps2,
                             int include_self, double* out, cudaStream_t s);

@@ -243,6 +243,26 @@ void launch_direct_fp64(const float4* pos, int n, const int* sample, int ns, dou
   k_direct_fold<<<(4 * ns + 255) / 256, 256, 0, s>>>(part, ns, nsplit, out);
 }
 
+// The pending closing kick v += a dt/2 (the same operation the move applies
+// when the closing flag is set), for checkpoints with synchronised
+// velocities; the caller clears the flag afterwards.
+__global__ void __launch_bounds__(256) k_closing_kick(float4* __restrict__ vel, const float4* __restrict__ acc, int n,
+                                                      float dt, const int* __restrict__ closing) {
+  if (!*closing) return;
+  const float h = 0.5f * dt;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float4 v = vel[i];
+    const float4 a = acc[i];
+    v.x = fmaf(a.x, h, v.x); v.y = fmaf(a.y, h, v.y); v.z = fmaf(a.z, h, v.z);
+    vel[i] = v;
+  }
+}
+
+void launch_closing_kick(float4* vel, const float4* acc, int n, float dt, int* closing, int nblocks, cudaStream_t s) {
+  k_closing_kick<<<nblocks, 256, 0, s>>>(vel, acc, n, dt, closing);
+  cudaMemsetAsync(closing, 0, sizeof(int), s);
+}
+
 // Ensemble checker: each sample's force from the particles of its own system
 // only (positions in the caller's order, systems contiguous); one block per
 // sample, fixed-order block reduction.

@@ -335,9 +335,24 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_cells(
         int lc1 = 0;
         for (int q = 0; q < k; q++) lc1 += (ca[q] && ca[q] <= L + 1 && L + 1 <= cb[q]);
         const int first = (int)(boff[0][L + 1] + cpre[L + 1][threadIdx.x]) + lc1;
+        // the 7 inner octant boundaries are independent lower bounds over
+        // [i, pend): searched in lock-step, 7 loads in flight per step
+        int bl[8], bh[8];
+#pragma unroll
+        for (int o = 1; o < 8; o++) { bl[o] = i; bh[o] = pend; }
+        for (int span = pend - i; span > 0; span >>= 1) {
+#pragma unroll
+          for (int o = 1; o < 8; o++) {
+            if (bl[o] < bh[o]) {
+              const int mid = (bl[o] + bh[o]) >> 1;
+              if (__ldg(keys + mid) < (((pre << 3) | (unsigned long long)o) << (sh - 3))) bl[o] = mid + 1;
+              else bh[o] = mid;
+            }
+          }
+        }
         int nch = 0, lo = i;
         for (int o = 1; o <= 8; o++) {
-          const int bnd = (o == 8) ? pend : lower_bound_u64(keys, lo, pend, ((pre << 3) | (unsigned long long)o) << (sh - 3));
+          const int bnd = (o == 8) ? pend : bl[o];
           if (bnd > lo) {
             cell_data[first + nch].x = (unsigned)cidx | ((unsigned)(L + 1) << 27);
             cell_parent[first + nch] = cidx;

@@ -617,6 +617,10 @@ int last_cuda(void) {
 
 // Plummer initial conditions (host): plummer.cpp
 extern "C" int bonsai_plummer_impl(long n, unsigned int seed, float* pos4, float* vel4);
+// Tipsy snapshots (host): tipsy.cpp
+extern "C" int bonsai_read_tipsy_impl(const char* path, double* time, int* n, float* pos4, float* vel4, int* ids);
+extern "C" int bonsai_write_tipsy_impl(const char* path, double time, int n, int ndark, const float* pos4,
+                                       const float* vel4, const int* ids);
 // composite galaxy and clustered field (host): ics.cpp
 extern "C" int bonsai_galaxy_impl(long n, unsigned long long seed, double* pos4, float* vel4);
 extern "C" int bonsai_clustered_field_impl(long n, unsigned long long seed, int nclusters, float* pos4, float* vel4);
@@ -1008,6 +1012,23 @@ int bonsai_get_particles_f64(bonsai_handle hh, double* pos4, float* vel4, float*
   return last_cuda();
 }
 
+int bonsai_sync_velocities(bonsai_handle hh) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (h->n == 0) return BONSAI_ERR_NOT_ALLOCATED;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  int rc = h->build_checked(h->cur_nleaf);
+  if (rc) return rc;
+  h->enq_multipoles();
+  h->enq_groups(h->cur_ls, h->cur_ncrit);
+  h->enq_forces(h->cur_ncrit);
+  launch_closing_kick(h->vel[h->par], h->acc, h->n, h->prm.dt, h->closing, h->nsm * 4, h->st);
+  h->built = h->mp_done = h->grouped = h->forced = true;
+  h->ever_built = h->ever_mp = true;
+  h->moved_after_forces = false;
+  return last_cuda();
+}
+
 int bonsai_set_walk_layout(bonsai_handle hh, int layout) {
   Handle* h = H(hh);
   if (!h) return BONSAI_ERR_HANDLE;
@@ -1082,6 +1103,7 @@ const char* bonsai_error_string(int code) {
     case BONSAI_ERR_ORDER: return "stage called before the stage it depends on";
     case BONSAI_ERR_ARG: return "invalid argument";
     case BONSAI_ERR_NO_DEVICE: return "no CUDA device";
+    case BONSAI_ERR_IO: return "file could not be opened, read or written (or is not a Tipsy snapshot)";
     case BONSAI_ERR_TOO_LARGE: return "request exceeds the fixed scratch capacity (bonsai_direct_fp64_noalloc: ns <= 65536)";
     default: break;
   }
@@ -1413,6 +1435,15 @@ int bonsai_mlp_predict(int device, const float* X, int S, const float* w, float 
 int bonsai_plummer(long n, unsigned int seed, float* pos4, float* vel4) {
   if (n < 1 || !pos4 || !vel4) return BONSAI_ERR_ARG;
   return bonsai_plummer_impl(n, seed, pos4, vel4);
+}
+
+int bonsai_read_tipsy(const char* path, double* time, int* n, float* pos4, float* vel4, int* ids) {
+  return bonsai_read_tipsy_impl(path, time, n, pos4, vel4, ids);
+}
+
+int bonsai_write_tipsy(const char* path, double time, int n, int ndark, const float* pos4, const float* vel4,
+                       const int* ids) {
+  return bonsai_write_tipsy_impl(path, time, n, ndark, pos4, vel4, ids);
 }
 
 int bonsai_galaxy(long n, unsigned long long seed, double* pos4, float* vel4) {

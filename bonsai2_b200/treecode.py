@@ -75,6 +75,32 @@ def clustered_field(n: int, seed: int = 1, nclusters: int = 64):
     return pos, vel
 
 
+def read_tipsy(path: str):
+    """(time, pos4 (n,4) float32 = x,y,z,mass, vel4 (n,4) float32 = vx,vy,vz,eps,
+    ids (n,) int32) from a Tipsy snapshot (bonsai_read_tipsy)."""
+    L = load()
+    t = ctypes.c_double(0.0)
+    n = ctypes.c_int(0)
+    _check(L.bonsai_read_tipsy(path.encode(), ctypes.byref(t), ctypes.byref(n), None, None, None), "read_tipsy")
+    pos = np.empty((n.value, 4), np.float32)
+    vel = np.empty((n.value, 4), np.float32)
+    ids = np.empty(n.value, np.int32)
+    _check(L.bonsai_read_tipsy(path.encode(), ctypes.byref(t), ctypes.byref(n), _p(pos), _p(vel), _p(ids)),
+           "read_tipsy")
+    return t.value, pos, vel, ids
+
+
+def write_tipsy(path: str, pos4, vel4, ids=None, time: float = 0.0, ndark: int = None):
+    """Writes a Tipsy snapshot: the first ndark particles (default all) as dark
+    records, the rest as star records (bonsai_write_tipsy)."""
+    p = np.ascontiguousarray(pos4, np.float32)
+    v = np.ascontiguousarray(vel4, np.float32)
+    i = None if ids is None else np.ascontiguousarray(ids, np.int32)
+    n = p.shape[0]
+    _check(load().bonsai_write_tipsy(path.encode(), float(time), n, n if ndark is None else ndark, _p(p), _p(v),
+                                     _p(i)), "write_tipsy")
+
+
 class Treecode:
     def __init__(self, eps: float = 0.01, theta: float = 0.75, ncrit: int = 64, nleaf: int = 16,
                  level_split: int = 5, dt: float = 1.0 / 64, device: int = 0):
@@ -196,6 +222,11 @@ class Treecode:
         a = np.empty((n, 4), np.float32)
         _check(self._L.bonsai_get_particles_f64(self._h, _p(p), _p(v), _p(a)), "bonsai_get_particles_f64")
         return p, v, a
+
+    def sync_velocities(self):
+        """Forces at the current positions and the pending half kick applied,
+        so that ptcl_d2h returns synchronised (x, v) for a checkpoint."""
+        _check(self._L.bonsai_sync_velocities(self._h), "bonsai_sync_velocities")
 
     def set_walk_layout(self, layout: int):
         """0: two half-warps per group (nCrit <= 64), 1: one warp per group."""

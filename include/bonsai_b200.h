@@ -44,6 +44,7 @@ extern "C" {
 #define BONSAI_ERR_ARG (-4)
 #define BONSAI_ERR_NO_DEVICE (-5)
 #define BONSAI_ERR_TOO_LARGE (-6) /* request beyond a fixed capacity (bonsai_direct_fp64_noalloc) */
+#define BONSAI_ERR_IO (-7)        /* snapshot file could not be opened, read or written */
 
 typedef struct bonsai_handle_s *bonsai_handle;
 
@@ -275,6 +276,27 @@ int bonsai_autotune(bonsai_handle h, const int *nleaf, int n_nleaf, const int *n
  * code/plummer.h:9-138 (glibc rand(), same stream), converted to float4 like
  * treecode.cu:65-87: pos4 = (x,y,z,m), vel4 = (vx,vy,vz,m).  n >= 1. */
 int bonsai_plummer(long n, unsigned int seed, float *pos4, float *vel4);
+
+/* Tipsy snapshots (host; ReadTipsy, read_tipsy.h:108-160, records of
+ * tipsydefs.h): native-order header {double time; int nbodies, ndim, nsph,
+ * ndark, nstar} (32 bytes), ndark dark records {mass, pos[3], vel[3], eps,
+ * int phi}, then nbodies - ndark star records {mass, pos[3], vel[3], metals,
+ * tform, eps, int phi}, as the reference reads them (nsph ignored).  pos4 =
+ * (x, y, z, mass), vel4 = (vx, vy, vz, eps), ids = phi.
+ * bonsai_read_tipsy with pos4, vel4 and ids all NULL returns the particle count
+ * in *n (and the time); otherwise *n is the capacity of the arrays on entry and
+ * the count on return.  bonsai_write_tipsy writes the same layout (ids NULL:
+ * 0..n-1; nsph 0, nstar = n - ndark), which the reference's reader reads back. */
+int bonsai_read_tipsy(const char *path, double *time, int *n, float *pos4, float *vel4, int *ids);
+int bonsai_write_tipsy(const char *path, double time, int n, int ndark, const float *pos4, const float *vel4,
+                       const int *ids);
+/* Checkpoints: after a step the velocities are half a step ahead of the
+ * positions (kick-drift-kick with merged kicks).  This evaluates the forces at
+ * the current positions and applies the pending closing kick in place, so that
+ * bonsai_get_particles returns synchronised (x, v) that a restart loads with
+ * bonsai_set_particles and continues exactly (the next move skips the kick it
+ * would have applied). */
+int bonsai_sync_velocities(bonsai_handle h);
 
 /* Composite galaxy on the host (no counterpart in the reference): 60 % NFW-like
  * halo (r_s 10, truncated at 200), 30 % exponential disk (R_d 3, sech^2
