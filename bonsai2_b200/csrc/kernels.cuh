@@ -76,7 +76,7 @@ void launch_walk(int variant, int nblocks, const int2* groups, const TreeInfo* i
                  const float2* cell_ls, const float* group_inv_theta, float eps2, float4* acc, int* ring_pool,
                  int ring_cap, unsigned* group_counter, unsigned long long* stats, int* status, const int* sys_off,
                  int nsys, const int* root_beg, const float4* ipos_lo, const float4* jpos_lo, const float4* cell_lo,
-                 uint2* group_counts, cudaStream_t s);
+                 uint2* group_counts, const int* group_list, const unsigned* group_list_n, cudaStream_t s);
 
 // move.cu
 // lo (nullable): double-single position low parts, drifted with the high parts
@@ -87,6 +87,17 @@ void launch_move(float4* pos, float4* vel, const float4* acc, int n, float dt, i
 void launch_move_sys(float4* pos, float4* vel, const float4* acc, const int4* chunks, int nchunks,
                      const int* chunk_beg, int nsys, float dt, int* closing, float eps, int write, double* chunk_part,
                      int nblocks, unsigned* ticket, double* energies, double* sys_energies, cudaStream_t s);
+// block time steps (hierarchical levels, kick-drift-kick per particle)
+void launch_bts_open_drift(float4* pos, float4* vel, const float4* acc, const unsigned char* lev, int n, float dt,
+                           int K, int s, float4* lo, int nblocks, cudaStream_t st);
+void launch_bts_close(float4* vel, const float4* acc, unsigned char* lev, int n, float dt, int K, int s1, float eta,
+                      float eps, int assign, int nblocks, cudaStream_t st);
+void launch_bts_active_groups(const int2* groups, const TreeInfo* info, const unsigned char* lev, int K, int s1,
+                              int* list, unsigned* count, int nblocks, cudaStream_t st);
+void launch_gather_u8(const int* perm, int n, const unsigned char* in, unsigned char* out, int nblocks,
+                      cudaStream_t st);
+void launch_scatter_u8(const int* id, int n, const unsigned char* in, unsigned char* out, int nblocks,
+                       cudaStream_t st);
 // pending closing kick applied in place, then the closing flag cleared
 void launch_closing_kick(float4* vel, const float4* acc, int n, float dt, int* closing, int nblocks, cudaStream_t s);
 // FP64 direct sum inside each sample's own system (one block per sample)

@@ -263,6 +263,120 @@ void launch_closing_kick(float4* vel, const float4* acc, int n, float dt, int* c
   cudaMemsetAsync(closing, 0, sizeof(int), s);
 }
 
+// ---------------------------------------------------------------------------
+// Block time steps: hierarchical power-of-two levels, kick-drift-kick per
+// particle.  Level k steps by dt_k = dt / 2^k; the big step dt is cut into
+// 2^K substeps of dt / 2^K.  At substep s a level-k particle starts a step when
+// s is a multiple of 2^(K-k) and ends one when s + 1 is.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool on_boundary(int s, int k, int K) { return (s & ((1 << (K - k)) - 1)) == 0; }
+
+// opening half kick of the particles whose step starts at substep s, then the
+// drift of every particle by one substep (double-single when lo is given)
+__global__ void __launch_bounds__(256) k_bts_open_drift(float4* __restrict__ pos, float4* __restrict__ vel,
+                                                        const float4* __restrict__ acc,
+                                                        const unsigned char* __restrict__ lev, int n, float dt, int K,
+                                                        int s, float4* __restrict__ lo) {
+  const float dmin = ldexpf(dt, -K);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int k = lev[i];
+    float4 p = pos[i], v = vel[i];
+    if (on_boundary(s, k, K)) {
+      const float h = ldexpf(dt, -k - 1);
+      const float4 a = acc[i];
+      v.x = fmaf(a.x, h, v.x); v.y = fmaf(a.y, h, v.y); v.z = fmaf(a.z, h, v.z);
+      vel[i] = v;
+    }
+    if (lo) {
+      float4 l = lo[i];
+      ds_add(p.x, l.x, __fmul_rn(v.x, dmin));
+      ds_add(p.y, l.y, __fmul_rn(v.y, dmin));
+      ds_add(p.z, l.z, __fmul_rn(v.z, dmin));
+      lo[i] = l;
+    } else {
+      p.x = fmaf(v.x, dmin, p.x); p.y = fmaf(v.y, dmin, p.y); p.z = fmaf(v.z, dmin, p.z);
+    }
+    pos[i] = p;
+  }
+}
+
+// Closing half kick of the particles whose step ends at s1 (= s + 1) with
+// their new accelerations, then their next level: the smallest k with
+// dt / 2^k <= eta sqrt(eps / |a|), no smaller than K - (trailing zeros of s1)
+// (a step must start on its own boundary) and than the old level - 1 (a step
+// at most doubles).  assign: levels for every particle, no kick (start).
+__global__ void __launch_bounds__(256) k_bts_close(float4* __restrict__ vel, const float4* __restrict__ acc,
+                                                   unsigned char* __restrict__ lev, int n, float dt, int K, int s1,
+                                                   float eta, float eps, int assign) {
+  const int sync = (s1 & ((1 << K) - 1)) == 0 ? 0 : K - (__ffs(s1) - 1);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int k = lev[i];
+    if (!assign && !on_boundary(s1, k, K)) continue;
+    const float4 a = acc[i];
+    if (!assign) {
+      const float h = ldexpf(dt, -k - 1);
+      float4 v = vel[i];
+      v.x = fmaf(a.x, h, v.x); v.y = fmaf(a.y, h, v.y); v.z = fmaf(a.z, h, v.z);
+      vel[i] = v;
+    }
+    const float am = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(a.x, a.x), __fmul_rn(a.y, a.y)), __fmul_rn(a.z, a.z)));
+    const float dti = am > 0.f ? __fmul_rn(eta, __fsqrt_rn(__fdiv_rn(eps, am))) : 3.0e38f;
+    int kn = 0;
+    while (kn < K && ldexpf(dt, -kn) > dti) kn++;
+    kn = max(kn, sync);
+    if (!assign) kn = max(kn, k - 1);
+    lev[i] = (unsigned char)kn;
+  }
+}
+
+// groups holding at least one particle whose step ends at s1, compacted
+__global__ void __launch_bounds__(256) k_bts_active_groups(const int2* __restrict__ groups,
+                                                           const TreeInfo* __restrict__ info,
+                                                           const unsigned char* __restrict__ lev, int K, int s1,
+                                                           int* __restrict__ list, unsigned* __restrict__ count) {
+  const int ng = info->ngroups;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
+    const int2 gd = groups[g];
+    bool act = false;
+    for (int i = gd.x; i < gd.x + gd.y && !act; i++) act = on_boundary(s1, lev[i], K);
+    if (act) list[atomicAdd(count, 1u)] = g;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_gather_u8(const int* __restrict__ perm, int n,
+                                                   const unsigned char* __restrict__ in,
+                                                   unsigned char* __restrict__ out) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) out[k] = in[perm[k]];
+}
+
+__global__ void __launch_bounds__(256) k_scatter_u8(const int* __restrict__ id, int n,
+                                                    const unsigned char* __restrict__ in,
+                                                    unsigned char* __restrict__ out) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) out[id[k]] = in[k];
+}
+
+void launch_bts_open_drift(float4* pos, float4* vel, const float4* acc, const unsigned char* lev, int n, float dt,
+                           int K, int s, float4* lo, int nblocks, cudaStream_t st) {
+  k_bts_open_drift<<<nblocks, 256, 0, st>>>(pos, vel, acc, lev, n, dt, K, s, lo);
+}
+void launch_bts_close(float4* vel, const float4* acc, unsigned char* lev, int n, float dt, int K, int s1, float eta,
+                      float eps, int assign, int nblocks, cudaStream_t st) {
+  k_bts_close<<<nblocks, 256, 0, st>>>(vel, acc, lev, n, dt, K, s1, eta, eps, assign);
+}
+void launch_bts_active_groups(const int2* groups, const TreeInfo* info, const unsigned char* lev, int K, int s1,
+                              int* list, unsigned* count, int nblocks, cudaStream_t st) {
+  cudaMemsetAsync(count, 0, sizeof(unsigned), st);
+  k_bts_active_groups<<<nblocks, 256, 0, st>>>(groups, info, lev, K, s1, list, count);
+}
+void launch_gather_u8(const int* perm, int n, const unsigned char* in, unsigned char* out, int nblocks,
+                      cudaStream_t st) {
+  k_gather_u8<<<nblocks, 256, 0, st>>>(perm, n, in, out);
+}
+void launch_scatter_u8(const int* id, int n, const unsigned char* in, unsigned char* out, int nblocks,
+                       cudaStream_t st) {
+  k_scatter_u8<<<nblocks, 256, 0, st>>>(id, n, in, out);
+}
+
 // Ensemble checker: each sample's force from the particles of its own system
 // only (positions in the caller's order, systems contiguous); one block per
 // sample, fixed-order block reduction.

@@ -111,6 +111,18 @@ struct Handle {
   int out_slot = 0;
   cudaEvent_t ev_in_copied = nullptr, ev_in_consumed = nullptr, ev_out_ready[2] = {nullptr, nullptr},
               ev_out_done[2] = {nullptr, nullptr};
+  // block time steps (bts_K >= 0): per-particle level (state order, double
+  // buffered like the state), accelerations carried between substeps, and the
+  // list of groups walked in a substep
+  int bts_K = -1;
+  float bts_eta = 0.2f;
+  bool bts_ready = false;
+  unsigned char* lev[2] = {nullptr, nullptr};
+  float4* acc_alt = nullptr;
+  int* walk_list = nullptr;
+  unsigned* walk_list_n = nullptr;
+  bool walk_list_on = false;
+  bool bts_gathering = false;  // inside block_steps: levels and accelerations follow the state
   int nsys = 1, nchunks = 0;
   int *sys_off = nullptr, *chunk_beg = nullptr, *root_beg = nullptr;
   int4* chunks = nullptr;
@@ -168,9 +180,27 @@ struct Handle {
       for (int a = 0; a < 3; a++) dfree(&out_buf[k][a]);
   }
 
+  void release_bts() {
+    dfree(&lev[0]); dfree(&lev[1]); dfree(&acc_alt); dfree(&walk_list); dfree(&walk_list_n);
+    bts_ready = false;
+  }
+  int alloc_bts() {
+    release_bts();
+    if (bts_K < 0 || n == 0) return 0;
+    for (int p = 0; p < 2; p++) {
+      BONSAI_CUDA_TRY(dalloc(&lev[p], (size_t)n));
+      BONSAI_CUDA_TRY(cudaMemset(lev[p], 0, (size_t)n));
+    }
+    BONSAI_CUDA_TRY(dalloc(&acc_alt, (size_t)n));
+    BONSAI_CUDA_TRY(dalloc(&walk_list, (size_t)n));
+    BONSAI_CUDA_TRY(dalloc(&walk_list_n, 1));
+    return 0;
+  }
+
   void release_particles() {
     release_graphs();
     release_staging();
+    release_bts();
     release_systems();
     release_lo();
     for (int p = 0; p < 2; p++) { dfree(&pos[p]); dfree(&vel[p]); dfree(&id[p]); }
@@ -312,6 +342,8 @@ struct Handle {
     if (rc) return rc;
     rc = alloc_lo();
     if (rc) return rc;
+    rc = alloc_bts();
+    if (rc) return rc;
     par = 0;
     built = mp_done = grouped = forced = moved_after_forces = false;
     ever_built = ever_mp = false;
@@ -411,6 +443,14 @@ struct Handle {
     const int q = par ^ 1;
     k_gather_state<<<nsm * 8, 256, 0, st>>>(pperm, n, pos[par], vel[par], id[par], pos[q], vel[q], id[q]);
     if (precision) k_gather_pos<<<nsm * 8, 256, 0, st>>>(pperm, n, plo[par], plo[q]);
+    if (bts_K >= 0 && bts_gathering) {
+      // levels and the accelerations of inactive particles travel with them
+      launch_gather_u8(pperm, n, lev[par], lev[q], nsm * 8, st);
+      k_gather_pos<<<nsm * 8, 256, 0, st>>>(pperm, n, acc, acc_alt);
+      std::swap(acc, acc_alt);
+    } else {
+      bts_ready = false;  // the levels no longer follow the particle order
+    }
     par = q;
   }
   void enq_forces(int ncrit) {
@@ -427,7 +467,8 @@ struct Handle {
     }
     launch_walk(k, walk_blocks[k], groups, info, pos[par], jpos, cell_data, cell_open, cell_q0, cell_q1, cell_ls,
                 ginv, prm.eps * prm.eps, acc, ring, kRingCap, group_counter, stats, &info->status, so(), nsys, root_beg,
-                precision ? plo[par] : nullptr, jlo, cell_lo, ginv ? group_counts : nullptr, st);
+                precision ? plo[par] : nullptr, jlo, cell_lo, ginv ? group_counts : nullptr,
+                walk_list_on ? walk_list : nullptr, walk_list_on ? walk_list_n : nullptr, st);
   }
   void enq_move(bool write) {
     launch_move_wrapper(write);
@@ -575,6 +616,48 @@ struct Handle {
     return rc;
   }
 
+  // Block time steps over nsteps big steps of prm.dt (eager launches).
+  int block_steps(int nsteps) {
+    bts_gathering = true;
+    const int rc = block_steps_impl(nsteps);
+    bts_gathering = false;
+    return rc;
+  }
+  int block_steps_impl(int nsteps) {
+    const int nb = nsm * 8;
+    float4* lo_p = nullptr;
+    if (!bts_ready) {
+      // forces at the start, any pending closing kick, first levels
+      int rc = build_checked(cur_nleaf);
+      if (rc) return rc;
+      enq_multipoles();
+      enq_groups(cur_ls, cur_ncrit);
+      walk_list_on = false;
+      enq_forces(cur_ncrit);
+      launch_closing_kick(vel[par], acc, n, prm.dt, closing, nsm * 4, st);
+      launch_bts_close(vel[par], acc, lev[par], n, prm.dt, bts_K, 0, bts_eta, prm.eps, 1, nb, st);
+      bts_ready = true;
+    }
+    const int nsub = 1 << bts_K;
+    for (int b = 0; b < nsteps; b++) {
+      for (int s = 0; s < nsub; s++) {
+        lo_p = precision ? plo[par] : nullptr;
+        launch_bts_open_drift(pos[par], vel[par], acc, lev[par], n, prm.dt, bts_K, s, lo_p, nb, st);
+        enq_build(cur_nleaf);
+        enq_multipoles();
+        enq_groups(cur_ls, cur_ncrit);
+        launch_bts_active_groups(groups, info, lev[par], bts_K, s + 1, walk_list, walk_list_n, nb, st);
+        walk_list_on = true;
+        enq_forces(cur_ncrit);
+        walk_list_on = false;
+        launch_bts_close(vel[par], acc, lev[par], n, prm.dt, bts_K, s + 1, bts_eta, prm.eps, 0, nb, st);
+      }
+      // energies at the synchronised end of the big step (closing flag is 0)
+      enq_move(false);
+    }
+    return 0;
+  }
+
   int read_status(bool clear) {
     int s = 0;
     cudaError_t e = cudaMemcpyAsync(&s, &info->status, sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -695,6 +778,7 @@ static int set_particles_impl(Handle* h, const float* pos4, const float* vel4, i
   if (h->precision) BONSAI_CUDA_TRY(cudaMemsetAsync(h->plo[h->par], 0, bytes, h->st));  // float input: lo = 0
   BONSAI_CUDA_TRY(cudaMemsetAsync(h->closing, 0, sizeof(int), h->st));
   h->built = h->mp_done = h->grouped = h->forced = h->moved_after_forces = false;
+  h->bts_ready = false;
   return last_cuda();
 }
 
@@ -756,6 +840,7 @@ int bonsai_set_particles_async(bonsai_handle hh, const float* pos4, const float*
   if (h->precision) BONSAI_CUDA_TRY(cudaMemsetAsync(h->plo[h->par], 0, bytes, h->st));
   BONSAI_CUDA_TRY(cudaMemsetAsync(h->closing, 0, sizeof(int), h->st));
   h->built = h->mp_done = h->grouped = h->forced = h->moved_after_forces = false;
+  h->bts_ready = false;
   return last_cuda();
 }
 
@@ -1026,6 +1111,47 @@ int bonsai_sync_velocities(bonsai_handle hh) {
   h->built = h->mp_done = h->grouped = h->forced = true;
   h->ever_built = h->ever_mp = true;
   h->moved_after_forces = false;
+  return last_cuda();
+}
+
+int bonsai_set_block_steps(bonsai_handle hh, int max_level, float eta) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (max_level > 16 || (max_level >= 0 && !(eta > 0.f))) return BONSAI_ERR_ARG;
+  if (max_level >= 0 && h->nsys > 1) return BONSAI_ERR_ARG;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  h->bts_K = max_level < 0 ? -1 : max_level;
+  h->bts_eta = eta;
+  h->release_graphs();
+  return h->alloc_bts();
+}
+
+int bonsai_block_step(bonsai_handle hh, int nsteps) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (h->n == 0) return BONSAI_ERR_NOT_ALLOCATED;
+  if (h->bts_K < 0) return BONSAI_ERR_ORDER;
+  if (nsteps < 0) return BONSAI_ERR_ARG;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  const int rc = h->block_steps(nsteps);
+  if (rc) return rc;
+  h->built = h->mp_done = h->grouped = false;
+  h->ever_built = h->ever_mp = true;
+  h->forced = h->moved_after_forces = true;
+  return last_cuda();
+}
+
+int bonsai_get_levels(bonsai_handle hh, unsigned char* out) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (!out) return BONSAI_ERR_ARG;
+  if (h->bts_K < 0 || !h->bts_ready) return BONSAI_ERR_ORDER;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  unsigned char* tmp = h->lev[h->par ^ 1];
+  launch_scatter_u8(h->id[h->par], h->n, h->lev[h->par], tmp, h->nsm * 8, h->st);
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(out, tmp, (size_t)h->n, cudaMemcpyDeviceToHost, h->st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
   return last_cuda();
 }
 

@@ -144,7 +144,8 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
            unsigned long long* __restrict__ stats, int* __restrict__ status, const int* __restrict__ sys_off,
            int nsys, const int* __restrict__ root_beg, const float4* __restrict__ ipos_lo,
            const float4* __restrict__ jpos_lo, const float4* __restrict__ cell_lo,
-           uint2* __restrict__ group_counts) {
+           uint2* __restrict__ group_counts, const int* __restrict__ group_list,
+           const unsigned* __restrict__ group_list_n) {
   constexpr int STRIDE = SPLIT ? 16 : 32;
   constexpr int JSTEP = SPLIT ? 2 : 1;
   __shared__ float4 s_a0[kWalkWarps][64];
@@ -159,7 +160,8 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
   // widest level (a sweeping ring would push its dirty lines out to HBM)
   int* lists = ring_pool + (size_t)(blockIdx.x * kWalkWarps + w) * (size_t)ring_cap;
   const int half_cap = ring_cap >> 1;
-  const int ngroups = info->ngroups;
+  // group_list (optional): walk only the listed groups (block time steps)
+  const int ngroups = group_list ? (int)*group_list_n : info->ngroups;
   int l1b = info->level_beg[1], l1e = info->level_end[1];
   const unsigned lt = lanemask_lt();
   unsigned long long sum_app = 0, sum_dir = 0;
@@ -170,6 +172,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
     if (lane == 0) g = (int)atomicAdd(group_counter, 1u);
     g = __shfl_sync(kFull, g, 0);
     if (g >= ngroups) break;
+    if (group_list) g = __ldg(group_list + g);
     const int2 gd = groups[g];
     const int pbeg = gd.x, np = gd.y;
     const float inv_theta_g = PERGROUP ? group_inv_theta[g] : 0.0f;
@@ -430,10 +433,12 @@ void launch_walk(int variant, int nblocks, const int2* groups, const TreeInfo* i
                  const float4* cell_q1, const float2* cell_ls, const float* group_inv_theta, float eps2,
                  float4* acc, int* ring_pool, int ring_cap, unsigned* group_counter, unsigned long long* stats,
                  int* status, const int* sys_off, int nsys, const int* root_beg, const float4* ipos_lo,
-                 const float4* jpos_lo, const float4* cell_lo, uint2* group_counts, cudaStream_t s) {
+                 const float4* jpos_lo, const float4* cell_lo, uint2* group_counts, const int* group_list,
+                 const unsigned* group_list_n, cudaStream_t s) {
 #define BONSAI_WALK_ARGS                                                                                          \
   groups, info, ipos, jpos, cell_data, cell_open, cell_q0, cell_q1, cell_ls, group_inv_theta, eps2, acc, ring_pool, \
-      ring_cap, group_counter, stats, status, sys_off, nsys, root_beg, ipos_lo, jpos_lo, cell_lo, group_counts
+      ring_cap, group_counter, stats, status, sys_off, nsys, root_beg, ipos_lo, jpos_lo, cell_lo, group_counts,  \
+      group_list, group_list_n
 #define BONSAI_WALK(NI, SP)                                                                \
   do {                                                                                     \
     if (nsys > 1)                                                                          \

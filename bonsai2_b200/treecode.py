@@ -228,6 +228,19 @@ class Treecode:
         so that ptcl_d2h returns synchronised (x, v) for a checkpoint."""
         _check(self._L.bonsai_sync_velocities(self._h), "bonsai_sync_velocities")
 
+    def set_block_steps(self, max_level: int, eta: float = 0.2):
+        """Per-particle power-of-two time steps dt/2^k, k <= max_level
+        (max_level < 0: off)."""
+        _check(self._L.bonsai_set_block_steps(self._h, max_level, eta), "bonsai_set_block_steps")
+
+    def block_step(self, nsteps: int = 1):
+        _check(self._L.bonsai_block_step(self._h, nsteps), "bonsai_block_step")
+
+    def levels(self) -> np.ndarray:
+        out = np.empty(self.nPtcl, np.uint8)
+        _check(self._L.bonsai_get_levels(self._h, _p(out)), "bonsai_get_levels")
+        return out
+
     def set_walk_layout(self, layout: int):
         """0: two half-warps per group (nCrit <= 64), 1: one warp per group."""
         _check(self._L.bonsai_set_walk_layout(self._h, layout), "bonsai_set_walk_layout")

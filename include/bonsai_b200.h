@@ -298,6 +298,26 @@ int bonsai_write_tipsy(const char *path, double time, int n, int ndark, const fl
  * would have applied). */
 int bonsai_sync_velocities(bonsai_handle h);
 
+/* Block time steps (no counterpart in the reference; Bonsai proper's
+ * per-particle steps).  max_level = K >= 0 enables them: levels 0..K, a
+ * level-k particle steps by dt/2^k (dt from bonsai_params), kick-drift-kick
+ * per particle; its level is the smallest k with dt/2^k <= eta sqrt(eps/|a|),
+ * taken at the end of each of its steps, never before its boundary (a step
+ * starts where a step of its length may) and at most doubling the step at a
+ * time.  max_level < 0 turns them off.  Single systems only. */
+int bonsai_set_block_steps(bonsai_handle h, int max_level, float eta);
+/* nsteps big steps of dt, each 2^K substeps: per substep the opening kicks of
+ * the particles whose step starts, the drift of all particles, a tree of all
+ * particles, a walk of only the groups holding a particle whose step ends, and
+ * those particles' closing kicks and new levels.  The first call evaluates all
+ * forces and applies any pending closing kick.  All particles are
+ * synchronised at the end of every big step (bonsai_compute_energies then
+ * returns that time's energies).  With K = 0 this is the bonsai_step
+ * sequence, bit for bit. */
+int bonsai_block_step(bonsai_handle h, int nsteps);
+/* current levels in the caller's particle order (n bytes) */
+int bonsai_get_levels(bonsai_handle h, unsigned char *levels);
+
 /* Composite galaxy on the host (no counterpart in the reference): 60 % NFW-like
  * halo (r_s 10, truncated at 200), 30 % exponential disk (R_d 3, sech^2
  * z_d 0.3), 10 % Hernquist bulge (a 0.5) by particle index; log-normal masses
