@@ -69,6 +69,8 @@ def parse():
                     help="particles of the precision form (composite galaxy; 0: skip)")
     ap.add_argument("--field-n", type=int, default=1 << 25,
                     help="particles of the learned form's clustered field (0: skip)")
+    ap.add_argument("--autotune", type=int, default=1, help="report the autotuned headline configuration (0: skip)")
+    ap.add_argument("--block-levels", type=int, default=3, help="levels of the block time step block (<0: skip)")
     ap.add_argument("--batch-systems", type=int, default=512,
                     help="systems of the batching form reported beside the headline (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=32)
@@ -78,7 +80,7 @@ def parse():
     ap.add_argument("--level-split", type=int, default=5)
     ap.add_argument("--dt", type=float, default=1.0 / 128)
     ap.add_argument("--seed", type=int, default=19810614)
-    ap.add_argument("--e2e-steps", type=int, default=6)
+    ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--error-samples", type=int, default=4096)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-group-fraction", type=float, default=1.0 / 512)
@@ -350,6 +352,8 @@ def run_ours(a):
     sweep = theta_sweep(B, L, pos, vel, a, d.local) if (d.rank == 0 and a.sweep) else None
     learned = learned_theta(B, L, pos, vel, a, d.local, sweep) if (d.rank == 0 and a.learned_target > 0) else None
     batching = batching_form(B, L, a, d.local) if (d.rank == 0 and a.batch_systems > 0) else None
+    tuned = autotuned_headline(B, L, pos, vel, a, d.local) if (d.rank == 0 and a.autotune) else None
+    blocks = block_steps_form(B, L, pos, vel, a, d.local) if (d.rank == 0 and a.block_levels >= 0) else None
     precision = precision_form(B, L, a, d.local) if (d.rank == 0 and a.precision_n > 0) else None
     field = learned_field_form(B, L, a, d.local) if (d.rank == 0 and a.field_n > 0) else None
 
@@ -396,6 +400,8 @@ def run_ours(a):
             "theta_sweep": sweep,
             "learned_theta": learned,
             "batching": batching,
+            "autotuned_headline": tuned,
+            "block_time_steps": blocks,
             "precision_form": precision,
             "learned_form_clustered_field": field,
         }
@@ -662,6 +668,72 @@ def learned_field_form(B, L, a, device):
             "fixed_approx_per_particle_at_equal_median": ip_m,
             "training": {"system": "clustered field seed %d" % (a.seed + 1), "pairs": int(X.shape[0]),
                          "final_loss": loss, "seconds": t_train, "target": a.learned_target}}
+
+
+def autotuned_headline(B, L, pos, vel, a, device):
+    """The headline system with nLeaf / nCrit / walk layout from the
+    autotuner (nLeaf {8, 16, 32} x nCrit {32, 64, 128} x 2 layouts, 2 timed
+    graph steps each, untimed setup), then measured like the sweep: throughput
+    and error against the FP64 direct sum.  Reported beside the headline, which
+    keeps the reference's nLeaf 16 / nCrit 64."""
+    from bonsai2_b200.treecode import _p
+    n = pos.shape[0]
+    t = B.Treecode(eps=a.eps, theta=a.theta, ncrit=a.ncrit, nleaf=a.nleaf, level_split=a.level_split, dt=a.dt,
+                   device=device)
+    t.alloc(n)
+    L.bonsai_set_particles(t.handle, _p(pos), _p(vel), n)
+    t0 = time.perf_counter()
+    r = t.autotune(nleaf=(8, 16, 32), ncrit=(32, 64, 128), steps=2)
+    secs = time.perf_counter() - t0
+    t.close()
+    rng = np.random.default_rng(2048)
+    samp = np.ascontiguousarray(np.sort(rng.choice(n, 2048, replace=False)).astype(np.int32))
+    u = B.Treecode(eps=a.eps, theta=a.theta, device=device)
+    u.alloc(n)
+    u.h_ptclPos[:] = pos
+    u.h_ptclVel[:] = vel
+    u.ptcl_h2d()
+    ref = u.direct_fp64(samp, include_self=True)
+    u.close()
+    out = measure(B, L, pos, vel, samp, ref, theta=a.theta, eps=a.eps, device=device, nleaf=r["nleaf"],
+                  ncrit=r["ncrit"], level_split=a.level_split, dt=a.dt, steps=3)
+    out.update({"nleaf": r["nleaf"], "ncrit": r["ncrit"], "walk_layout": r["layout"], "autotune_seconds": secs,
+                "candidates_ms": r["ms"].tolist()})
+    return out
+
+
+def block_steps_form(B, L, pos, vel, a, device):
+    """Block time steps on the headline system: levels 0..K (dt/2^k),
+    eta 0.05, one big step of dt timed after one untimed big step; compared
+    with what the finest substep would cost for every particle (2^K plain
+    steps) and reported with the level histogram and the energy change over
+    the step."""
+    from bonsai2_b200.treecode import _p
+    import torch
+    n = pos.shape[0]
+    K = a.block_levels
+    t = B.Treecode(eps=a.eps, theta=a.theta, ncrit=a.ncrit, nleaf=a.nleaf, level_split=a.level_split, dt=a.dt,
+                   device=device)
+    t.alloc(n)
+    L.bonsai_set_particles(t.handle, _p(pos), _p(vel), n)
+    t.set_block_steps(K, 0.05)
+    t.block_step(1)
+    e0 = t.computeEnergies()
+    st = torch.cuda.ExternalStream(L.bonsai_stream(t.handle))
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(st)
+    t.block_step(1)
+    ev1.record(st)
+    ev1.synchronize()
+    status = t.synchronize()
+    e1 = t.computeEnergies()
+    lev = t.levels()
+    t.close()
+    ms = ev0.elapsed_time(ev1)
+    return {"levels": K, "eta": 0.05, "ms_per_big_step": ms, "substeps": 1 << K,
+            "value": n / (ms * 1e-3) / 1e6, "unit": "Mparticles per big step per s",
+            "level_histogram": np.bincount(lev, minlength=K + 1).tolist(),
+            "energy_rel_change": abs(float(e1[3]) - float(e0[3])) / abs(float(e0[3])), "status": int(status)}
 
 
 def batching_form(B, L, a, device):

@@ -36,6 +36,28 @@ def test_single_level_is_the_plain_step():
     b.close()
 
 
+def test_single_level_is_the_plain_step_in_double_single():
+    import bonsai2_b200 as B
+    p, v = B.galaxy(16384, seed=4)
+    p[:, :3] += 1000.0
+    out = []
+    for block in (False, True):
+        t = B.Treecode(**PRM)
+        t.set_precision(1)
+        t.set_particles_f64(p, v)
+        if block:
+            t.set_block_steps(0, 0.2)
+            t.block_step(3)
+        else:
+            t.step(3, graph=True)
+            t.sync_velocities()
+        assert t.synchronize() == 0
+        out.append(t.get_particles_f64())
+        t.close()
+    assert np.array_equal(out[0][0].view(np.uint64), out[1][0].view(np.uint64))
+    assert np.array_equal(out[0][1].view(np.uint32), out[1][1].view(np.uint32))
+
+
 def test_levels_follow_the_criterion_and_energy_is_kept():
     import bonsai2_b200 as B
     n, K, eta = 65536, 3, 0.05
