@@ -94,6 +94,8 @@ void launch_bts_close(float4* vel, const float4* acc, unsigned char* lev, int n,
                       float eps, int assign, int nblocks, cudaStream_t st);
 void launch_bts_active_groups(const int2* groups, const TreeInfo* info, const unsigned char* lev, int K, int s1,
                               int* list, unsigned* count, int nblocks, cudaStream_t st);
+// largest level present (into *out)
+void launch_max_level(const unsigned char* lev, int n, int* out, int nblocks, cudaStream_t st);
 void launch_gather_u8(const int* perm, int n, const unsigned char* in, unsigned char* out, int nblocks,
                       cudaStream_t st);
 void launch_scatter_u8(const int* id, int n, const unsigned char* in, unsigned char* out, int nblocks,

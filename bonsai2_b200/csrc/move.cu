@@ -343,6 +343,19 @@ __global__ void __launch_bounds__(256) k_bts_active_groups(const int2* __restric
   }
 }
 
+__global__ void __launch_bounds__(256) k_max_level(const unsigned char* __restrict__ lev, int n,
+                                                   int* __restrict__ out) {
+  int m = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) m = max(m, (int)lev[i]);
+  for (int o = 16; o >= 1; o >>= 1) m = max(m, __shfl_xor_sync(kFull, m, o));
+  if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(out, m);
+}
+
+void launch_max_level(const unsigned char* lev, int n, int* out, int nblocks, cudaStream_t st) {
+  cudaMemsetAsync(out, 0, sizeof(int), st);
+  k_max_level<<<nblocks, 256, 0, st>>>(lev, n, out);
+}
+
 __global__ void __launch_bounds__(256) k_gather_u8(const int* __restrict__ perm, int n,
                                                    const unsigned char* __restrict__ in,
                                                    unsigned char* __restrict__ out) {

@@ -121,6 +121,7 @@ struct Handle {
   float4* acc_alt = nullptr;
   int* walk_list = nullptr;
   unsigned* walk_list_n = nullptr;
+  int* max_lev = nullptr;  // device: largest level present
   bool walk_list_on = false;
   bool bts_gathering = false;  // inside block_steps: levels and accelerations follow the state
   int nsys = 1, nchunks = 0;
@@ -181,7 +182,7 @@ struct Handle {
   }
 
   void release_bts() {
-    dfree(&lev[0]); dfree(&lev[1]); dfree(&acc_alt); dfree(&walk_list); dfree(&walk_list_n);
+    dfree(&lev[0]); dfree(&lev[1]); dfree(&acc_alt); dfree(&walk_list); dfree(&walk_list_n); dfree(&max_lev);
     bts_ready = false;
   }
   int alloc_bts() {
@@ -194,6 +195,7 @@ struct Handle {
     BONSAI_CUDA_TRY(dalloc(&acc_alt, (size_t)n));
     BONSAI_CUDA_TRY(dalloc(&walk_list, (size_t)n));
     BONSAI_CUDA_TRY(dalloc(&walk_list_n, 1));
+    BONSAI_CUDA_TRY(dalloc(&max_lev, 1));
     return 0;
   }
 
@@ -639,10 +641,19 @@ struct Handle {
       bts_ready = true;
     }
     const int nsub = 1 << bts_K;
+    int maxl = bts_K;
     for (int b = 0; b < nsteps; b++) {
       for (int s = 0; s < nsub; s++) {
         lo_p = precision ? plo[par] : nullptr;
         launch_bts_open_drift(pos[par], vel[par], acc, lev[par], n, prm.dt, bts_K, s, lo_p, nb, st);
+        // the particles ending at s + 1 have level >= K - tz(s + 1); when none
+        // is that fine, the substep is the drift alone (nothing else changes)
+        if (bts_K > 0 && s + 1 < nsub) {
+          launch_max_level(lev[par], n, max_lev, nb, st);
+          BONSAI_CUDA_TRY(cudaMemcpyAsync(&maxl, max_lev, sizeof(int), cudaMemcpyDeviceToHost, st));
+          BONSAI_CUDA_TRY(cudaStreamSynchronize(st));
+          if (maxl < bts_K - (__builtin_ctz((unsigned)(s + 1)))) continue;
+        }
         enq_build(cur_nleaf);
         enq_multipoles();
         enq_groups(cur_ls, cur_ncrit);
