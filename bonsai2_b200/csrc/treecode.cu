@@ -56,6 +56,14 @@ struct Handle {
   unsigned long long *tkey = nullptr, *pkey = nullptr, *kalt = nullptr;
   int *tperm = nullptr, *pperm = nullptr, *valt = nullptr;
   unsigned *sort_counts = nullptr, *bsum = nullptr;
+  // the group branch of a step (PH sort, groups, state gather) runs on st2,
+  // beside the tree branch (tree sort, tree, multipoles), with its own sort
+  // scratch; ev_fork / ev_join tie it to the handle's stream
+  cudaStream_t st2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  unsigned long long* kalt2 = nullptr;
+  int* valt2 = nullptr;
+  unsigned* sort_counts2 = nullptr;
   uint8_t* dlev = nullptr;
   uint16_t* chain = nullptr;
   unsigned* hist = nullptr;
@@ -208,6 +216,7 @@ struct Handle {
     for (int p = 0; p < 2; p++) { dfree(&pos[p]); dfree(&vel[p]); dfree(&id[p]); }
     dfree(&acc); dfree(&jpos); dfree(&tkey); dfree(&pkey); dfree(&kalt);
     dfree(&tperm); dfree(&pperm); dfree(&valt); dfree(&sort_counts); dfree(&bsum);
+    dfree(&kalt2); dfree(&valt2); dfree(&sort_counts2);
     dfree(&dlev); dfree(&chain); dfree(&hist); dfree(&groups); dfree(&group_inv); dfree(&group_feat);
     dfree(&group_counts);
     release_cells();
@@ -228,6 +237,9 @@ struct Handle {
     dfree(&ph_table); dfree(&direct_part); dfree(&direct_out); dfree(&direct_sample);
     dfree(&mlp_w);
     if (mlp_wh) { cudaFree(mlp_wh); mlp_wh = nullptr; }
+    if (st2) { cudaStreamSynchronize(st2); cudaStreamDestroy(st2); st2 = nullptr; }
+    if (ev_fork) { cudaEventDestroy(ev_fork); ev_fork = nullptr; }
+    if (ev_join) { cudaEventDestroy(ev_join); ev_join = nullptr; }
     if (st_h2d) { cudaStreamDestroy(st_h2d); st_h2d = nullptr; }
     if (st_d2h) { cudaStreamDestroy(st_d2h); st_d2h = nullptr; }
     cudaEvent_t* evs[6] = {&ev_in_copied, &ev_in_consumed, &ev_out_ready[0], &ev_out_ready[1], &ev_out_done[0],
@@ -266,6 +278,9 @@ struct Handle {
     BONSAI_CUDA_TRY(cudaSetDevice(dev));
     BONSAI_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     BONSAI_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    BONSAI_CUDA_TRY(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
+    BONSAI_CUDA_TRY(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    BONSAI_CUDA_TRY(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     BONSAI_CUDA_TRY(cudaStreamCreateWithFlags(&st_h2d, cudaStreamNonBlocking));
     BONSAI_CUDA_TRY(cudaStreamCreateWithFlags(&st_d2h, cudaStreamNonBlocking));
     {
@@ -325,6 +340,9 @@ struct Handle {
     BONSAI_CUDA_TRY(dalloc(&pperm, N));
     BONSAI_CUDA_TRY(dalloc(&valt, N));
     BONSAI_CUDA_TRY(dalloc(&sort_counts, sort_status_words(nn)));
+    BONSAI_CUDA_TRY(dalloc(&kalt2, N));
+    BONSAI_CUDA_TRY(dalloc(&valt2, N));
+    BONSAI_CUDA_TRY(dalloc(&sort_counts2, sort_status_words(nn)));
     // scans: group counts per bin (8^7), and per position for ensembles (n)
     const int scan_m = std::max(std::max(256 * sort_tiles(nn), 1 << (3 * kMaxLevelSplit)), nn);
     BONSAI_CUDA_TRY(dalloc(&bsum, (size_t)scan_blocks(scan_m) + 1));
@@ -413,6 +431,10 @@ struct Handle {
 
   // ---------------- stages (enqueue only) ----------------
   void enq_build(int nleaf) {
+    enq_keys();
+    enq_tree(nleaf);
+  }
+  void enq_keys() {
     if (nsys > 1) {
       launch_sys_keys(pos[par], chunks, nchunks, chunk_beg, nsys, sys_box_part, sys_box, ph_table, tkey, pkey,
                       &info->status, nsm * 8, st);
@@ -421,6 +443,8 @@ struct Handle {
       k_box<<<box_blocks, 256, 0, st>>>(pos[par], n, box_partial, box_ticket, box, &info->status);
       k_keys<<<nsm * 8, 256, 0, st>>>(pos[par], n, box, ph_table, tkey, pkey);
     }
+  }
+  void enq_tree(int nleaf) {
     radix_sort_pairs(tkey, kalt, tperm, valt, nullptr, n, sort_counts, &info->status, 8, so(), nsys, st);
     k_gather_pos<<<nsm * 8, 256, 0, st>>>(tperm, n, pos[par], jpos);
     if (precision) k_gather_pos<<<nsm * 8, 256, 0, st>>>(tperm, n, plo[par], jlo);
@@ -432,28 +456,41 @@ struct Handle {
                       cell_q0, cell_q1, cell_ls, mp_count, cap_cells, precision ? jlo : nullptr,
                       precision ? cell_lo : nullptr, nsm * 8, st);
   }
-  void enq_groups(int ls, int ncrit) {
-    radix_sort_pairs(pkey, kalt, pperm, valt, nullptr, n, sort_counts, &info->status, 8, so(), nsys, st);
+  void enq_groups(int ls, int ncrit) { enq_groups_on(ls, ncrit, st, kalt, valt, sort_counts); }
+  void enq_groups_on(int ls, int ncrit, cudaStream_t s, unsigned long long* ka, int* va, unsigned* work) {
+    radix_sort_pairs(pkey, ka, pperm, va, nullptr, n, work, &info->status, 8, so(), nsys, s);
     if (nsys > 1) {
-      // kalt (8 bytes per particle) is free after the sort: segment flags and indices
-      unsigned* flag = reinterpret_cast<unsigned*>(kalt);
+      // ka (8 bytes per particle) is free after the sort: segment flags and indices
+      unsigned* flag = reinterpret_cast<unsigned*>(ka);
       make_groups_sys(pkey, n, ls, ncrit, sys_off, nsys, flag, flag + n, seg_beg, seg_end, nseg, bsum, groups, n, info,
-                      st);
+                      s);
     } else {
-      make_groups(pkey, n, ls, ncrit, g_count, g_seg, g_ng, bsum, groups, theta_mode ? gcap : n, info, st);
+      make_groups(pkey, n, ls, ncrit, g_count, g_seg, g_ng, bsum, groups, theta_mode ? gcap : n, info, s);
     }
     const int q = par ^ 1;
-    k_gather_state<<<nsm * 8, 256, 0, st>>>(pperm, n, pos[par], vel[par], id[par], pos[q], vel[q], id[q]);
-    if (precision) k_gather_pos<<<nsm * 8, 256, 0, st>>>(pperm, n, plo[par], plo[q]);
+    k_gather_state<<<nsm * 8, 256, 0, s>>>(pperm, n, pos[par], vel[par], id[par], pos[q], vel[q], id[q]);
+    if (precision) k_gather_pos<<<nsm * 8, 256, 0, s>>>(pperm, n, plo[par], plo[q]);
     if (bts_K >= 0 && bts_gathering) {
       // levels and the accelerations of inactive particles travel with them
-      launch_gather_u8(pperm, n, lev[par], lev[q], nsm * 8, st);
-      k_gather_pos<<<nsm * 8, 256, 0, st>>>(pperm, n, acc, acc_alt);
+      launch_gather_u8(pperm, n, lev[par], lev[q], nsm * 8, s);
+      k_gather_pos<<<nsm * 8, 256, 0, s>>>(pperm, n, acc, acc_alt);
       std::swap(acc, acc_alt);
     } else {
       bts_ready = false;  // the levels no longer follow the particle order
     }
     par = q;
+  }
+  // keys, then the tree branch (handle's stream) and the group branch (st2)
+  // concurrently; both only read the keys and the current state
+  void enq_build_groups(int nleaf, int ls, int ncrit) {
+    enq_keys();
+    cudaEventRecord(ev_fork, st);
+    cudaStreamWaitEvent(st2, ev_fork, 0);
+    enq_tree(nleaf);
+    enq_multipoles();
+    enq_groups_on(ls, ncrit, st2, kalt2, valt2, sort_counts2);
+    cudaEventRecord(ev_join, st2);
+    cudaStreamWaitEvent(st, ev_join, 0);
   }
   void enq_forces(int ncrit) {
     const int k = walk_variant(ncrit, walk_layout);
@@ -478,18 +515,14 @@ struct Handle {
   void launch_move_wrapper(bool write);
 
   void enq_step() {
-    enq_build(cur_nleaf);
-    enq_multipoles();
-    enq_groups(cur_ls, cur_ncrit);
+    enq_build_groups(cur_nleaf, cur_ls, cur_ncrit);
     enq_forces(cur_ncrit);
     enq_move(true);
   }
 
   void enq_phase(int k) {
     if (k == 0) {
-      enq_build(cur_nleaf);
-      enq_multipoles();
-      enq_groups(cur_ls, cur_ncrit);
+      enq_build_groups(cur_nleaf, cur_ls, cur_ncrit);
     } else if (k == 1) {
       enq_forces(cur_ncrit);
     } else {
@@ -654,9 +687,7 @@ struct Handle {
           BONSAI_CUDA_TRY(cudaStreamSynchronize(st));
           if (maxl < bts_K - (__builtin_ctz((unsigned)(s + 1)))) continue;
         }
-        enq_build(cur_nleaf);
-        enq_multipoles();
-        enq_groups(cur_ls, cur_ncrit);
+        enq_build_groups(cur_nleaf, cur_ls, cur_ncrit);
         launch_bts_active_groups(groups, info, lev[par], bts_K, s + 1, walk_list, walk_list_n, nb, st);
         walk_list_on = true;
         enq_forces(cur_ncrit);
