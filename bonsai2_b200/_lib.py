@@ -84,6 +84,7 @@ SIGNATURES = {
     "bonsai_read_tipsy": (I, [ctypes.c_char_p, P, P, P, P, P]),
     "bonsai_write_tipsy": (I, [ctypes.c_char_p, ctypes.c_double, I, I, P, P, P]),
     "bonsai_sync_velocities": (I, [P]),
+    "bonsai_compute_forces_fp64": (I, [P, P, P]),
     "bonsai_set_block_steps": (I, [P, I, ctypes.c_float]),
     "bonsai_block_step": (I, [P, I]),
     "bonsai_get_levels": (I, [P, P]),

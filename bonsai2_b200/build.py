@@ -23,9 +23,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INCLUDE, "--expt-relaxed-constexpr"]
 # extra -D tuning flags (e.g. BONSAI_WALK_SPLIT=0) for alternative builds
 EXTRA = os.environ.get("BONSAI_NVCC_DEFINES", "").split()
-PER_FILE = {"walk.cu": ["-ftz=true"]}
+PER_FILE = {"walk.cu": ["-ftz=true"], "walk64.cu": ["-ftz=true"]}
 SOURCES = ["keys.cu", "sort.cu", "tree.cu", "multipoles.cu", "groups.cu", "walk.cu", "move.cu", "treecode.cu",
-           "noalloc.cu", "learned.cu"]
+           "noalloc.cu", "learned.cu", "walk64.cu"]
 HOST_SOURCES = ["plummer.cpp", "ics.cpp", "tipsy.cpp"]
 
 

@@ -78,6 +78,14 @@ void launch_walk(int variant, int nblocks, const int2* groups, const TreeInfo* i
                  int nsys, const int* root_beg, const float4* ipos_lo, const float4* jpos_lo, const float4* cell_lo,
                  uint2* group_counts, const int* group_list, const unsigned* group_list_n, cudaStream_t s);
 
+// walk64.cu: the FP64 checker walk (same interaction lists as the float walk)
+void launch_walk64(int nblocks, const int2* groups, const TreeInfo* info, const float4* ipos, const float4* ipos_lo,
+                   const float4* jpos, const float4* jpos_lo, const uint4* cell_data, const float4* cell_open,
+                   const float4* cell_lo, const float2* cell_ls, const float* group_inv_theta, const MpRec* rec,
+                   double eps2, double4* acc, int* ring_pool, int ring_cap, unsigned* group_counter,
+                   unsigned long long* stats, int* status, cudaStream_t s);
+void launch_scatter_d4(const int* id, int n, const double4* in, double4* out, int nblocks, cudaStream_t s);
+
 // move.cu
 // lo (nullable): double-single position low parts, drifted with the high parts
 void launch_move(float4* pos, float4* vel, const float4* acc, int n, float dt, int* closing, float eps, int write,

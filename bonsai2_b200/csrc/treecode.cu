@@ -81,6 +81,7 @@ struct Handle {
   float* group_inv = nullptr;
   float* group_feat = nullptr;
   uint2* group_counts = nullptr;  // per-group (approx, direct) counts of the per-group angle walk
+  double4 *acc64 = nullptr, *acc64_tmp = nullptr;  // FP64 checker walk output (group order, caller order)
   float* mlp_w = nullptr;
   void* mlp_wh = nullptr;
   bool mlp_loaded = false;
@@ -218,7 +219,7 @@ struct Handle {
     dfree(&tperm); dfree(&pperm); dfree(&valt); dfree(&sort_counts); dfree(&bsum);
     dfree(&kalt2); dfree(&valt2); dfree(&sort_counts2);
     dfree(&dlev); dfree(&chain); dfree(&hist); dfree(&groups); dfree(&group_inv); dfree(&group_feat);
-    dfree(&group_counts);
+    dfree(&group_counts); dfree(&acc64); dfree(&acc64_tmp);
     release_cells();
     n = 0;
   }
@@ -1136,6 +1137,34 @@ int bonsai_get_particles_f64(bonsai_handle hh, double* pos4, float* vel4, float*
     pos4[4 * i + 2] = (double)hi[i].z + (double)lo[i].z;
     pos4[4 * i + 3] = (double)hi[i].w;
   }
+  return last_cuda();
+}
+
+int bonsai_compute_forces_fp64(bonsai_handle hh, double* acc4, unsigned long long* stats4) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (!h->built || !h->mp_done || !h->grouped) return BONSAI_ERR_ORDER;
+  if (h->nsys > 1) return BONSAI_ERR_ARG;
+  if (h->theta_mode == 1 && !h->forced) return BONSAI_ERR_ORDER;  // the network's angles come from compute_forces
+  if (h->cur_ncrit > 128) return BONSAI_ERR_ARG;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  if (!h->acc64) {
+    BONSAI_CUDA_TRY(dalloc(&h->acc64, (size_t)h->n));
+    BONSAI_CUDA_TRY(dalloc(&h->acc64_tmp, (size_t)h->n));
+  }
+  BONSAI_CUDA_TRY(cudaMemsetAsync(h->group_counter, 0, sizeof(unsigned), h->st));
+  BONSAI_CUDA_TRY(cudaMemsetAsync(h->stats, 0, 4 * sizeof(unsigned long long), h->st));
+  const double e2 = (double)h->prm.eps * (double)h->prm.eps;
+  const int nblocks = h->ring_warps / (256 / 32);
+  launch_walk64(nblocks, h->groups, h->info, h->pos[h->par], h->precision ? h->plo[h->par] : nullptr, h->jpos,
+                h->jlo, h->cell_data, h->cell_open, h->cell_lo, h->cell_ls, h->theta_mode ? h->group_inv : nullptr,
+                h->rec, e2, h->acc64, h->ring, kRingCap, h->group_counter, h->stats, &h->info->status, h->st);
+  if (acc4) {
+    launch_scatter_d4(h->id[h->par], h->n, h->acc64, h->acc64_tmp, h->nsm * 8, h->st);
+    BONSAI_CUDA_TRY(cudaMemcpyAsync(acc4, h->acc64_tmp, (size_t)h->n * sizeof(double4), cudaMemcpyDeviceToHost, h->st));
+  }
+  if (stats4) BONSAI_CUDA_TRY(cudaMemcpyAsync(stats4, h->stats, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
   return last_cuda();
 }
 

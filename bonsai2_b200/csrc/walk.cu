@@ -33,6 +33,7 @@
 
 #include "common.cuh"
 #include "kernels.cuh"
+#include "walk_common.cuh"
 
 namespace bonsai {
 
@@ -53,19 +54,6 @@ constexpr int kWalkWarps = kWalkThreads / 32;
 struct IPart {
   float x, y, z;
 };
-
-// Opening test of split_node_grav_impbh (computeForces.cu:30-54), explicitly
-// rounded so that the CPU restatement reproduces it bit for bit.
-__device__ __forceinline__ bool open_cell(const float4 co, const float3 gc, const float3 gs) {
-  float dx = __fsub_rn(fabsf(__fsub_rn(gc.x, co.x)), gs.x);
-  float dy = __fsub_rn(fabsf(__fsub_rn(gc.y, co.y)), gs.y);
-  float dz = __fsub_rn(fabsf(__fsub_rn(gc.z, co.z)), gs.z);
-  dx = __fmul_rn(__fadd_rn(dx, fabsf(dx)), 0.5f);
-  dy = __fmul_rn(__fadd_rn(dy, fabsf(dy)), 0.5f);
-  dz = __fmul_rn(__fadd_rn(dz, fabsf(dz)), 0.5f);
-  const float ds2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
-  return ds2 < fabsf(co.w);
-}
 
 // quadrupole: a0 = (COM, -0.5 tr I), a1 = (M, 3Ixx, 3Iyy, 3Izz), a2 = (3Ixy, 3Ixz, 3Iyz, 1.5 tr I)
 //   phi -= M/r - 0.5 tr/r^3 + 1.5 dIdr/r^5
@@ -102,17 +90,6 @@ __device__ __forceinline__ void mono_acc(float4& acc, const IPart& p, const floa
   acc.x = fmaf(mr3, dx, acc.x);
   acc.y = fmaf(mr3, dy, acc.y);
   acc.z = fmaf(mr3, dz, acc.z);
-}
-
-// binary search over the warp's inclusive scan: the lane whose range holds s
-__device__ __forceinline__ int find_src(int incl, int s) {
-  int src = 0;
-#pragma unroll
-  for (int step = 16; step >= 1; step >>= 1) {
-    const int v = __shfl_sync(kFull, incl, src + step - 1);
-    if (v <= s) src += step;
-  }
-  return src;
 }
 
 // Particle ownership.  SPLIT: lane l holds particles (l & 15) + 16k, k < NI,

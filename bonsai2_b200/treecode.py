@@ -223,6 +223,15 @@ class Treecode:
         _check(self._L.bonsai_get_particles_f64(self._h, _p(p), _p(v), _p(a)), "bonsai_get_particles_f64")
         return p, v, a
 
+    def compute_forces_fp64(self):
+        """FP64 checker walk with the float walk's interaction lists:
+        ((n, 4) float64 accelerations and potentials in caller order,
+        interaction statistics as get_stats)."""
+        a = np.empty((self.nPtcl, 4), np.float64)
+        st = np.zeros(4, np.uint64)
+        _check(self._L.bonsai_compute_forces_fp64(self._h, _p(a), _p(st)), "bonsai_compute_forces_fp64")
+        return a, st
+
     def sync_velocities(self):
         """Forces at the current positions and the pending half kick applied,
         so that ptcl_d2h returns synchronised (x, v) for a checkpoint."""

@@ -217,6 +217,18 @@ int bonsai_mlp_train(int device, const float *X, const float *y, int S, float *w
                      float hi, float over, double *loss);
 int bonsai_mlp_predict(int device, const float *X, int S, const float *w, float lo, float hi, float *theta);
 
+/* FP64 checker walk (the FP64 option; no counterpart in the reference, whose
+ * tree-build experiments have a -DFP64 switch, treebuild/readme:8-9): after
+ * the stages up to makeGroups (and compute_forces for theta mode 1), walks the
+ * same tree for the same groups with the float walk's opening decisions, so the
+ * interaction lists are identical, and evaluates every interaction in FP64
+ * from the FP64 cell records and the exact positions.  acc4 (optional):
+ * n x (ax, ay, az, phi) doubles in caller order; stats4 (optional): as
+ * bonsai_get_stats.  Against the float walk the difference is rounding alone;
+ * against bonsai_direct_fp64 it is multipole truncation alone.  Slow (a
+ * checker).  Single systems, nCrit <= 128. */
+int bonsai_compute_forces_fp64(bonsai_handle h, double *acc4, unsigned long long *stats4);
+
 /* ---- Double-single positions (precision form) ----
  * No counterpart in the reference (float positions throughout).  mode 1
  * keeps every position as a float pair hi + lo: the tree, keys and groups are
