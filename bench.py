@@ -614,6 +614,17 @@ def precision_form(B, L, a, device):
         r = measure(B, L, small, vel[:m], small_samp, ref_far, theta=a.theta, eps=eps, device=device, precision=prec,
                     steps=1)
         far[key] = {"median_rel_force_err": r["median_rel_force_err"], "p99_rel_force_err": r["p99_rel_force_err"]}
+    # the FP64 checker walk on the same lists: the truncation error alone
+    t = B.Treecode(eps=eps, theta=a.theta, device=device)
+    t.set_precision(1)
+    t.set_particles_f64(small, vel[:m])
+    t.buildTree(16)
+    t.computeMultipoles()
+    t.makeGroups(5, 64)
+    a64, _ = t.compute_forces_fp64()
+    t.close()
+    e64 = np.linalg.norm(a64[small_samp, :3] - ref_far[:, :3], axis=1) / np.linalg.norm(ref_far[:, :3], axis=1)
+    far["fp64_walk"] = {"median_rel_force_err": float(np.median(e64)), "p99_rel_force_err": float(np.percentile(e64, 99))}
     out["shifted_to_1e4"] = dict(far, particles=m, shift=[1.0e4, -7.0e3, 5.0e3])
     return out
 
