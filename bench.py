@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--field-n", type=int, default=1 << 25,
                     help="particles of the learned form's clustered field (0: skip)")
     ap.add_argument("--autotune", type=int, default=1, help="report the autotuned headline configuration (0: skip)")
+    ap.add_argument("--octree-n", type=int, default=20000000,
+                    help="particles of the octree-build comparison with the reference's published build (0: skip)")
     ap.add_argument("--block-levels", type=int, default=3, help="levels of the block time step block (<0: skip)")
     ap.add_argument("--batch-systems", type=int, default=512,
                     help="systems of the batching form reported beside the headline (0: skip)")
@@ -353,6 +355,7 @@ def run_ours(a):
     learned = learned_theta(B, L, pos, vel, a, d.local, sweep) if (d.rank == 0 and a.learned_target > 0) else None
     batching = batching_form(B, L, a, d.local) if (d.rank == 0 and a.batch_systems > 0) else None
     tuned = autotuned_headline(B, L, pos, vel, a, d.local) if (d.rank == 0 and a.autotune) else None
+    octree = octree_build_form(B, L, a, d.local) if (d.rank == 0 and a.octree_n > 0) else None
     blocks = block_steps_form(B, L, pos, vel, a, d.local) if (d.rank == 0 and a.block_levels >= 0) else None
     precision = precision_form(B, L, a, d.local) if (d.rank == 0 and a.precision_n > 0) else None
     field = learned_field_form(B, L, a, d.local) if (d.rank == 0 and a.field_n > 0) else None
@@ -401,6 +404,7 @@ def run_ours(a):
             "learned_theta": learned,
             "batching": batching,
             "autotuned_headline": tuned,
+            "octree_build": octree,
             "block_time_steps": blocks,
             "precision_form": precision,
             "learned_form_clustered_field": field,
@@ -679,6 +683,45 @@ def learned_field_form(B, L, a, device):
             "fixed_approx_per_particle_at_equal_median": ip_m,
             "training": {"system": "clustered field seed %d" % (a.seed + 1), "pairs": int(X.shape[0]),
                          "final_loss": loss, "seconds": t_train, "target": a.learned_target}}
+
+
+# the reference's one published number: the standalone octree build of a
+# float32 Plummer sphere, N = 20,000,000, NLEAF 16, sm_35 (treebuild/readme:32-40)
+PUBLISHED_OCTREE_MPTCL_S = 58.7943
+PUBLISHED_OCTREE_SHAPE = {"nodes": 596463, "leaves": 4041848, "cells": 4638311, "levels": 15}
+
+
+def octree_build_form(B, L, a, device):
+    """The octree build alone (box, both keys, tree-key sort, gather into tree
+    order, cells, levels, leaves: bonsai_build_tree) on the configuration of
+    the reference's published build, timed with CUDA events over 5 builds
+    after a warm-up build; tree shape beside the published one."""
+    import torch
+    from bonsai2_b200.treecode import _p
+    n = a.octree_n
+    p, v = B.plummer(n, a.seed)
+    t = B.Treecode(eps=a.eps, theta=a.theta, nleaf=16, device=device)
+    t.alloc(n)
+    L.bonsai_set_particles(t.handle, _p(p), _p(v), n)
+    t.buildTree(16)
+    st = torch.cuda.ExternalStream(L.bonsai_stream(t.handle))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 5
+    e0.record(st)
+    for _ in range(reps):
+        t.buildTree(16)
+    e1.record(st)
+    e1.synchronize()
+    info = t.tree_info()
+    t.close()
+    ms = e0.elapsed_time(e1) / reps
+    value = n / (ms * 1e-3) / 1e6
+    return {"particles": n, "nleaf": 16, "ms": ms, "value": value, "unit": "Mparticles/s",
+            "published_value": PUBLISHED_OCTREE_MPTCL_S, "vs_published": value / PUBLISHED_OCTREE_MPTCL_S,
+            "published_hardware": "sm_35 (K20+), treebuild_scan.cu PreferEqual", "note": "different GPU generations",
+            "shape": {"nodes": info["nnodes"], "leaves": info["nleaves"], "cells": info["ncells"],
+                      "levels": info["nlevels"]},
+            "published_shape": PUBLISHED_OCTREE_SHAPE}
 
 
 def autotuned_headline(B, L, pos, vel, a, device):
