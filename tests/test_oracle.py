@@ -151,3 +151,17 @@ def test_multipoles_ref_vs_fp64(oracle):
     ex = oracle.multipoles_fp64(t.pbeg, t.pend, S.jpos)
     assert np.allclose(S.mono4[:, 3], ex[:, 0], rtol=1e-6)
     assert np.allclose(S.mono4[:, :3], ex[:, 1:4], rtol=1e-5, atol=1e-6)
+
+
+def test_oracle_tree_shape_matches_the_published_build(oracle):
+    """treebuild/readme:33-39: the reference's build of a float32 Plummer sphere
+    (plummer.h, default seed), N = 20,000,000, NLEAF 16, has 596,463 nodes,
+    4,041,848 leaves, 4,638,311 cells and 15 levels.  The oracle's comparison
+    partition reproduces it exactly (about 10 s on 8 cores)."""
+    pos, _ = oracle.plummer_float4(20_000_000, 19810614)
+    box, _ = oracle.bbox(pos)
+    T = oracle.OracleTree(pos, box, 16)
+    assert T.ncells == 4638311
+    assert int((T.nchild > 0).sum()) == 596463
+    assert int((T.nchild == 0).sum()) == 4041848
+    assert int(T.level.max()) == 15
