@@ -351,14 +351,17 @@ def run_ours(a):
     e2e_value = n * d.world / (e2e * 1e-3) / 1e6
 
     t.close()
-    sweep = theta_sweep(B, L, pos, vel, a, d.local) if (d.rank == 0 and a.sweep) else None
-    learned = learned_theta(B, L, pos, vel, a, d.local, sweep) if (d.rank == 0 and a.learned_target > 0) else None
-    batching = batching_form(B, L, a, d.local) if (d.rank == 0 and a.batch_systems > 0) else None
-    tuned = autotuned_headline(B, L, pos, vel, a, d.local) if (d.rank == 0 and a.autotune) else None
-    octree = octree_build_form(B, L, a, d.local) if (d.rank == 0 and a.octree_n > 0) else None
-    blocks = block_steps_form(B, L, pos, vel, a, d.local) if (d.rank == 0 and a.block_levels >= 0) else None
-    precision = precision_form(B, L, a, d.local) if (d.rank == 0 and a.precision_n > 0) else None
-    field = learned_field_form(B, L, a, d.local) if (d.rank == 0 and a.field_n > 0) else None
+    # the forms beside the headline run on a single GPU only (under torchrun
+    # every rank reports the replicated headline and leaves together)
+    solo = d.rank == 0 and d.world == 1
+    sweep = theta_sweep(B, L, pos, vel, a, d.local) if (solo and a.sweep) else None
+    learned = learned_theta(B, L, pos, vel, a, d.local, sweep) if (solo and a.learned_target > 0) else None
+    batching = batching_form(B, L, a, d.local) if (solo and a.batch_systems > 0) else None
+    tuned = autotuned_headline(B, L, pos, vel, a, d.local) if (solo and a.autotune) else None
+    octree = octree_build_form(B, L, a, d.local) if (solo and a.octree_n > 0) else None
+    blocks = block_steps_form(B, L, pos, vel, a, d.local) if (solo and a.block_levels >= 0) else None
+    precision = precision_form(B, L, a, d.local) if (solo and a.precision_n > 0) else None
+    field = learned_field_form(B, L, a, d.local) if (solo and a.field_n > 0) else None
 
     cpu = None
     if d.rank == 0 and d.world == 1 and not a.no_cpu_baseline:
