@@ -409,9 +409,11 @@ struct Handle {
     BONSAI_CUDA_TRY(cudaMemcpy(chunks, ch.data(), ch.size() * sizeof(int4), cudaMemcpyHostToDevice));
     BONSAI_CUDA_TRY(cudaMemset(sys_energy, 0, (size_t)ns * 8 * sizeof(double)));
     BONSAI_CUDA_TRY(cudaMemset(root_beg, 0, (size_t)(ns + 1) * sizeof(int)));
-    theta_mode = 0;  // per-group angles and double-single positions are single-system features
+    theta_mode = 0;  // per-group angles, double-single positions, block steps: single systems
     precision = 0;
     release_lo();
+    bts_K = -1;
+    release_bts();
     return 0;
   }
 
@@ -579,21 +581,24 @@ struct Handle {
   // before each trial and at the end, and keeps the fastest.
   int autotune(const int* nl, int nnl, const int* nc, int nnc, int steps, float* results, int* best) {
     const size_t N = (size_t)n;
-    float4 *sp = nullptr, *sv = nullptr;
+    float4 *sp = nullptr, *sv = nullptr, *sl = nullptr;
     int* si = nullptr;
     int closing0 = 0;
     BONSAI_CUDA_TRY(dalloc(&sp, N));
     BONSAI_CUDA_TRY(dalloc(&sv, N));
     BONSAI_CUDA_TRY(dalloc(&si, N));
+    if (precision) BONSAI_CUDA_TRY(dalloc(&sl, N));
     BONSAI_CUDA_TRY(cudaMemcpyAsync(sp, pos[par], N * sizeof(float4), cudaMemcpyDeviceToDevice, st));
     BONSAI_CUDA_TRY(cudaMemcpyAsync(sv, vel[par], N * sizeof(float4), cudaMemcpyDeviceToDevice, st));
     BONSAI_CUDA_TRY(cudaMemcpyAsync(si, id[par], N * sizeof(int), cudaMemcpyDeviceToDevice, st));
+    if (precision) BONSAI_CUDA_TRY(cudaMemcpyAsync(sl, plo[par], N * sizeof(float4), cudaMemcpyDeviceToDevice, st));
     BONSAI_CUDA_TRY(cudaMemcpyAsync(&closing0, closing, sizeof(int), cudaMemcpyDeviceToHost, st));
     BONSAI_CUDA_TRY(cudaStreamSynchronize(st));
     auto restore = [&]() -> int {
       BONSAI_CUDA_TRY(cudaMemcpyAsync(pos[par], sp, N * sizeof(float4), cudaMemcpyDeviceToDevice, st));
       BONSAI_CUDA_TRY(cudaMemcpyAsync(vel[par], sv, N * sizeof(float4), cudaMemcpyDeviceToDevice, st));
       BONSAI_CUDA_TRY(cudaMemcpyAsync(id[par], si, N * sizeof(int), cudaMemcpyDeviceToDevice, st));
+      if (precision) BONSAI_CUDA_TRY(cudaMemcpyAsync(plo[par], sl, N * sizeof(float4), cudaMemcpyDeviceToDevice, st));
       BONSAI_CUDA_TRY(cudaMemcpyAsync(closing, &closing0, sizeof(int), cudaMemcpyHostToDevice, st));
       return 0;
     };
@@ -640,7 +645,7 @@ struct Handle {
     if (rc >= 0) rc = (int)cudaStreamSynchronize(st) == 0 ? 0 : -1000 - (int)cudaGetLastError();
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    dfree(&sp); dfree(&sv); dfree(&si);
+    dfree(&sp); dfree(&sv); dfree(&si); dfree(&sl);
     cur_nleaf = bl;
     cur_ncrit = bc;
     walk_layout = blay;

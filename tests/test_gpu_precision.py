@@ -135,3 +135,18 @@ def test_precision_rejected_for_ensembles():
     t.set_systems(np.array([100, 200], np.int32))
     assert t._L.bonsai_set_precision(t.handle, 1) == -4
     t.close()
+
+
+def test_autotune_restores_double_single_state():
+    import bonsai2_b200 as B
+    pos, vel = B.galaxy(1 << 15, seed=8)
+    pos[:, :3] += 1.0e4
+    t = B.Treecode(eps=0.01, theta=0.5)
+    t.set_precision(1)
+    t.set_particles_f64(pos, vel)
+    before = t.get_particles_f64()
+    t.autotune(nleaf=(8, 16), ncrit=(32, 64), steps=1)
+    after = t.get_particles_f64()
+    assert np.array_equal(before[0].view(np.uint64), after[0].view(np.uint64))
+    assert np.array_equal(before[1].view(np.uint32), after[1].view(np.uint32))
+    t.close()
