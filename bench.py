@@ -76,6 +76,7 @@ def parse():
     ap.add_argument("--batch-systems", type=int, default=512,
                     help="systems of the batching form reported beside the headline (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=32)
+    ap.add_argument("--batch-autotune", type=int, default=1, help="autotune the ensemble's nLeaf/nCrit/layout (0: keep 16/64)")
     ap.add_argument("--eps", type=float, default=0.005)
     ap.add_argument("--nleaf", type=int, default=16)
     ap.add_argument("--ncrit", type=int, default=64)
@@ -811,7 +812,10 @@ def batching_form(B, L, a, device):
     t.set_systems(counts)
     L.bonsai_set_particles(t.handle, _p(pos), _p(vel), n)
     t0 = time.perf_counter()
-    tune = t.autotune(nleaf=(8, 16, 32), ncrit=(16, 32, 64, 128), steps=2)
+    if a.batch_autotune:
+        tune = t.autotune(nleaf=(8, 16, 32), ncrit=(16, 32, 64, 128), steps=2)
+    else:
+        tune = {"nleaf": 16, "ncrit": 64, "layout": 0}
     t_tune = time.perf_counter() - t0
     nl, nc, lay = tune["nleaf"], tune["ncrit"], tune["layout"]
     # accuracy at the initial positions
