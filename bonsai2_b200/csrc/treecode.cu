@@ -732,7 +732,8 @@ Handle* H(bonsai_handle h) { return reinterpret_cast<Handle*>(h); }
 
 int check_params(const bonsai_params* p) {
   if (!p) return BONSAI_ERR_ARG;
-  if (!(p->theta > 0.f) || !(p->eps >= 0.f) || !std::isfinite(p->dt)) return BONSAI_ERR_ARG;
+  // eps > 0: every particle's own term is part of its sum (as in the reference), singular at eps = 0
+  if (!(p->theta > 0.f) || !(p->eps > 0.f) || !std::isfinite(p->dt)) return BONSAI_ERR_ARG;
   if (p->nleaf < 1 || p->nleaf > 64) return BONSAI_ERR_ARG;
   if (p->ncrit < 1 || p->ncrit > 128) return BONSAI_ERR_ARG;
   if (p->level_split < 1 || p->level_split > kMaxLevelSplit) return BONSAI_ERR_ARG;

@@ -50,7 +50,7 @@ typedef struct bonsai_handle_s *bonsai_handle;
 
 typedef struct bonsai_params {
   float theta;      /* opening angle: Treecode::theta (Treecode.h:133,167) */
-  float eps;        /* softening: Treecode::eps2 = eps*eps (Treecode.h:133,166) */
+  float eps;        /* softening > 0: Treecode::eps2 = eps*eps (Treecode.h:133,166); the i == j term is summed */
   int nleaf;        /* max particles per leaf, 1..64: buildTree(nLeaf) (Treecode.h:216) */
   int ncrit;        /* max particles per group, 1..128: makeGroups(levelSplit, nCrit) (Treecode.h:218) */
   int level_split;  /* PH octal digits per group segment, 1..7 (Treecode.h:218; treecode.cu:142 passes 5) */

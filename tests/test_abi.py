@@ -56,3 +56,17 @@ def test_default_params(lib):
     p = B.default_params()
     assert abs(p.theta - 0.75) < 1e-7 and abs(p.eps - 0.01) < 1e-7   # Treecode.h:164
     assert p.nleaf == 16 and p.ncrit == 64 and p.level_split == 5
+
+
+def test_parameters_are_checked_before_any_device_work(lib):
+    # argument errors come back before the device is touched, so they hold on any machine
+    import ctypes
+
+    import bonsai2_b200 as B
+    for field, bad in (("eps", 0.0), ("eps", -1.0), ("theta", 0.0), ("nleaf", 0), ("nleaf", 65), ("ncrit", 129),
+                       ("level_split", 8)):
+        p = B.default_params()
+        setattr(p, field, bad)
+        h = ctypes.c_void_p()
+        assert lib.bonsai_create(ctypes.byref(p), ctypes.byref(h)) == -4, (field, bad)
+        assert not h.value
