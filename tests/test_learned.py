@@ -143,3 +143,41 @@ def test_learned_theta_gains_over_fixed_theta(oracle, lib):
     c_eq = _interp_cost([(th, p, c) for th, m, p, c in sweep], pL)
     assert c_eq is not None, (pL, sweep)
     assert cL < c_eq, (mL, pL, cL, c_eq, sweep)
+
+
+@pytest.mark.gpu
+def test_cost_optimal_allocation_beats_fixed_angle():
+    """The cost-optimal per-group angles (allocation_labels on every group's
+    error and cost tables) walk the same system at equal median error for
+    less work than a fixed angle: measured in the walk's model flops from its
+    interaction counts, so the result is deterministic."""
+    import bonsai2_b200 as B
+    from bonsai2_b200 import learned as Lr
+    n = 1 << 18
+    p, v = B.plummer(n, 21)
+    F, E, C, sz = Lr.training_tables(p, v, eps=0.01, samples_per_group=8, max_groups=1 << 30)
+    y, info = Lr.allocation_labels(E, C, sz, Lr.DEFAULT_GRID, 1e-3)
+    assert info["bound_gain"] > 1.1
+    # the same tables, read for the allocation and for every fixed angle: cost at equal median
+    rows = np.arange(E.shape[0])
+    j = np.abs(np.asarray(Lr.DEFAULT_GRID)[None, :] - y[:, None].astype(np.float64)).argmin(axis=1)
+    med_alloc = Lr._wmedian(E[rows, j], sz)
+    cost_alloc = C[rows, j].sum()
+    fixed = [(Lr._wmedian(E[:, k], sz), C[:, k].sum()) for k in range(E.shape[1])]
+    cheaper = [c for m, c in fixed if m <= med_alloc]
+    assert cheaper and cost_alloc < 0.9 * min(cheaper)
+    # and applied in a walk (theta mode 2), the counted work matches the tables
+    t = B.Treecode(eps=0.01, theta=0.5)
+    t.alloc(n)
+    t.h_ptclPos[:] = p
+    t.h_ptclVel[:] = v
+    t.ptcl_h2d()
+    t.buildTree(16)
+    t.computeMultipoles()
+    t.makeGroups(5, 64)
+    Lr.set_theta_mode(t, 2)
+    Lr.set_group_theta(t, y)
+    t.computeForces(False)
+    cnt = Lr.group_interactions(t).astype(np.float64)
+    assert np.isclose((64.0 * cnt[:, 0] + 20.0 * cnt[:, 1]).sum(), cost_alloc, rtol=1e-9)
+    t.close()
