@@ -39,14 +39,16 @@ struct Chain {
   int a, b;  // levels [a, b]; a == 0: no cell starts here
 };
 
-__device__ __forceinline__ Chain make_chain(const uint8_t* sd, int loc, int i, int n, int nleaf, bool* fat) {
-  // sd[loc + j] = d(i + j) for j in [-kHalo, kHalo]
+// sd[loc + j] = d(i + j) for j in [-kHalo, kHalo] (0 past n); wm[x] = min of sd
+// over [x, x + wp), wp the largest power of two <= nleaf, so that
+// m(i) = min d(i+1 .. i+nleaf) = min(wm[loc + 1], wm[loc + 1 + nleaf - wp])
+__device__ __forceinline__ Chain make_chain(const uint8_t* sd, const uint8_t* wm, int wp, int loc, int i, int n,
+                                            int nleaf, bool* fat) {
   Chain c{0, 0};
   const int di = (i == 0) ? 0 : (int)sd[loc];
   const int ls = max(di, 1);
   if (ls > kMaxLevel) return c;
-  int m = kMaxLevel + 1;
-  for (int j = 1; j <= nleaf; j++) m = min(m, (i + j >= n) ? 0 : (int)sd[loc + j]);
+  const int m = min((int)wm[loc + 1], (int)wm[loc + 1 + nleaf - wp]);
   if (ls < m) {
     c.a = ls;
     c.b = min(m, kMaxLevel);
@@ -118,6 +120,18 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_chains(const unsigned lon
   load_d_from_keys(keys, n, t0, sd, sk, sys_off, nsys);
   for (int j = threadIdx.x; j < kTreeTile; j += blockDim.x)
     if (t0 + j < n) dlev[t0 + j] = sd[kHalo + j];
+  // window minima of d by doubling, in the key buffer's space (no longer read)
+  constexpr int kLen = kTreeTile + 2 * kHalo;
+  uint8_t* cur = reinterpret_cast<uint8_t*>(sk);
+  uint8_t* nxt = cur + kLen;
+  for (int j = threadIdx.x; j < kLen; j += blockDim.x) cur[j] = sd[j];
+  __syncthreads();
+  int wp = 1;
+  for (; 2 * wp <= nleaf; wp *= 2) {
+    for (int j = threadIdx.x; j < kLen; j += blockDim.x) nxt[j] = min(cur[j], j + wp < kLen ? cur[j + wp] : (uint8_t)0);
+    __syncthreads();
+    uint8_t* t = cur; cur = nxt; nxt = t;
+  }
   bool anyfat = false;
   const int i0 = t0 + threadIdx.x * kTreeItems;
 #pragma unroll 1
@@ -125,7 +139,7 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_chains(const unsigned lon
     const int i = i0 + k;
     if (i >= n) break;
     bool fat = false;
-    const Chain c = make_chain(sd, kHalo + (i - t0), i, n, nleaf, &fat);
+    const Chain c = make_chain(sd, cur, wp, kHalo + (i - t0), i, n, nleaf, &fat);
     anyfat |= fat;
     chain[i] = (uint16_t)(c.a | (c.b << 8));
     if (c.a) {
