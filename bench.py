@@ -652,7 +652,9 @@ def learned_field_form(B, L, a, device):
     X, y, _ = Lr.training_set(ptr, vtr, eps=eps, target=a.learned_target, max_groups=8192, device=device)
     w, loss = Lr.train(X, y, epochs=3000, lr=3e-3, device=device)
     t_train = time.perf_counter() - t0
-    c, lo, hi, e_cal = Lr.calibrate(ptr, vtr, w, eps, a.learned_target, device=device)
+    # field realisations differ more than Plummer seeds: calibrate to 0.8 x target
+    # (0.9 x target on the training field gave 1.07e-3 on the bench field)
+    c, lo, hi, e_cal = Lr.calibrate(ptr, vtr, w, eps, a.learned_target, fraction=0.8, device=device)
     del ptr, vtr
     rng = np.random.default_rng(2048)
     samp = np.ascontiguousarray(np.sort(rng.choice(n, 2048, replace=False)).astype(np.int32))
@@ -673,6 +675,7 @@ def learned_field_form(B, L, a, device):
         r["gain_at_equal_median"] = r["value"] / em if em else None
         r["gain_at_equal_p99"] = r["value"] / ep if ep else None
         r["scale"] = c
+        r["calibration_fraction"] = 0.8
         r["median_err_on_training_field"] = e_cal
     eq_m = at_equal(sweep, "value", "median_rel_force_err", lrn["median_rel_force_err"])
     eq_p = at_equal(sweep, "value", "p99_rel_force_err", lrn["p99_rel_force_err"])
