@@ -51,6 +51,7 @@ SIGNATURES = {
     "bonsai_graph_kernel_count": (I, [P]),
     "bonsai_get_stats": (I, [P, P]),
     "bonsai_fp32_peak": (I, [I, P]),
+    "bonsai_selftest_wait_bound": (I, [I]),
     "bonsai_synchronize": (I, [P]),
     "bonsai_stream": (P, [P]),
     "bonsai_copy_streams": (I, [P, P, P]),

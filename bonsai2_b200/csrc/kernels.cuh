@@ -35,6 +35,9 @@ void radix_sort_pairs(unsigned long long* keys_a, unsigned long long* keys_b, in
                       const int* vals_in, int n, unsigned* work, int* err, int passes, const int* sys_off, int nsys,
                       cudaStream_t s);
 
+// bounded look-back self-test: returns the status bits of a pass whose first tile never runs
+int sort_timeout_selftest(cudaStream_t s);
+
 // tree.cu
 int tree_tiles(int n);
 void build_tree(const unsigned long long* sorted_keys, int n, int nleaf, int cell_cap, int leaf_cap, uint8_t* dlev,

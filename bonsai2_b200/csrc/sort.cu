@@ -322,4 +322,39 @@ void radix_sort_pairs(unsigned long long* keys_a, unsigned long long* keys_b, in
   }
 }
 
+// Self-test of the look-back bound: one pass over three tiles launched as two
+// blocks with the tile counter starting at 1, so tile 0 never runs and tile 1
+// waits on a flag that nothing sets.  The wait must end at its bound with
+// kStatusSortTimeout in *err, and tile 2 must then finish behind tile 1.
+// Returns the status bits (or a CUDA error as -1000 - code).
+int sort_timeout_selftest(cudaStream_t s) {
+  const int n = 3 * kSortTile, nt = 3;
+  unsigned long long *ka = nullptr, *kb = nullptr;
+  int *va = nullptr, *err = nullptr;
+  unsigned *status = nullptr, *counter = nullptr, *gbase = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (e == cudaSuccess) e = cudaMalloc(&ka, n * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc(&kb, n * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc(&va, 2 * n * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&err, sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&status, (size_t)nt * 256 * sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMalloc(&counter, sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMalloc(&gbase, 256 * sizeof(unsigned));
+  int result = 0;
+  if (e == cudaSuccess) {
+    cudaMemsetAsync(ka, 0, n * sizeof(unsigned long long), s);
+    cudaMemsetAsync(status, 0, (size_t)nt * 256 * sizeof(unsigned), s);
+    cudaMemsetAsync(gbase, 0, 256 * sizeof(unsigned), s);
+    cudaMemsetAsync(err, 0, sizeof(int), s);
+    const unsigned one = 1u;
+    cudaMemcpyAsync(counter, &one, sizeof(unsigned), cudaMemcpyHostToDevice, s);
+    k_sort_onesweep<false><<<nt - 1, kSortThreads, 0, s>>>(ka, nullptr, n, 0, gbase, status, counter, kb, va + n, err,
+                                                           nullptr, 0);
+    cudaMemcpyAsync(&result, err, sizeof(int), cudaMemcpyDeviceToHost, s);
+    e = cudaStreamSynchronize(s);
+  }
+  cudaFree(ka); cudaFree(kb); cudaFree(va); cudaFree(err); cudaFree(status); cudaFree(counter); cudaFree(gbase);
+  return e == cudaSuccess ? result : -(int)e - 1000;
+}
+
 }  // namespace bonsai

@@ -1657,6 +1657,15 @@ int bonsai_clustered_field(long n, unsigned long long seed, int nclusters, float
   return bonsai_clustered_field_impl(n, seed, nclusters, pos4, vel4);
 }
 
+int bonsai_selftest_wait_bound(int device) {
+  BONSAI_CUDA_TRY(cudaSetDevice(device));
+  cudaStream_t st;
+  BONSAI_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  const int r = sort_timeout_selftest(st);
+  cudaStreamDestroy(st);
+  return r;
+}
+
 int bonsai_fp32_peak(int device, double* tflops) {
   if (!tflops) return BONSAI_ERR_ARG;
   BONSAI_CUDA_TRY(cudaSetDevice(device));

@@ -137,6 +137,12 @@ int bonsai_graph_kernel_count(bonsai_handle h);
 /* interaction statistics of the last walk (computeForces.cu:568-609):
  * {sum over particles of n_approx, of n_direct, max n_approx, max n_direct} */
 int bonsai_get_stats(bonsai_handle h, unsigned long long *out4);
+/* Failure-detection self-test (no counterpart in the reference, whose waits
+ * are unbounded): runs one radix-sort pass whose first tile never starts, so
+ * the next tile's look-back waits on a flag nothing sets; the wait must end at
+ * its bound and report.  Returns the status bits (BONSAI_STATUS_SORT_TIMEOUT
+ * expected) after a fraction of a second; the device stays usable. */
+int bonsai_selftest_wait_bound(int device);
 /* measured FP32 FMA throughput of the device (TFLOP/s): the walk's roofline */
 int bonsai_fp32_peak(int device, double *tflops);
 /* Wait for the handle's stream and its copy streams; returns the sticky device

@@ -169,3 +169,23 @@ def test_full_size_properties(lib):
     d = t.direct_fp64(samp, include_self=True)
     err = np.linalg.norm(acc[samp, :3] - d[:, :3], axis=1) / np.linalg.norm(d[:, :3], axis=1)
     assert np.median(err) < 1e-3
+
+
+def test_bounded_wait_reports_and_device_stays_usable():
+    """A radix-sort pass whose first tile never starts: the next tile's
+    look-back waits on a flag nothing sets, ends at its bound and reports
+    BONSAI_STATUS_SORT_TIMEOUT; the device then runs a normal step."""
+    import bonsai2_b200 as B
+    L = B.load()
+    r = L.bonsai_selftest_wait_bound(0)
+    assert r >= 0 and (r & 64)
+    p, v = B.plummer(4096, 3)
+    t = B.Treecode(eps=0.01, theta=0.5)
+    t.alloc(4096)
+    t.h_ptclPos[:] = p
+    t.h_ptclVel[:] = v
+    t.ptcl_h2d()
+    t.step(1, graph=True)
+    assert t.synchronize() == 0
+    assert np.isfinite(t.get_acc()).all()
+    t.close()
