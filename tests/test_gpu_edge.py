@@ -189,3 +189,68 @@ def test_bounded_wait_reports_and_device_stays_usable():
     assert t.synchronize() == 0
     assert np.isfinite(t.get_acc()).all()
     t.close()
+
+
+def test_walk_level_list_overflow_reports_status():
+    """A uniform cube at a tiny opening angle: breadth-first levels wider than
+    a warp's list capacity.  The walk reports BONSAI_STATUS_WALK_STACK and
+    marks the affected groups' forces NaN instead of writing past its lists."""
+    import bonsai2_b200 as B
+    n = 1 << 18
+    rng = np.random.default_rng(4)
+    p = np.zeros((n, 4), np.float32)
+    p[:, :3] = rng.uniform(-1, 1, (n, 3))
+    p[:, 3] = 1.0 / n
+    v = np.zeros((n, 4), np.float32)
+    t = B.Treecode(eps=0.01, theta=0.02)
+    t.alloc(n)
+    t.h_ptclPos[:] = p
+    t.h_ptclVel[:] = v
+    t.ptcl_h2d()
+    t.buildTree(1)
+    t.computeMultipoles()
+    t.makeGroups(5, 64)
+    with pytest.raises(B.BonsaiError) as e:
+        B.treecode._check(t._L.bonsai_compute_forces(t.handle, 0, None) or t._L.bonsai_synchronize(t.handle), "walk")
+    assert e.value.code & 4
+    a = t.get_acc()
+    assert np.isnan(a[:, 0]).any()
+    t.close()
+
+
+def test_cell_capacity_overflow_in_graph_replay_then_recovery():
+    """Graphs are captured with cell arrays sized for the particles of the
+    time (plus a margin).  Particles that need many more cells (tightly bound
+    pairs at nLeaf 1) overflow them on replay: the step reports
+    BONSAI_STATUS_CELL_CAPACITY without writing past the arrays; an eager build
+    regrows them and the next step is clean."""
+    import bonsai2_b200 as B
+    n = 4096
+    rng = np.random.default_rng(5)
+    a = np.zeros((n, 4), np.float32)
+    a[:, :3] = rng.uniform(-1, 1, (n, 3))
+    a[:, 3] = 1.0 / n
+    v = np.zeros((n, 4), np.float32)
+    t = B.Treecode(eps=0.01, theta=0.5, nleaf=1)
+    t.alloc(n)
+    t.h_ptclPos[:] = a
+    t.h_ptclVel[:] = v
+    t.ptcl_h2d()
+    t.step(1, graph=True)
+    assert t.synchronize() == 0
+    cells_a = t.tree_info()["ncells"]
+    b = a.copy()
+    b[1::2, :3] = b[0::2, :3] + np.float32(1e-5)  # pairs 1e-5 apart: ~17 more levels each
+    t.h_ptclPos[:] = b
+    t.ptcl_h2d()
+    t.step(1, graph=True)
+    st = t._L.bonsai_synchronize(t.handle)
+    assert st > 0 and (st & 1)
+    t.buildTree(1)  # eager build: grows the cell arrays (and drops the graphs)
+    assert t.tree_info()["ncells"] > 2 * cells_a
+    t.h_ptclPos[:] = b
+    t.ptcl_h2d()
+    t.step(1, graph=True)
+    assert t.synchronize() == 0
+    assert np.isfinite(t.get_acc()).all()
+    t.close()
