@@ -30,6 +30,7 @@
 //     formulation, counted as 64 flops by treecode.cu:149-158, is the same
 //     algebra).
 #include <algorithm>
+#include <type_traits>
 
 #include "common.cuh"
 #include "kernels.cuh"
@@ -51,46 +52,100 @@ constexpr int kWalkWarps = kWalkThreads / 32;
 #define BONSAI_DO_PRAGMA(x) _Pragma(#x)
 #define BONSAI_UNROLL_N(n) BONSAI_DO_PRAGMA(unroll n)
 
+#ifndef BONSAI_WALK_PACKED
+#define BONSAI_WALK_PACKED 1
+#endif
+
 struct IPart {
   float x, y, z;
 };
 
-// quadrupole: a0 = (COM, -0.5 tr I), a1 = (M, 3Ixx, 3Iyy, 3Izz), a2 = (3Ixy, 3Ixz, 3Iyz, 1.5 tr I)
+// Interaction arithmetic over V = float (one i-particle) or V = float2 (two
+// i-particles of the lane, evaluated by the packed FFMA2/FMUL2/FADD2 of
+// sm_100: one instruction per pair, same FP32 pipe rate, half the issue
+// slots).  Sources are scalars broadcast into both halves.
+__device__ __forceinline__ float vfma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ float vmul(float a, float b) { return a * b; }
+__device__ __forceinline__ float vadd(float a, float b) { return a + b; }
+__device__ __forceinline__ float vrsqrt(float a) { return rsqrtf(a); }
+__device__ __forceinline__ float vdup(float a, float) { return a; }
+__device__ __forceinline__ float2 vfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 vmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 vadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 vrsqrt(float2 a) { return make_float2(rsqrtf(a.x), rsqrtf(a.y)); }
+__device__ __forceinline__ float2 vdup(float a, float2) { return make_float2(a, a); }
+
+// i-state: negated coordinates n = -x_i; accumulators (ax, ay, az, -phi)
+template <class V>
+struct IVec {
+  V nx, ny, nz;
+};
+template <class V>
+struct AVec {
+  V x, y, z, w;
+};
+
+// Staged sources.  Quadrupole (moments negated at staging):
+//   a0 = (COM, -0.5 tr I), a1 = (M, -3Ixx, -3Iyy, -3Izz), a2 = (-3Ixy, -3Ixz, -3Iyz, -1.5 tr I)
+// With d = COM - x_i = -dr, q = -3I d = 3 I dr and w = q.d = -3 dIdr:
 //   phi -= M/r - 0.5 tr/r^3 + 1.5 dIdr/r^5
 //   a   += [-M + u (1.5 tr - 7.5 dIdr u)] dr / r^3 + 3 I dr / r^5,   dr = x_i - COM
-__device__ __forceinline__ void quad_acc(float4& acc, const IPart& p, const float4 a0, const float4 a1,
-                                         const float4 a2, float eps2) {
-  const float dx = p.x - a0.x, dy = p.y - a0.y, dz = p.z - a0.z;
-  const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
-  const float rinv = rsqrtf(r2);
-  const float u = rinv * rinv;
-  const float qx = fmaf(a2.y, dz, fmaf(a2.x, dy, a1.y * dx));
-  const float qy = fmaf(a2.z, dz, fmaf(a1.z, dy, a2.x * dx));
-  const float qz = fmaf(a1.w, dz, fmaf(a2.z, dy, a2.y * dx));
-  const float qrr = fmaf(qz, dz, fmaf(qy, dy, qx * dx));  // 3 dIdr
-  const float r3 = rinv * u;
-  const float r5 = r3 * u;
-  const float b = qrr * u;
-  const float ca = fmaf(u, fmaf(-2.5f, b, a2.w), -a1.x) * r3;
-  acc.x = fmaf(r5, qx, fmaf(ca, dx, acc.x));
-  acc.y = fmaf(r5, qy, fmaf(ca, dy, acc.y));
-  acc.z = fmaf(r5, qz, fmaf(ca, dz, acc.z));
-  const float pp = fmaf(u, fmaf(0.5f, b, a0.w), a1.x);
-  acc.w = fmaf(-rinv, pp, acc.w);
+// is a += [M - u (1.5 tr + 2.5 w u)] d / r^3 + q / r^5 and
+// -phi += [M + u (-0.5 tr - 0.5 w u)] / r: 34 FP32 operations + 1 rsqrt.
+template <class V>
+__device__ __forceinline__ void quad_acc(AVec<V>& acc, const IVec<V>& p, const float4 a0, const float4 a1,
+                                         const float4 a2, V eps2) {
+  const V dx = vadd(vdup(a0.x, eps2), p.nx), dy = vadd(vdup(a0.y, eps2), p.ny), dz = vadd(vdup(a0.z, eps2), p.nz);
+  const V r2 = vfma(dz, dz, vfma(dy, dy, vfma(dx, dx, eps2)));
+  const V rinv = vrsqrt(r2);
+  const V u = vmul(rinv, rinv);
+  const V qx = vfma(vdup(a2.y, eps2), dz, vfma(vdup(a2.x, eps2), dy, vmul(vdup(a1.y, eps2), dx)));
+  const V qy = vfma(vdup(a2.z, eps2), dz, vfma(vdup(a1.z, eps2), dy, vmul(vdup(a2.x, eps2), dx)));
+  const V qz = vfma(vdup(a1.w, eps2), dz, vfma(vdup(a2.z, eps2), dy, vmul(vdup(a2.y, eps2), dx)));
+  const V qrr = vfma(qz, dz, vfma(qy, dy, vmul(qx, dx)));
+  const V r3 = vmul(rinv, u);
+  const V r5 = vmul(r3, u);
+  const V b = vmul(qrr, u);
+  const V ca = vmul(vfma(u, vfma(vdup(-2.5f, eps2), b, vdup(a2.w, eps2)), vdup(a1.x, eps2)), r3);
+  acc.x = vfma(r5, qx, vfma(ca, dx, acc.x));
+  acc.y = vfma(r5, qy, vfma(ca, dy, acc.y));
+  acc.z = vfma(r5, qz, vfma(ca, dz, acc.z));
+  const V pp = vfma(u, vfma(vdup(-0.5f, eps2), b, vdup(a0.w, eps2)), vdup(a1.x, eps2));
+  acc.w = vfma(rinv, pp, acc.w);
 }
 
-// monopole (computeForces.cu:58-78): dr = x_j - x_i
-__device__ __forceinline__ void mono_acc(float4& acc, const IPart& p, const float4 j, float eps2) {
-  const float dx = j.x - p.x, dy = j.y - p.y, dz = j.z - p.z;
-  const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
-  const float rinv = rsqrtf(r2);
-  const float mr = j.w * rinv;
-  const float mr3 = mr * rinv * rinv;
-  acc.w -= mr;
-  acc.x = fmaf(mr3, dx, acc.x);
-  acc.y = fmaf(mr3, dy, acc.y);
-  acc.z = fmaf(mr3, dz, acc.z);
+// monopole (computeForces.cu:58-78): d = x_j - x_i
+template <class V>
+__device__ __forceinline__ void mono_acc(AVec<V>& acc, const IVec<V>& p, const float4 j, V eps2) {
+  const V dx = vadd(vdup(j.x, eps2), p.nx), dy = vadd(vdup(j.y, eps2), p.ny), dz = vadd(vdup(j.z, eps2), p.nz);
+  const V r2 = vfma(dz, dz, vfma(dy, dy, vfma(dx, dx, eps2)));
+  const V rinv = vrsqrt(r2);
+  const V mr = vmul(vdup(j.w, eps2), rinv);
+  const V mr3 = vmul(vmul(mr, rinv), rinv);
+  acc.w = vadd(acc.w, mr);
+  acc.x = vfma(mr3, dx, acc.x);
+  acc.y = vfma(mr3, dy, acc.y);
+  acc.z = vfma(mr3, dz, acc.z);
 }
+
+// NI i-particles of a lane as NV vectors of type V
+template <int NI>
+struct Lanes {
+#if BONSAI_WALK_PACKED
+  typedef typename std::conditional<(NI >= 2), float2, float>::type V;
+  static constexpr int NV = NI >= 2 ? NI / 2 : NI;
+#else
+  typedef float V;
+  static constexpr int NV = NI;
+#endif
+};
+
+__device__ __forceinline__ void set_lane(float& v, int, float x) { v = x; }
+__device__ __forceinline__ void set_lane(float2& v, int h, float x) {
+  if (h) v.y = x; else v.x = x;
+}
+__device__ __forceinline__ float get_lane(float v, int) { return v; }
+__device__ __forceinline__ float get_lane(float2 v, int h) { return h ? v.y : v.x; }
 
 // Particle ownership.  SPLIT: lane l holds particles (l & 15) + 16k, k < NI,
 // both half-warps hold the same particles, the two halves evaluate alternate
@@ -158,8 +213,9 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
       l1b = __ldg(root_beg + sy);
       l1e = __ldg(root_beg + sy + 1);
     }
+    typedef typename Lanes<NI>::V V;
+    constexpr int NV = Lanes<NI>::NV;
     IPart pi[NI];
-    float4 ai[NI];
     float3 R = make_float3(0.f, 0.f, 0.f);
     if (DS) {
       const float4 r0 = ipos[pbeg];
@@ -178,7 +234,6 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
       } else {
         pi[k].x = p.x; pi[k].y = p.y; pi[k].z = p.z;
       }
-      ai[k] = make_float4(0.f, 0.f, 0.f, 0.f);
       mnx = fminf(mnx, pi[k].x); mny = fminf(mny, pi[k].y); mnz = fminf(mnz, pi[k].z);
       mxx = fmaxf(mxx, pi[k].x); mxy = fmaxf(mxy, pi[k].y); mxz = fmaxf(mxz, pi[k].z);
     }
@@ -188,6 +243,17 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
                                   __fmul_rn(0.5f, __fadd_rn(mxz, mnz)));
     const float3 gs = make_float3(__fmul_rn(0.5f, __fsub_rn(mxx, mnx)), __fmul_rn(0.5f, __fsub_rn(mxy, mny)),
                                   __fmul_rn(0.5f, __fsub_rn(mxz, mnz)));
+    const V veps2 = vdup(eps2, V());
+    IVec<V> iv[NV];
+    AVec<V> av[NV];
+#pragma unroll
+    for (int k = 0; k < NI; k++) {
+      set_lane(iv[k % NV].nx, k / NV, -pi[k].x);
+      set_lane(iv[k % NV].ny, k / NV, -pi[k].y);
+      set_lane(iv[k % NV].nz, k / NV, -pi[k].z);
+    }
+#pragma unroll
+    for (int v = 0; v < NV; v++) av[v].x = av[v].y = av[v].z = av[v].w = vdup(0.0f, V());
 
     int cb = 0;  // base of the current level's half; the next level's is cb ^ half_cap
     int ncur = l1e - l1b, nnext = 0;
@@ -243,9 +309,10 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
         if (app) {
           const int slot = (a_head + a_cnt + __popc(bal & lt)) & 63;
           const float4 q1 = __ldg(cell_q1 + cell);
+          const float4 q0 = __ldg(cell_q0 + cell);
           s_a0[w][slot] = make_float4(co.x, co.y, co.z, q1.w * (-1.0f / 3.0f));
-          s_a1[w][slot] = __ldg(cell_q0 + cell);
-          s_a2[w][slot] = q1;
+          s_a1[w][slot] = make_float4(q0.x, -q0.y, -q0.z, -q0.w);
+          s_a2[w][slot] = make_float4(-q1.x, -q1.y, -q1.z, -q1.w);
         }
         a_cnt += __popc(bal);
         if (a_cnt >= 32) {
@@ -257,7 +324,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
           for (int j = 0; j < 32; j += JSTEP) {
             const float4 a0 = A0[j], a1 = A1[j], a2 = A2[j];
 #pragma unroll
-            for (int k = 0; k < NI; k++) quad_acc(ai[k], pi[k], a0, a1, a2, eps2);
+            for (int v = 0; v < NV; v++) quad_acc(av[v], iv[v], a0, a1, a2, veps2);
           }
           __syncwarp();
           a_head = (a_head + 32) & 63;
@@ -295,7 +362,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
             for (int j = 0; j < 32; j += JSTEP) {
               const float4 pj = D[j];
 #pragma unroll
-              for (int k = 0; k < NI; k++) mono_acc(ai[k], pi[k], pj, eps2);
+              for (int v = 0; v < NV; v++) mono_acc(av[v], iv[v], pj, veps2);
             }
             __syncwarp();
             d_head = (d_head + 32) & 63;
@@ -316,16 +383,21 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
       const int sl = (a_head + j) & 63;
       const float4 a0 = s_a0[w][sl], a1 = s_a1[w][sl], a2 = s_a2[w][sl];
 #pragma unroll
-      for (int k = 0; k < NI; k++) quad_acc(ai[k], pi[k], a0, a1, a2, eps2);
+      for (int v = 0; v < NV; v++) quad_acc(av[v], iv[v], a0, a1, a2, veps2);
     }
     n_app += a_cnt;
     for (int j = half; j < d_cnt; j += JSTEP) {
       const float4 pj = s_d[w][(d_head + j) & 63];
 #pragma unroll
-      for (int k = 0; k < NI; k++) mono_acc(ai[k], pi[k], pj, eps2);
+      for (int v = 0; v < NV; v++) mono_acc(av[v], iv[v], pj, veps2);
     }
     n_dir += d_cnt;
     __syncwarp();
+    float4 ai[NI];
+#pragma unroll
+    for (int k = 0; k < NI; k++)
+      ai[k] = make_float4(get_lane(av[k % NV].x, k / NV), get_lane(av[k % NV].y, k / NV),
+                          get_lane(av[k % NV].z, k / NV), -get_lane(av[k % NV].w, k / NV));
     if (SPLIT) {
 #pragma unroll
       for (int k = 0; k < NI; k++) {

@@ -143,7 +143,8 @@ int bonsai_get_stats(bonsai_handle h, unsigned long long *out4);
  * its bound and report.  Returns the status bits (BONSAI_STATUS_SORT_TIMEOUT
  * expected) after a fraction of a second; the device stays usable. */
 int bonsai_selftest_wait_bound(int device);
-/* measured FP32 FMA throughput of the device (TFLOP/s): the walk's roofline */
+/* measured FP32 FMA throughput of the device (TFLOP/s; the faster of scalar
+ * FFMA and packed FFMA2 chains): the walk's roofline */
 int bonsai_fp32_peak(int device, double *tflops);
 /* Wait for the handle's stream and its copy streams; returns the sticky device
  * status (and clears it). */
