@@ -9,8 +9,10 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-# BONSAI_B200_LIB selects an alternative build of the same library (tuning builds)
+# BONSAI_B200_LIB selects an alternative build of the same library (tuning
+# builds, or the bounds-checked CHECKED_LIB_PATH)
 LIB_PATH = os.environ.get("BONSAI_B200_LIB") or os.path.join(HERE, "libbonsai_b200.so")
+CHECKED_LIB_PATH = os.path.join(HERE, "libbonsai_b200_checks.so")
 
 
 class bonsai_params(ctypes.Structure):
@@ -52,6 +54,8 @@ SIGNATURES = {
     "bonsai_get_stats": (I, [P, P]),
     "bonsai_fp32_peak": (I, [I, P]),
     "bonsai_selftest_wait_bound": (I, [I]),
+    "bonsai_bounds_check": (I, [P, P, I]),
+    "bonsai_bounds_selftest": (I, [I]),
     "bonsai_synchronize": (I, [P]),
     "bonsai_stream": (P, [P]),
     "bonsai_copy_streams": (I, [P, P, P]),

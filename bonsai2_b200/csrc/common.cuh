@@ -40,7 +40,8 @@ struct TreeInfo {
   int nlevels;
   int ngroups;
   int status;
-  int pad[2];
+  int npart;  // particles of the build (all systems of an ensemble)
+  int pad;
   int level_beg[kLevels];   // half-open [beg, end) cell range of level L
   int level_end[kLevels];
 };
@@ -89,6 +90,39 @@ __device__ __forceinline__ int warp_incl_scan(int v) {
 __device__ __forceinline__ int set_status(int* status, int bit) {
   return atomicOr(status, bit);
 }
+
+// Bounds-checked build (compiled with -DBONSAI_CHECKS).  BONSAI_IN_RANGE(i, n,
+// site) tests 0 <= i < n; a failure is counted in this translation unit's
+// word, the first failing site is recorded, and the caller skips the access
+// (no trap: the kernel runs on and the host reads the count).  Sites are
+// (kernel file << 8) | number.  In the normal build the macro is the constant
+// true and the guarded accesses compile exactly as before.
+#ifdef BONSAI_CHECKS
+static __device__ unsigned g_bounds_word[2];  // violations, first failing site
+__device__ __forceinline__ bool in_range_checked(long long i, long long n, unsigned site) {
+  if (i >= 0 && i < n) return true;
+  if (atomicAdd(&g_bounds_word[0], 1u) == 0u) g_bounds_word[1] = site;
+  return false;
+}
+#define BONSAI_IN_RANGE(i, n, site) ::bonsai::in_range_checked((long long)(i), (long long)(n), (unsigned)(site))
+// host accessor of this translation unit's word (after a device synchronise)
+#define BONSAI_BOUNDS_ACCESSOR(name)                                                    \
+  int name(unsigned* w, bool reset) {                                                   \
+    if (cudaMemcpyFromSymbol(w, g_bounds_word, 2 * sizeof(unsigned)) != cudaSuccess)    \
+      return -1;                                                                        \
+    const unsigned zero[2] = {0u, 0u};                                                  \
+    if (reset && cudaMemcpyToSymbol(g_bounds_word, zero, sizeof(zero)) != cudaSuccess) \
+      return -1;                                                                        \
+    return 0;                                                                           \
+  }
+#else
+#define BONSAI_IN_RANGE(i, n, site) true
+#define BONSAI_BOUNDS_ACCESSOR(name) \
+  int name(unsigned* w, bool) {      \
+    w[0] = w[1] = 0u;                \
+    return 0;                        \
+  }
+#endif
 
 // Ensemble layout: system s owns particles [off[s], off[s+1]) of the state
 // arrays; every stage keeps that partition (sorts and gathers stay inside a

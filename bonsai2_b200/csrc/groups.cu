@@ -21,11 +21,12 @@ namespace bonsai {
 // Each bin has one start and one end, so every entry is written by exactly one
 // thread (no atomics); empty bins keep [0, 0) from the memset.
 __global__ void __launch_bounds__(256) k_group_bounds(const unsigned long long* __restrict__ sorted, int n,
-                                                      int shift, unsigned* __restrict__ seg_beg,
-                                                      unsigned* __restrict__ seg_end) {
+                                                      int shift, [[maybe_unused]] int nbins,
+                                                      unsigned* __restrict__ seg_beg, unsigned* __restrict__ seg_end) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const unsigned b = (unsigned)(sorted[i] >> shift);
     const unsigned p = i > 0 ? (unsigned)(sorted[i - 1] >> shift) : ~0u;
+    if (!BONSAI_IN_RANGE(b, nbins, 0x201) || (i > 0 && !BONSAI_IN_RANGE(p, nbins, 0x202))) continue;
     if (b != p) {
       seg_beg[b] = (unsigned)i;
       if (i > 0) seg_end[p] = (unsigned)i;
@@ -47,7 +48,7 @@ __global__ void __launch_bounds__(256) k_group_write(const unsigned* __restrict_
                                                      const unsigned* __restrict__ seg_start,
                                                      const unsigned* __restrict__ goff, int nbins, int ncrit,
                                                      int2* __restrict__ groups, int group_cap,
-                                                     TreeInfo* __restrict__ info) {
+                                                     TreeInfo* __restrict__ info, [[maybe_unused]] int n) {
   const int ng = info->ngroups;
   if (ng > group_cap) {
     if (blockIdx.x == 0 && threadIdx.x == 0) set_status(&info->status, kStatusGroupCapacity);
@@ -64,6 +65,8 @@ __global__ void __launch_bounds__(256) k_group_write(const unsigned* __restrict_
     const int k = g - (int)goff[lo];
     const int off = k * ncrit;
     const int count = (int)(seg_end[lo] - seg_start[lo]);
+    // every group holds at least one particle, inside the particle range
+    if (!BONSAI_IN_RANGE(off, count, 0x203) || !BONSAI_IN_RANGE((int)seg_start[lo] + count - 1, n, 0x204)) continue;
     groups[g] = make_int2((int)seg_start[lo] + off, min(ncrit, count - off));
   }
 }
@@ -75,10 +78,10 @@ void make_groups(const unsigned long long* sorted_ph, int n, int level_split, in
   const int shift = 63 - 3 * level_split;
   cudaMemsetAsync(seg_start, 0, sizeof(unsigned) * (size_t)nbins, s);
   cudaMemsetAsync(seg_end, 0, sizeof(unsigned) * (size_t)nbins, s);
-  k_group_bounds<<<1184, 256, 0, s>>>(sorted_ph, n, shift, seg_start, seg_end);
+  k_group_bounds<<<1184, 256, 0, s>>>(sorted_ph, n, shift, nbins, seg_start, seg_end);
   k_group_sizes<<<(nbins + 255) / 256, 256, 0, s>>>(seg_start, seg_end, nbins, ncrit, ng);
   exclusive_scan(ng, ng, nbins, bsum, (unsigned*)&info->ngroups, s);
-  k_group_write<<<1184, 256, 0, s>>>(seg_end, seg_start, ng, nbins, ncrit, groups, group_cap, info);
+  k_group_write<<<1184, 256, 0, s>>>(seg_end, seg_start, ng, nbins, ncrit, groups, group_cap, info, n);
 }
 
 // Ensembles.  Bins repeat from system to system, so segments are numbered by
@@ -103,6 +106,7 @@ __global__ void __launch_bounds__(256) k_seg_bounds(const unsigned* __restrict__
                                                     unsigned* __restrict__ seg_beg, unsigned* __restrict__ seg_end) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const unsigned f = flag[i], k = sid[i];
+    if (!BONSAI_IN_RANGE(k + f - 1, n, 0x205) || (f && !BONSAI_IN_RANGE(k, n, 0x206))) continue;
     if (f) {
       seg_beg[k] = (unsigned)i;
       if (i > 0) seg_end[k - 1] = (unsigned)i;
@@ -131,7 +135,7 @@ void make_groups_sys(const unsigned long long* sorted_ph, int n, int level_split
   unsigned* ng = flag;
   k_seg_group_sizes<<<1184, 256, 0, s>>>(seg_beg, seg_end, nseg, n, ncrit, ng);
   exclusive_scan(ng, ng, n, bsum, (unsigned*)&info->ngroups, s);
-  k_group_write<<<1184, 256, 0, s>>>(seg_end, seg_beg, ng, n, ncrit, groups, group_cap, info);
+  k_group_write<<<1184, 256, 0, s>>>(seg_end, seg_beg, ng, n, ncrit, groups, group_cap, info, n);
 }
 
 // state gather: out[k] = in[perm[k]] for positions, velocities and ids
@@ -141,6 +145,7 @@ __global__ void __launch_bounds__(256) k_gather_state(const int* __restrict__ pe
                                                       float4* __restrict__ vel_o, int* __restrict__ id_o) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     const int j = __ldcs(perm + k);
+    if (!BONSAI_IN_RANGE(j, n, 0x207)) continue;
     __stcs(pos_o + k, __ldg(pos + j));
     __stcs(vel_o + k, __ldg(vel + j));
     __stcs(id_o + k, __ldg(id + j));
@@ -149,8 +154,12 @@ __global__ void __launch_bounds__(256) k_gather_state(const int* __restrict__ pe
 
 __global__ void __launch_bounds__(256) k_gather_pos(const int* __restrict__ perm, int n,
                                                     const float4* __restrict__ pos, float4* __restrict__ out) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
-    out[k] = __ldg(pos + __ldcs(perm + k));
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int j = __ldcs(perm + k);
+    if (BONSAI_IN_RANGE(j, n, 0x208)) out[k] = __ldg(pos + j);
+  }
 }
+
+BONSAI_BOUNDS_ACCESSOR(bounds_word_groups)
 
 }  // namespace bonsai

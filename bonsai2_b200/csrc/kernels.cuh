@@ -124,6 +124,21 @@ __global__ void k_scatter_by_id(const int* __restrict__ id, int n, const float4*
 __global__ void k_iota(int* __restrict__ a, int n);
 double fma_probe_tflops(int nsm, cudaStream_t st, float* scratch);
 
+// Bounds-checked builds (-DBONSAI_CHECKS): the violation word (count, first
+// failing site) of each translation unit with guarded accesses; reset clears
+// it.  Zeros in the normal build.
+int bounds_word_sort(unsigned* w, bool reset);
+int bounds_word_tree(unsigned* w, bool reset);
+int bounds_word_multipoles(unsigned* w, bool reset);
+int bounds_word_groups(unsigned* w, bool reset);
+int bounds_word_walk(unsigned* w, bool reset);
+int bounds_word_walk64(unsigned* w, bool reset);
+int bounds_word_move(unsigned* w, bool reset);
+// checked-build self-test (move.cu): one guarded write at the logical end of
+// a buffer that has a spare element, so the access is inside the allocation
+// in every build; returns the violations it recorded (1 in a checked build)
+int bounds_selftest(cudaStream_t s);
+
 // learned.cu
 size_t mlp_train_scratch_floats(int S);
 void mlp_loss_grad(const float* X, const float* y, int S, const float* w, float lo, float hi, float over,

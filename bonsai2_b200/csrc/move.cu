@@ -341,7 +341,10 @@ __global__ void __launch_bounds__(256) k_bts_active_groups(const int2* __restric
     const int2 gd = groups[g];
     bool act = false;
     for (int i = gd.x; i < gd.x + gd.y && !act; i++) act = on_boundary(s1, lev[i], K);
-    if (act) list[atomicAdd(count, 1u)] = g;
+    if (act) {
+      const unsigned slot = atomicAdd(count, 1u);
+      if (BONSAI_IN_RANGE(slot, ng, 0x701)) list[slot] = g;
+    }
   }
 }
 
@@ -367,7 +370,10 @@ __global__ void __launch_bounds__(256) k_gather_u8(const int* __restrict__ perm,
 __global__ void __launch_bounds__(256) k_scatter_u8(const int* __restrict__ id, int n,
                                                     const unsigned char* __restrict__ in,
                                                     unsigned char* __restrict__ out) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) out[id[k]] = in[k];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int d = id[k];
+    if (BONSAI_IN_RANGE(d, n, 0x702)) out[d] = in[k];
+  }
 }
 
 void launch_bts_open_drift(float4* pos, float4* vel, const float4* acc, const unsigned char* lev, int n, float dt,
@@ -518,6 +524,31 @@ double fma_probe_tflops(int nsm, cudaStream_t st, float* scratch) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return best_tf;
+}
+
+// Self-test of the checked build's machinery: index n of a logical length n,
+// in a buffer of n + 1 elements (so the write stays inside the allocation in
+// every build).  A checked build skips the write and counts it.
+__global__ void k_bounds_selftest(int* __restrict__ buf, int n) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    if (BONSAI_IN_RANGE(n, n, 0x7FF)) buf[n] = 1;
+  }
+}
+
+BONSAI_BOUNDS_ACCESSOR(bounds_word_move)
+
+int bounds_selftest(cudaStream_t s) {
+  constexpr int n = 32;
+  int* buf = nullptr;
+  if (cudaMalloc(&buf, (n + 1) * sizeof(int)) != cudaSuccess) return -1;
+  unsigned before[2], after[2];
+  int r = -1;
+  if (cudaStreamSynchronize(s) == cudaSuccess && bounds_word_move(before, false) == 0) {
+    k_bounds_selftest<<<1, 32, 0, s>>>(buf, n);
+    if (cudaStreamSynchronize(s) == cudaSuccess && bounds_word_move(after, false) == 0) r = (int)(after[0] - before[0]);
+  }
+  cudaFree(buf);
+  return r;
 }
 
 }  // namespace bonsai

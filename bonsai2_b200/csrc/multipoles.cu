@@ -87,7 +87,8 @@ __device__ __forceinline__ bool arrive_last(int* p, int nch) {
 
 // Combines parents bottom-up while this thread is the last child to arrive.
 template <bool DS>
-__device__ void climb(int c, const uint4* __restrict__ cell_data, const int* __restrict__ cell_parent,
+__device__ void climb(int c, [[maybe_unused]] int ncells, const uint4* __restrict__ cell_data,
+                      const int* __restrict__ cell_parent,
                       float inv_theta, MpRec* __restrict__ rec, typename BoxOf<DS>::T* __restrict__ box,
                       float4* __restrict__ cell_open, float4* __restrict__ cell_q0, float4* __restrict__ cell_q1,
                       float2* __restrict__ cell_ls, int* __restrict__ mp_count, float4* __restrict__ cell_lo) {
@@ -95,8 +96,10 @@ __device__ void climb(int c, const uint4* __restrict__ cell_data, const int* __r
   while (true) {
     const int p = cell_parent[c];
     if (p < 0) break;
+    if (!BONSAI_IN_RANGE(p, ncells, 0x303)) break;
     const unsigned y = cell_data[p].y;
     const int first = (int)(y & 0x1FFFFFFFu), nch = (int)(y >> 29) + 1;
+    if (!BONSAI_IN_RANGE(first + nch - 1, ncells, 0x304) || !BONSAI_IN_RANGE(c - first, nch, 0x305)) break;
     if (!arrive_last(mp_count + p, nch)) break;
     double M = 0, X = 0, Y = 0, Z = 0;
     B bmn[3] = {(B)3.0e38, (B)3.0e38, (B)3.0e38}, bmx[3] = {(B)-3.0e38, (B)-3.0e38, (B)-3.0e38};
@@ -153,10 +156,13 @@ __global__ void __launch_bounds__(256) k_multipoles(const int* __restrict__ leaf
   typedef typename BoxOf<DS>::T B;
   const int nleaves = info->nleaves;
   if (info->ncells > cell_cap) return;
+  [[maybe_unused]] const int ncells = info->ncells, npart = info->npart;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nleaves; t += gridDim.x * blockDim.x) {
     const int c = leaf_list[t];
+    if (!BONSAI_IN_RANGE(c, ncells, 0x301)) continue;
     const uint4 cd = cell_data[c];
     const int b = (int)cd.z, e = (int)cd.w;
+    if (!BONSAI_IN_RANGE(e - 1, npart, 0x302) || !BONSAI_IN_RANGE(b, e, 0x306)) continue;
     MpRec r;
     double m = 0, sx = 0, sy = 0, sz = 0;
     B mn[3] = {(B)3.0e38, (B)3.0e38, (B)3.0e38}, mx[3] = {(B)-3.0e38, (B)-3.0e38, (B)-3.0e38};
@@ -194,7 +200,7 @@ __global__ void __launch_bounds__(256) k_multipoles(const int* __restrict__ leaf
     r.m = m;
     r.ixx = q[0]; r.iyy = q[1]; r.izz = q[2]; r.ixy = q[3]; r.ixz = q[4]; r.iyz = q[5];
     store_cell<DS>(c, r, mn, mx, inv_theta, rec, box, cell_open, cell_q0, cell_q1, cell_ls, cell_lo);
-    climb<DS>(c, cell_data, cell_parent, inv_theta, rec, box, cell_open, cell_q0, cell_q1, cell_ls, mp_count, cell_lo);
+    climb<DS>(c, ncells, cell_data, cell_parent, inv_theta, rec, box, cell_open, cell_q0, cell_q1, cell_ls, mp_count, cell_lo);
   }
 }
 
@@ -230,5 +236,7 @@ __global__ void k_multipoles_ref_layout(const TreeInfo* __restrict__ info, const
     quad1[c] = make_float2((float)(r.ixz * im), (float)(r.iyz * im));
   }
 }
+
+BONSAI_BOUNDS_ACCESSOR(bounds_word_multipoles)
 
 }  // namespace bonsai

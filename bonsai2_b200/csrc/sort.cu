@@ -253,7 +253,8 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_sort_onesweep(
   for (int j = threadIdx.x; j < tile_n; j += kSortThreads) {
     const unsigned long long kk = stage[j];
     const unsigned dd = sdig[j];
-    keys_out[dstart[dd] + (unsigned)j - tile_off[dd]] = kk;
+    const unsigned dst = dstart[dd] + (unsigned)j - tile_off[dd];
+    if (BONSAI_IN_RANGE(dst, n, 0x601)) keys_out[dst] = kk;
   }
   __syncthreads();
   unsigned* stage32 = reinterpret_cast<unsigned*>(stage);
@@ -265,7 +266,8 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_sort_onesweep(
   __syncthreads();
   for (int j = threadIdx.x; j < tile_n; j += kSortThreads) {
     const unsigned dd = sdig[j];
-    vals_out[dstart[dd] + (unsigned)j - tile_off[dd]] = (int)stage32[j];
+    const unsigned dst = dstart[dd] + (unsigned)j - tile_off[dd];
+    if (BONSAI_IN_RANGE(dst, n, 0x602)) vals_out[dst] = (int)stage32[j];
   }
 }
 
@@ -356,5 +358,7 @@ int sort_timeout_selftest(cudaStream_t s) {
   cudaFree(ka); cudaFree(kb); cudaFree(va); cudaFree(err); cudaFree(status); cudaFree(counter); cudaFree(gbase);
   return e == cudaSuccess ? result : -(int)e - 1000;
 }
+
+BONSAI_BOUNDS_ACCESSOR(bounds_word_sort)
 
 }  // namespace bonsai

@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_chains(const unsigned lon
 // One block: exclusive scan of each histogram row across tiles, rows chained
 // so that offsets are global (cells level-major; leaves ordered likewise).
 __global__ void __launch_bounds__(1024) k_tree_scan(unsigned* __restrict__ hist, int nb, int cell_cap,
-                                                    int leaf_cap, TreeInfo* __restrict__ info) {
+                                                    int leaf_cap, int n, TreeInfo* __restrict__ info) {
   __shared__ unsigned sh[32];
   __shared__ unsigned carry;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -216,6 +216,7 @@ __global__ void __launch_bounds__(1024) k_tree_scan(unsigned* __restrict__ hist,
     info->nleaves = (int)tot_leaves;
     info->nnodes = (int)(tot_cells - tot_leaves);
     info->nlevels = nlevels;
+    info->npart = n;
     if ((int)tot_cells > cell_cap || (int)tot_leaves > leaf_cap) set_status(&info->status, kStatusCellCapacity);
   }
 }
@@ -252,6 +253,7 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_cells(
   __shared__ uint16_t lpre[kNL][kTreeThreads];
   __shared__ unsigned boff[2][kNL];
   if (info->ncells > cell_cap || info->nleaves > cell_cap) return;
+  [[maybe_unused]] const int ncells = info->ncells, nleaves = info->nleaves;
   if (nsys > 1 && blockIdx.x == 0 && threadIdx.x == 0) root_beg[nsys] = info->level_end[1];
   const int t0 = blockIdx.x * kTreeTile;
   for (int j = threadIdx.x; j < kTreeTile + 2 * kHalo; j += blockDim.x) {
@@ -313,12 +315,13 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_cells(
       const int leaf_idx = (int)(boff[1][b] + lpre[b][threadIdx.x]) + lk;
       int lc = 0;
       for (int q = 0; q < k; q++) lc += (ca[q] && ca[q] <= b && b <= cb[q]);
-      leaf_list[leaf_idx] = (int)(boff[0][b] + cpre[b][threadIdx.x]) + lc;
+      if (BONSAI_IN_RANGE(leaf_idx, nleaves, 0x101)) leaf_list[leaf_idx] = (int)(boff[0][b] + cpre[b][threadIdx.x]) + lc;
     }
     for (int L = a; L <= b; L++) {
       int lc = 0;
       for (int q = 0; q < k; q++) lc += (ca[q] && ca[q] <= L && L <= cb[q]);
       const int cidx = (int)(boff[0][L] + cpre[L][threadIdx.x]) + lc;
+      if (!BONSAI_IN_RANGE(cidx, ncells, 0x102)) continue;
       const bool leaf = (L == b);
       const int sh = 63 - 3 * L;
       const unsigned long long pre = ki >> sh;
@@ -368,14 +371,17 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_cells(
         for (int o = 1; o <= 8; o++) {
           const int bnd = (o == 8) ? pend : bl[o];
           if (bnd > lo) {
-            cell_data[first + nch].x = (unsigned)cidx | ((unsigned)(L + 1) << 27);
-            cell_parent[first + nch] = cidx;
+            if (BONSAI_IN_RANGE(first + nch, ncells, 0x103)) {
+              cell_data[first + nch].x = (unsigned)cidx | ((unsigned)(L + 1) << 27);
+              cell_parent[first + nch] = cidx;
+            }
             nch++;
           }
           lo = bnd;
         }
         ywd = (unsigned)first | ((unsigned)(nch - 1) << 29);
       }
+      if (!BONSAI_IN_RANGE(pend - 1, n, 0x104) || !BONSAI_IN_RANGE(i, pend, 0x105)) pend = min(max(pend, i + 1), n);
       cd->y = ywd;
       cd->z = (unsigned)i;
       cd->w = (unsigned)pend;
@@ -391,9 +397,11 @@ void build_tree(const unsigned long long* sorted_keys, int n, int nleaf, int cel
   const int nb = tree_tiles(n);
   k_tree_chains<<<nb, kTreeThreads, 0, s>>>(sorted_keys, n, nleaf, dlev, chain, hist, nb, &info->status, sys_off,
                                             nsys);
-  k_tree_scan<<<1, 1024, 0, s>>>(hist, nb, cell_cap, leaf_cap, info);
+  k_tree_scan<<<1, 1024, 0, s>>>(hist, nb, cell_cap, leaf_cap, n, info);
   k_tree_cells<<<nb, kTreeThreads, 0, s>>>(sorted_keys, dlev, chain, hist, n, nleaf, nb, cell_cap, info, cell_data,
                                            cell_parent, leaf_list, mp_count, sys_off, nsys, root_beg);
 }
+
+BONSAI_BOUNDS_ACCESSOR(bounds_word_tree)
 
 }  // namespace bonsai

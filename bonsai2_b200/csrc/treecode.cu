@@ -1281,7 +1281,45 @@ int bonsai_synchronize(bonsai_handle hh) {
   BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st_d2h));
   const int c = last_cuda();
   if (c) return c;
-  return h->read_status(true);
+  int st = h->read_status(true);
+#ifdef BONSAI_CHECKS
+  unsigned count = 0, site = 0;
+  if (st >= 0 && bonsai_bounds_check(&count, &site, 0) == 1 && count > 0) st |= BONSAI_STATUS_BOUNDS;
+#endif
+  return st;
+}
+
+int bonsai_bounds_check(unsigned* count, unsigned* first_site, int reset) {
+  unsigned tot = 0, first = 0;
+#ifdef BONSAI_CHECKS
+  BONSAI_CUDA_TRY(cudaDeviceSynchronize());
+  int (*const words[])(unsigned*, bool) = {bounds_word_sort,   bounds_word_tree,   bounds_word_multipoles,
+                                           bounds_word_groups, bounds_word_walk,   bounds_word_walk64,
+                                           bounds_word_move};
+  for (auto f : words) {
+    unsigned w[2] = {0u, 0u};
+    if (f(w, reset != 0) != 0) return -(int)cudaErrorUnknown - 1000;
+    if (w[0] && !tot) first = w[1];
+    tot += w[0];
+  }
+  if (count) *count = tot;
+  if (first_site) *first_site = first;
+  return 1;
+#else
+  (void)reset;
+  if (count) *count = tot;
+  if (first_site) *first_site = first;
+  return 0;
+#endif
+}
+
+int bonsai_bounds_selftest(int device) {
+  BONSAI_CUDA_TRY(cudaSetDevice(device));
+  cudaStream_t st;
+  BONSAI_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  const int r = bounds_selftest(st);
+  cudaStreamDestroy(st);
+  return r;
 }
 
 int bonsai_copy_streams(bonsai_handle hh, void** h2d, void** d2h) {
@@ -1318,6 +1356,7 @@ const char* bonsai_error_string(int code) {
     if (code & BONSAI_STATUS_DEPTH) return "tree deeper than 21 levels (fat leaf kept)";
     if (code & BONSAI_STATUS_BAD_PARAM) return "bad parameter";
     if (code & BONSAI_STATUS_SORT_TIMEOUT) return "radix sort look-back wait timed out";
+    if (code & BONSAI_STATUS_BOUNDS) return "index out of range (bounds-checked build; access skipped)";
   }
   return "unknown";
 }

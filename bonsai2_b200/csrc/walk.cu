@@ -195,6 +195,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
   // group_list (optional): walk only the listed groups (block time steps)
   const int ngroups = group_list ? (int)*group_list_n : info->ngroups;
   int l1b = info->level_beg[1], l1e = info->level_end[1];
+  [[maybe_unused]] const int ncells = info->ncells, npart = info->npart, ngroups_all = info->ngroups;
   const unsigned lt = lanemask_lt();
   unsigned long long sum_app = 0, sum_dir = 0;
   unsigned max_app = 0, max_dir = 0;
@@ -205,8 +206,12 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
     g = __shfl_sync(kFull, g, 0);
     if (g >= ngroups) break;
     if (group_list) g = __ldg(group_list + g);
+    if (!BONSAI_IN_RANGE(g, ngroups_all, 0x401)) continue;
     const int2 gd = groups[g];
     const int pbeg = gd.x, np = gd.y;
+    if (!BONSAI_IN_RANGE(np - 1, NI * STRIDE, 0x402) || !BONSAI_IN_RANGE(pbeg + np - 1, npart, 0x403) ||
+        !BONSAI_IN_RANGE(pbeg, npart, 0x407))
+      continue;
     const float inv_theta_g = PERGROUP ? group_inv_theta[g] : 0.0f;
     if (ENS) {
       const int sy = sys_of(sys_off, nsys, pbeg);
@@ -266,8 +271,9 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
     while (ncur > 0 && !overflow) {
       for (int blk = 0; blk < ncur; blk += 32) {
         const int li = blk + lane;
-        const bool valid = li < ncur;
-        const int cell = valid ? lists[cb + li] : 0;
+        const bool inlist = li < ncur;
+        const int cell = inlist ? lists[cb + li] : 0;
+        const bool valid = inlist && BONSAI_IN_RANGE(cell, ncells, 0x404);
         uint4 cd = make_uint4(0u, 0xFFFFFFFFu, 0u, 0u);
         float4 co = make_float4(0.f, 0.f, 0.f, 0.f);
         if (valid) {
@@ -299,7 +305,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
           const int src = find_src(incl, s);
           const int f = __shfl_sync(kFull, first, src);
           const int e = __shfl_sync(kFull, incl - nch, src);
-          if (s < tot) lists[(cb ^ half_cap) + nnext + s] = f + (s - e);
+          if (s < tot) lists[(cb ^ half_cap) + nnext + s] = BONSAI_IN_RANGE(f + (s - e), ncells, 0x405) ? f + (s - e) : 0;
         }
         nnext += tot;
 
@@ -344,7 +350,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
           const int e = __shfl_sync(kFull, incl2 - nb, src);
           const int cnt = min(32, tot2 - base);
           if (lane < cnt) {
-            const int jj = f + (s - e);
+            const int jj = BONSAI_IN_RANGE(f + (s - e), npart, 0x406) ? f + (s - e) : 0;
             float4 pj = __ldg(jpos + jj);
             if (DS) {
               const float4 lo = __ldg(jpos_lo + jj);
@@ -514,5 +520,7 @@ void launch_walk(int variant, int nblocks, const int2* groups, const TreeInfo* i
 #undef BONSAI_WALK
 #undef BONSAI_WALK_ARGS
 }
+
+BONSAI_BOUNDS_ACCESSOR(bounds_word_walk)
 
 }  // namespace bonsai

@@ -68,6 +68,7 @@ __global__ void __launch_bounds__(kW64Threads) k_walk64(
   const int half_cap = ring_cap >> 1;
   const int ngroups = info->ngroups;
   const int l1b = info->level_beg[1], l1e = info->level_end[1];
+  [[maybe_unused]] const int ncells = info->ncells, npart = info->npart;
   unsigned long long sum_app = 0, sum_dir = 0;
   unsigned max_app = 0, max_dir = 0;
   while (true) {
@@ -77,6 +78,9 @@ __global__ void __launch_bounds__(kW64Threads) k_walk64(
     if (g >= ngroups) break;
     const int2 gd = groups[g];
     const int pbeg = gd.x, np = gd.y;
+    if (!BONSAI_IN_RANGE(np - 1, kW64NI * 32, 0x501) || !BONSAI_IN_RANGE(pbeg + np - 1, npart, 0x502) ||
+        !BONSAI_IN_RANGE(pbeg, npart, 0x503))
+      continue;
     const float inv_theta_g = PERGROUP ? group_inv_theta[g] : 0.0f;
     float3 R = make_float3(0.f, 0.f, 0.f);
     if (DS) {
@@ -118,8 +122,9 @@ __global__ void __launch_bounds__(kW64Threads) k_walk64(
     while (ncur > 0 && !overflow) {
       for (int blk = 0; blk < ncur; blk += 32) {
         const int li = blk + lane;
-        const bool valid = li < ncur;
-        const int cell = valid ? lists[cb + li] : 0;
+        const bool inlist = li < ncur;
+        const int cell = inlist ? lists[cb + li] : 0;
+        const bool valid = inlist && BONSAI_IN_RANGE(cell, ncells, 0x504);
         uint4 cd = make_uint4(0u, 0xFFFFFFFFu, 0u, 0u);
         float4 co = make_float4(0.f, 0.f, 0.f, 0.f);
         if (valid) {
@@ -150,7 +155,7 @@ __global__ void __launch_bounds__(kW64Threads) k_walk64(
           const int src = find_src(incl, s);
           const int f = __shfl_sync(kFull, first, src);
           const int e = __shfl_sync(kFull, incl - nch, src);
-          if (s < tot) lists[(cb ^ half_cap) + nnext + s] = f + (s - e);
+          if (s < tot) lists[(cb ^ half_cap) + nnext + s] = BONSAI_IN_RANGE(f + (s - e), ncells, 0x505) ? f + (s - e) : 0;
         }
         nnext += tot;
         // accepted cells: quadrupoles in FP64 from the cell records
@@ -169,7 +174,8 @@ __global__ void __launch_bounds__(kW64Threads) k_walk64(
         while (leaf_mask) {
           const int b = __ffs(leaf_mask) - 1;
           leaf_mask &= leaf_mask - 1;
-          const int pb = (int)__shfl_sync(kFull, cd.z, b), pe = (int)__shfl_sync(kFull, cd.w, b);
+          int pb = (int)__shfl_sync(kFull, cd.z, b), pe = (int)__shfl_sync(kFull, cd.w, b);
+          if (!BONSAI_IN_RANGE(pe - 1, npart, 0x506) || !BONSAI_IN_RANGE(pb, pe, 0x507)) pb = pe = 0;
           n_dir += (unsigned)(pe - pb);
           for (int j = pb; j < pe; j++) {
             const float4 q = __ldg(jpos + j);
@@ -236,5 +242,7 @@ void launch_walk64(int nblocks, const int2* groups, const TreeInfo* info, const 
 void launch_scatter_d4(const int* id, int n, const double4* in, double4* out, int nblocks, cudaStream_t s) {
   k_scatter_d4<<<nblocks, 256, 0, s>>>(id, n, in, out);
 }
+
+BONSAI_BOUNDS_ACCESSOR(bounds_word_walk64)
 
 }  // namespace bonsai

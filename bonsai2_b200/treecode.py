@@ -50,6 +50,18 @@ def default_params() -> bonsai_params:
     return p
 
 
+def bounds_check(reset: bool = False) -> dict:
+    """Violations recorded by a bounds-checked build of the library (loaded
+    through BONSAI_B200_LIB = _lib.CHECKED_LIB_PATH): {"checked", "count",
+    "first_site"}; checked is False for the normal build."""
+    count = ctypes.c_uint(0)
+    site = ctypes.c_uint(0)
+    rc = load().bonsai_bounds_check(ctypes.byref(count), ctypes.byref(site), 1 if reset else 0)
+    if rc < 0:
+        raise BonsaiError(rc, "bonsai_bounds_check")
+    return {"checked": rc == 1, "count": int(count.value), "first_site": int(site.value)}
+
+
 def plummer(n: int, seed: int = 19810614):
     """Plummer sphere (the reference's plummer.h algorithm), float4 pos/vel."""
     pos = np.empty((n, 4), np.float32)

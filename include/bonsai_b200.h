@@ -36,6 +36,7 @@ extern "C" {
 #define BONSAI_STATUS_GROUP_CAPACITY 16
 #define BONSAI_STATUS_BAD_PARAM 32
 #define BONSAI_STATUS_SORT_TIMEOUT 64  /* a radix-sort look-back wait hit its bound: results invalid */
+#define BONSAI_STATUS_BOUNDS 128       /* bounds-checked build only: a guarded index was out of range (access skipped) */
 
 /* API errors */
 #define BONSAI_ERR_HANDLE (-1)
@@ -143,6 +144,20 @@ int bonsai_get_stats(bonsai_handle h, unsigned long long *out4);
  * its bound and report.  Returns the status bits (BONSAI_STATUS_SORT_TIMEOUT
  * expected) after a fraction of a second; the device stays usable. */
 int bonsai_selftest_wait_bound(int device);
+/* Bounds-checked builds (the library compiled with -DBONSAI_CHECKS, e.g.
+ * `python -m bonsai2_b200.build --checks`): every guarded index of the kernels
+ * (cell, leaf, group, particle and scatter indexes) is tested, and an
+ * out-of-range one skips its access and is counted; bonsai_synchronize then
+ * reports BONSAI_STATUS_BOUNDS.  No reference counterpart (its kernels
+ * assert).  Waits for the device, writes the number of violations since the
+ * last reset and the first failing site ((kernel file << 8) | site), and
+ * clears them when reset != 0.  Returns 1 in a checked build, 0 in the normal
+ * build (count 0, no device access), < 0 on a CUDA error. */
+int bonsai_bounds_check(unsigned *count, unsigned *first_site, int reset);
+/* Runs one guarded access at the logical end of a buffer with a spare element
+ * (inside the allocation in every build) and returns the violations it
+ * recorded: 1 in a checked build, 0 in the normal build. */
+int bonsai_bounds_selftest(int device);
 /* measured FP32 FMA throughput of the device (TFLOP/s; the faster of scalar
  * FFMA and packed FFMA2 chains): the walk's roofline */
 int bonsai_fp32_peak(int device, double *tflops);

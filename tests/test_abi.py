@@ -30,6 +30,21 @@ def test_library_exports_every_declared_symbol(lib):
     assert set(names) == set(_lib.SIGNATURES)
 
 
+def test_checked_library_exports_every_declared_symbol():
+    from bonsai2_b200 import _lib
+    assert os.path.exists(_lib.CHECKED_LIB_PATH), "python -m bonsai2_b200.build --checks"
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.CHECKED_LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(l.split()[-1] for l in out.splitlines() if l.strip())
+    assert not [s for s in declared_symbols() if s not in exported]
+
+
+def test_bounds_check_of_normal_build_needs_no_device(lib):
+    count, site = ctypes.c_uint(7), ctypes.c_uint(7)
+    assert lib.bonsai_bounds_check(ctypes.byref(count), ctypes.byref(site), 1) == 0
+    assert count.value == 0 and site.value == 0
+    assert lib.bonsai_error_string(128)
+
+
 def test_library_is_built_for_sm100a(lib):
     from bonsai2_b200 import _lib
     out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", _lib.LIB_PATH],
