@@ -21,6 +21,10 @@ state, 1.3 GB, is larger than the 126 MB L2, so no flush is needed).
             (treecode.cu:149-158) / walk time from CUDA events recorded on the
             handle's stream inside the timed region; peak = this GPU's FP32
             FMA throughput measured by bonsai_fp32_peak
+  hbm_roofline: the other stages (build, multipoles, groups, gathers,
+            move) against HBM bandwidth: algorithmic bytes per particle and
+            per cell / their event time, beside the reference's IOCOUNT
+            build accounting (32 B per particle per level)
   cpu_baseline / --impl reference: the CPU restatement of the reference
             algorithm (oracle/, OpenMP over the host cores), on a bounded
             sample: full-N build, multipoles and groups, the walk of a sample
@@ -51,7 +55,7 @@ UNIT = "Mparticles/s"
 # the walk's DRAM traffic (read + write) per launch from one ncu capture of the
 # same workload at N = 2^22, theta 0.6 (profiles/walk_k_walk_plummer_4M.md);
 # scaled by the particle count for other N (the walk's misses grow with N)
-WALK_DRAM_BYTES_2P22 = 264.6e6 + 87.8e6
+WALK_DRAM_BYTES_2P22 = 224.8e6 + 69.5e6
 
 
 def parse():
@@ -88,6 +92,41 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-group-fraction", type=float, default=1.0 / 512)
     return ap.parse_args()
+
+
+# Algorithmic HBM bytes of the non-walk stages (keys, the PH permutation counted
+# once, state gather, tree, multipoles, groups, kick-drift-kick), per particle
+# and per cell; the reference's own build accounting (IOCOUNT,
+# treebuild/treebuild.cu:646-650) is 32 B per particle per level.
+HBM_BYTES_PER_PARTICLE = {"keys": 28, "sort": 24, "gather_pos_vel": 64, "tree": 8, "multipoles": 16, "groups": 8,
+                          "kdk": 80}
+HBM_BYTES_PER_CELL = {"tree": 16, "multipoles": 72}
+HBM_BYTES_PER_GROUP = 8
+HBM_FALLBACK_GBS = 6650.0
+
+
+def hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured copy bandwidth)"
+    except (OSError, KeyError, ValueError):
+        return HBM_FALLBACK_GBS, "fallback 6.65 TB/s (earlier copy measurement on this pool)"
+
+
+def hbm_roofline(n, info, stage_ms):
+    """The non-walk stages of one step against HBM bandwidth."""
+    per_step = (n * sum(HBM_BYTES_PER_PARTICLE.values()) + info["ncells"] * sum(HBM_BYTES_PER_CELL.values())
+                + HBM_BYTES_PER_GROUP * info["ngroups"])
+    peak, src = hbm_peak()
+    achieved = per_step / (stage_ms * 1e-3) / 1e9
+    ref_bytes = 32.0 * n * info["nlevels"]
+    return {"bound": "hbm", "stages": "box+keys+sorts+tree+multipoles+groups+gathers+move+energies",
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": src,
+            "stage_ms": stage_ms, "algorithmic_bytes_per_step": per_step,
+            "bytes_per_particle": HBM_BYTES_PER_PARTICLE, "bytes_per_cell": HBM_BYTES_PER_CELL,
+            "cells": info["ncells"], "groups": info["ngroups"], "levels": info["nlevels"],
+            "reference_build_bytes": ref_bytes, "reference_build_gbs": ref_bytes / (stage_ms * 1e-3) / 1e9,
+            "reference_build_accounting": "IOCOUNT: 32 B per particle per level (treebuild/treebuild.cu:646-650)"}
 
 
 def workload(a):
@@ -305,6 +344,7 @@ def run_ours(a):
     ph = phase[:4 * a.steps].reshape(a.steps, 4)
     walk_ms = float(ph[:, 1].mean())
     E1 = t.computeEnergies()
+    hbm = hbm_roofline(n, t.tree_info(), float(ph[:, 0].mean()) + float(ph[:, 2].mean()))
     st = np.zeros(4, np.uint64)
     L.bonsai_get_stats(t.handle, _p(st))
     n_app, n_dir = float(st[0]), float(st[1])
@@ -387,6 +427,7 @@ def run_ours(a):
                                            "theta 0.6, scaled by N",
                          "kernel": "k_walk", "peak_source": "measured FP32 FMA probe (bonsai_fp32_peak)",
                          "flops_per_launch": flops},
+            "hbm_roofline": hbm,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * nbytes,
                     "d2h_bytes_per_step": nbytes, "ms_per_step": e2e, "steps": a.e2e_steps,

@@ -10,7 +10,7 @@ constexpr int kMlpFeatures = 16;
 constexpr int kMlpHidden = 64;
 constexpr int kMlpWeights = kMlpHidden * kMlpFeatures + kMlpHidden + kMlpHidden * kMlpHidden + kMlpHidden + kMlpHidden + 1;
 #ifndef BONSAI_WALK_MINB
-#define BONSAI_WALK_MINB 3
+#define BONSAI_WALK_MINB 2
 #endif
 constexpr int kWalkMinBlocks = BONSAI_WALK_MINB;
 

@@ -47,7 +47,7 @@ constexpr int kWalkWarps = kWalkThreads / 32;
 #define BONSAI_WALK_SPLIT 1
 #endif
 #ifndef BONSAI_WALK_UNROLL
-#define BONSAI_WALK_UNROLL 2
+#define BONSAI_WALK_UNROLL 4
 #endif
 #define BONSAI_DO_PRAGMA(x) _Pragma(#x)
 #define BONSAI_UNROLL_N(n) BONSAI_DO_PRAGMA(unroll n)
