@@ -17,8 +17,9 @@
 // B200 design:
 //   * explicit __shfl_sync / __ballot_sync / redux.sync cooperation, no
 //     implicit warp-synchronous shared memory;
-//   * range expansion (children, leaf particles) with a shuffle binary search
-//     over the warp's inclusive scan: 32 outputs per step;
+//   * range expansion from the warp's inclusive scan: opened nodes write
+//     their own children at their offsets; leaf particles are expanded 32 at
+//     a time by a shuffle binary search over the scan;
 //   * the level lists live in a per-warp pair of buffers in global memory
 //     (current level / next level, swapped per level; L1/L2 resident),
 //     bounded; overflow sets a status bit, never traps;
@@ -28,7 +29,8 @@
 //   * the quadrupole kernel uses mass-weighted, pre-scaled moments
 //     (34 FP32 operations + 1 MUFU per interaction; the reference's
 //     formulation, counted as 64 flops by treecode.cu:149-158, is the same
-//     algebra).
+//     algebra), evaluated as packed FFMA2/FMUL2/FADD2 over pairs of a lane's
+//     particles.
 #include <algorithm>
 #include <type_traits>
 
@@ -54,6 +56,11 @@ constexpr int kWalkWarps = kWalkThreads / 32;
 
 #ifndef BONSAI_WALK_PACKED
 #define BONSAI_WALK_PACKED 1
+#endif
+// children of opened nodes written by their parent's lane (1) or expanded
+// 32 at a time by a shuffle search over the warp's scan (0)
+#ifndef BONSAI_WALK_CHILD_LOOP
+#define BONSAI_WALK_CHILD_LOOP 1
 #endif
 
 struct IPart {
@@ -300,6 +307,15 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
         const int tot = __shfl_sync(kFull, incl, 31);
         if (nnext + tot > half_cap) { overflow = true; break; }
         const int first = (int)(cd.y & 0x1FFFFFFFu);
+#if BONSAI_WALK_CHILD_LOOP
+        // each opened node writes its own (at most 8, contiguous) children at
+        // its scan offset: the same entries in the same order as the shuffle
+        // expansion, without the dependent shuffle search on the critical path
+        {
+          int* dst = lists + (cb ^ half_cap) + nnext + (incl - nch);
+          for (int k = 0; k < nch; k++) dst[k] = BONSAI_IN_RANGE(first + k, ncells, 0x405) ? first + k : 0;
+        }
+#else
         for (int base = 0; base < tot; base += 32) {
           const int s = base + lane;
           const int src = find_src(incl, s);
@@ -307,6 +323,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
           const int e = __shfl_sync(kFull, incl - nch, src);
           if (s < tot) lists[(cb ^ half_cap) + nnext + s] = BONSAI_IN_RANGE(f + (s - e), ncells, 0x405) ? f + (s - e) : 0;
         }
+#endif
         nnext += tot;
 
         // (2) accepted cells -> approximate list (staged by value)
