@@ -55,7 +55,7 @@ UNIT = "Mparticles/s"
 # the walk's DRAM traffic (read + write) per launch from one ncu capture of the
 # same workload at N = 2^22, theta 0.6 (profiles/walk_k_walk_plummer_4M.md);
 # scaled by the particle count for other N (the walk's misses grow with N)
-WALK_DRAM_BYTES_2P22 = 224.8e6 + 69.5e6
+WALK_DRAM_BYTES_2P22 = 225.7e6 + 71.6e6
 
 
 def parse():
