@@ -253,6 +253,42 @@ def cpu_reference_step(O, pos, vel, a, rng):
     return total, desc
 
 
+def reference_gpu_make_groups(O, pos, a, reps=10):
+    """The reference's own GPU group formation (code/makeGroups.cu: PH keys,
+    Thrust sort_by_key, segment scans, groups), the one hot-path CUDA file that
+    builds for sm_100a unmodified (oracle/build_ref.sh -> oracle/_ref/ref_groups),
+    timed with CUDA events on the same input; its domain box comes from the
+    oracle (buildTree.cu does not build for sm_100)."""
+    import tempfile
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_groups")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/ref_groups not built (oracle/build_ref.sh needs the reference tree)"}
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return {"unavailable": "no GPU"}
+    except ImportError:
+        return {"unavailable": "no torch to probe for a GPU"}
+    box, _ = O.bbox(pos)
+    n = pos.shape[0]
+    with tempfile.TemporaryDirectory() as dd:
+        inp = os.path.join(dd, "in.f32")
+        np.ascontiguousarray(pos, np.float32).tofile(inp)
+        args = [exe, inp, str(n)] + ["%.9g" % float(b) for b in box] + [str(a.level_split), str(a.ncrit), str(reps)]
+        r = subprocess.run(args, capture_output=True, text=True)
+    lines = [l for l in r.stdout.splitlines() if l.startswith("REFGROUPS ")]
+    if r.returncode != 0 or not lines:
+        return {"unavailable": "ref_groups exited %d" % r.returncode}
+    info = json.loads(lines[-1][len("REFGROUPS "):])
+    # best of the calls: the reference allocates its temporaries inside every
+    # call, and those host-side allocations vary from call to call
+    return {"value": n / info["ms_min"] / 1e3, "unit": "Mparticles/s", "ms": info["ms_min"],
+            "ms_median": info["ms_median"], "reps": info["reps"], "groups": info["groups"], "n": n,
+            "what": "code/makeGroups.cu unmodified for sm_100a (PH keys, Thrust sort_by_key, segment scans, "
+                    "groups; its own temporary allocations included), levelSplit %d, nCrit %d"
+                    % (a.level_split, a.ncrit)}
+
+
 def run_reference(a):
     d = Dist("gloo")
     if d.rank != 0:
@@ -261,6 +297,9 @@ def run_reference(a):
     from oracle import oracle as O
     O.build()
     pos, vel = O.plummer_float4(a.n, a.seed)
+    # the reference's GPU kernels first, before the OpenMP work (whose spinning
+    # threads would slow the reference's host-side allocations)
+    ref_gpu = reference_gpu_make_groups(O, pos, a)
     rng = np.random.default_rng(1)
     times = []
     desc = ""
@@ -277,7 +316,8 @@ def run_reference(a):
             "config": {"workload": workload(a), "n": a.n}, "impl": "reference",
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": "per step: " + desc},
-            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_gpu_make_groups": ref_gpu}
     print(json.dumps(line), flush=True)
     d.close()
 
@@ -400,6 +440,7 @@ def run_ours(a):
     batching = batching_form(B, L, a, d.local) if (solo and a.batch_systems > 0) else None
     tuned = autotuned_headline(B, L, pos, vel, a, d.local) if (solo and a.autotune) else None
     octree = octree_build_form(B, L, a, d.local) if (solo and a.octree_n > 0) else None
+    grouping = group_formation_form(B, L, pos, vel, a, d.local) if solo else None
     blocks = block_steps_form(B, L, pos, vel, a, d.local) if (solo and a.block_levels >= 0) else None
     precision = precision_form(B, L, a, d.local) if (solo and a.precision_n > 0) else None
     field = learned_field_form(B, L, a, d.local) if (solo and a.field_n > 0) else None
@@ -450,6 +491,7 @@ def run_ours(a):
             "batching": batching,
             "autotuned_headline": tuned,
             "octree_build": octree,
+            "group_formation": grouping,
             "block_time_steps": blocks,
             "precision_form": precision,
             "learned_form_clustered_field": field,
@@ -770,6 +812,36 @@ def octree_build_form(B, L, a, device):
             "shape": {"nodes": info["nnodes"], "leaves": info["nleaves"], "cells": info["ncells"],
                       "levels": info["nlevels"]},
             "published_shape": PUBLISHED_OCTREE_SHAPE}
+
+
+def group_formation_form(B, L, pos, vel, a, device):
+    """Group formation alone on the headline system (PH-key sort, segments,
+    groups, state gather into PH order: bonsai_make_groups after a build),
+    timed with CUDA events over 5 calls; the reference arm times the
+    reference's own makeGroups (code/makeGroups.cu, which also computes the PH
+    keys) on the same input."""
+    import torch
+    from bonsai2_b200.treecode import _p
+    n = pos.shape[0]
+    t = B.Treecode(eps=a.eps, theta=a.theta, ncrit=a.ncrit, nleaf=a.nleaf, level_split=a.level_split, device=device)
+    t.alloc(n)
+    L.bonsai_set_particles(t.handle, _p(pos), _p(vel), n)
+    st = torch.cuda.ExternalStream(L.bonsai_stream(t.handle))
+    reps, ms = 5, 0.0
+    for r in range(reps + 1):  # a build before every call (groups reorder the state); the first is a warm-up
+        t.buildTree(a.nleaf)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        t.makeGroups(a.level_split, a.ncrit)
+        e1.record(st)
+        e1.synchronize()
+        if r > 0:
+            ms += e0.elapsed_time(e1) / reps
+    ng = t.tree_info()["ngroups"]
+    t.close()
+    return {"ms": ms, "value": n / (ms * 1e-3) / 1e6, "unit": "Mparticles/s", "groups": ng,
+            "note": "PH keys are computed with the tree keys in the build (k_keys); the reference arm's "
+                    "reference_gpu_make_groups times code/makeGroups.cu on the same input"}
 
 
 def autotuned_headline(B, L, pos, vel, a, device):

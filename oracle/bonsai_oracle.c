@@ -11,12 +11,18 @@
  *   - oracle_plummer is pinned bit-exactly against the reference's own
  *     code/plummer.h, compiled unmodified from the reference tree by
  *     oracle/build_ref.sh (fixture tests/golden/plummer_*.bin).
- *   - keys, sort order, tree topology, groups and walk decisions are restated
- *     from the cited CUDA sources; the reference ships no golden vectors or
- *     known-answer tests for them and its CUDA kernels do not run on the CPU,
- *     so these rows are pinned only by this restatement (parity of those rows
- *     is "restated, not executed").  Forces are additionally judged against
- *     the FP64 direct sum below.
+ *   - oracle_ph_keys, oracle_argsort_u64 and oracle_make_groups are pinned
+ *     bit-exactly against the reference's own GPU group formation
+ *     (code/makeGroups.cu, compiled unmodified for sm_100a by
+ *     oracle/build_ref.sh and run on a B200; fixture
+ *     tests/golden/ref_groups.json: full PH keys, sorted order including a
+ *     2000-way tie, groups, over four inputs).
+ *   - tree keys, tree topology and walk decisions are restated from the cited
+ *     CUDA sources (buildTree.cu and computeForces.cu do not build for
+ *     sm_100, and the reference ships no golden vectors for them); the
+ *     topology is also checked against the tree shape the reference
+ *     publishes for its own N = 20,000,000 build.  Forces are additionally
+ *     judged against the FP64 direct sum below.
  *
  * Build: gcc -O2 -fopenmp -fPIC -shared (no -ffast-math, no -march: the
  * Plummer generator must round exactly as the reference's g++ build does).
