@@ -100,14 +100,22 @@ __global__ void __launch_bounds__(256) k_group_features(const int2* __restrict__
 
 // ---------------------------------------------------------------------------
 // Inference: FP16 weights in shared memory, FP32 accumulation; one warp per
-// group (lane holds hidden units lane and lane+32) writes 1/theta_g.
+// group (lane holds hidden units lane and lane+32) writes 1/theta_g.  W1 and
+// W2 are staged transposed (input-major), so that the 32 lanes of a step read
+// 32 consecutive weights: row-major, lane j's row starts j * 128 bytes apart
+// and every lane of the warp hits the same bank.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_mlp_infer(const float* __restrict__ feat, const __half* __restrict__ wh,
                                                    const TreeInfo* __restrict__ info, float lo, float hi,
                                                    float* __restrict__ group_inv_theta) {
   __shared__ __half sw[kMlpWeights + 1];
   __shared__ float sh[8][kH];
-  for (int t = threadIdx.x; t < kMlpWeights; t += blockDim.x) sw[t] = wh[t];
+  for (int t = threadIdx.x; t < kMlpWeights; t += blockDim.x) {
+    int d = t;
+    if (t < oB1) d = oW1 + (t % kF) * kH + t / kF;                          // W1[j][k] -> [k][j]
+    else if (t >= oW2 && t < oB2) d = oW2 + ((t - oW2) % kH) * kH + (t - oW2) / kH;  // W2[j][i] -> [i][j]
+    sw[d] = wh[t];
+  }
   __syncthreads();
   const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
   const int ng = info->ngroups;
@@ -119,7 +127,7 @@ __global__ void __launch_bounds__(256) k_mlp_infer(const float* __restrict__ fea
       const int j = lane + 32 * u;
       float a = __half2float(sw[oB1 + j]);
 #pragma unroll
-      for (int k = 0; k < kF; k++) a = fmaf(__half2float(sw[oW1 + j * kF + k]), __shfl_sync(kFull, xk, k), a);
+      for (int k = 0; k < kF; k++) a = fmaf(__half2float(sw[oW1 + k * kH + j]), __shfl_sync(kFull, xk, k), a);
       sh[wi][j] = tanhf(a);
     }
     __syncwarp();
@@ -129,7 +137,7 @@ __global__ void __launch_bounds__(256) k_mlp_infer(const float* __restrict__ fea
       const int j = lane + 32 * u;
       float a = __half2float(sw[oB2 + j]);
 #pragma unroll 8
-      for (int i = 0; i < kH; i++) a = fmaf(__half2float(sw[oW2 + j * kH + i]), sh[wi][i], a);
+      for (int i = 0; i < kH; i++) a = fmaf(__half2float(sw[oW2 + i * kH + j]), sh[wi][i], a);
       z = fmaf(__half2float(sw[oW3 + j]), tanhf(a), z);
     }
 #pragma unroll
