@@ -4,8 +4,9 @@
 // The reference (computeCellMultipoles, computeMultipoles.cu:81-190) gives a
 // warp to every cell and rescans all of that cell's particles, O(N * depth)
 // particle reads, with float products summed in double.  Here each leaf is
-// reduced from its own particles (one thread per leaf, FP64, two passes:
-// centre of mass, then central moments), and every node is combined from its
+// reduced from its own particles (one thread per leaf, FP64, one pass: sums
+// about the leaf's first particle, shifted to the centre of mass), and every
+// node is combined from its
 // children with the parallel-axis theorem by the child that finishes last
 // (an arrival counter per cell; no thread waits on another).
 // Each particle is read once.  The quantities match the reference's definitions:
@@ -24,6 +25,12 @@
 #include "kernels.cuh"
 
 namespace bonsai {
+
+// leaf moments in one pass over the particles (1) or two (0: centre of mass,
+// then central moments)
+#ifndef BONSAI_MP_ONE_PASS
+#define BONSAI_MP_ONE_PASS 1
+#endif
 
 template <bool DS>
 struct BoxOf {
@@ -140,8 +147,8 @@ __device__ void climb(int c, [[maybe_unused]] int ncells, const uint4* __restric
   }
 }
 
-// One thread per leaf: two passes over the leaf's particles (COM, then
-// central moments), then the bottom-up climb.  (Half-warp-cooperative leaves
+// One thread per leaf: the leaf's moments (one pass by default), then the
+// bottom-up climb.  (Half-warp-cooperative leaves
 // with shuffle reductions were measured 13x slower on the B200.)
 template <bool DS>
 __global__ void __launch_bounds__(256) k_multipoles(const int* __restrict__ leaf_list, const TreeInfo* __restrict__ info,
@@ -164,8 +171,49 @@ __global__ void __launch_bounds__(256) k_multipoles(const int* __restrict__ leaf
     const int b = (int)cd.z, e = (int)cd.w;
     if (!BONSAI_IN_RANGE(e - 1, npart, 0x302) || !BONSAI_IN_RANGE(b, e, 0x306)) continue;
     MpRec r;
-    double m = 0, sx = 0, sy = 0, sz = 0;
     B mn[3] = {(B)3.0e38, (B)3.0e38, (B)3.0e38}, mx[3] = {(B)-3.0e38, (B)-3.0e38, (B)-3.0e38};
+#if BONSAI_MP_ONE_PASS
+    // one pass: sums about the leaf's first particle x0 (d = x - x0), then the
+    // shift to the centre of mass: COM = x0 + S1/M, I = S2 - S1 S1^T / M; the
+    // cancellation is relative to the leaf's extent, not to |x0|
+    double x0, y0, z0;
+    {
+      const float4 p = __ldg(jpos + b);
+      x0 = p.x; y0 = p.y; z0 = p.z;
+      if (DS) {
+        const float4 l = __ldg(jlo + b);
+        x0 += l.x; y0 += l.y; z0 += l.z;
+      }
+    }
+    double m = 0, s1x = 0, s1y = 0, s1z = 0, q[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = b; i < e; i++) {
+      const float4 p = __ldg(jpos + i);
+      double px = p.x, py = p.y, pz = p.z;
+      if (DS) {
+        const float4 l = __ldg(jlo + i);
+        px += l.x; py += l.y; pz += l.z;
+        mn[0] = (B)fmin((double)mn[0], px); mn[1] = (B)fmin((double)mn[1], py); mn[2] = (B)fmin((double)mn[2], pz);
+        mx[0] = (B)fmax((double)mx[0], px); mx[1] = (B)fmax((double)mx[1], py); mx[2] = (B)fmax((double)mx[2], pz);
+      } else {
+        mn[0] = (B)fminf((float)mn[0], p.x); mn[1] = (B)fminf((float)mn[1], p.y); mn[2] = (B)fminf((float)mn[2], p.z);
+        mx[0] = (B)fmaxf((float)mx[0], p.x); mx[1] = (B)fmaxf((float)mx[1], p.y); mx[2] = (B)fmaxf((float)mx[2], p.z);
+      }
+      const double w = p.w, dx = px - x0, dy = py - y0, dz = pz - z0;
+      m += w;
+      s1x += w * dx; s1y += w * dy; s1z += w * dz;
+      q[0] += w * dx * dx; q[1] += w * dy * dy; q[2] += w * dz * dz;
+      q[3] += w * dx * dy; q[4] += w * dx * dz; q[5] += w * dy * dz;
+    }
+    if (m > 0.0) {
+      const double ux = s1x / m, uy = s1y / m, uz = s1z / m;
+      r.cx = x0 + ux; r.cy = y0 + uy; r.cz = z0 + uz;
+      q[0] -= s1x * ux; q[1] -= s1y * uy; q[2] -= s1z * uz;
+      q[3] -= s1x * uy; q[4] -= s1x * uz; q[5] -= s1y * uz;
+    } else {
+      r.cx = 0.5 * ((double)mn[0] + mx[0]); r.cy = 0.5 * ((double)mn[1] + mx[1]); r.cz = 0.5 * ((double)mn[2] + mx[2]);
+    }
+#else
+    double m = 0, sx = 0, sy = 0, sz = 0;
     for (int i = b; i < e; i++) {
       const float4 p = __ldg(jpos + i);
       double px = p.x, py = p.y, pz = p.z;
@@ -197,6 +245,7 @@ __global__ void __launch_bounds__(256) k_multipoles(const int* __restrict__ leaf
       q[0] += w * dx * dx; q[1] += w * dy * dy; q[2] += w * dz * dz;
       q[3] += w * dx * dy; q[4] += w * dx * dz; q[5] += w * dy * dz;
     }
+#endif
     r.m = m;
     r.ixx = q[0]; r.iyy = q[1]; r.izz = q[2]; r.ixy = q[3]; r.ixz = q[4]; r.iyz = q[5];
     store_cell<DS>(c, r, mn, mx, inv_theta, rec, box, cell_open, cell_q0, cell_q1, cell_ls, cell_lo);
