@@ -57,6 +57,8 @@ SIGNATURES = {
     "bonsai_bounds_check": (I, [P, P, I]),
     "bonsai_bounds_selftest": (I, [I]),
     "bonsai_synchronize": (I, [P]),
+    "bonsai_last_error": (I, [P]),
+    "bonsai_step_graph": (I, [P, I]),
     "bonsai_stream": (P, [P]),
     "bonsai_copy_streams": (I, [P, P, P]),
     "bonsai_error_string": (ctypes.c_char_p, [I]),

@@ -1289,6 +1289,17 @@ int bonsai_synchronize(bonsai_handle hh) {
   return st;
 }
 
+int bonsai_last_error(bonsai_handle hh) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  const cudaError_t e = cudaPeekAtLastError();
+  if (e != cudaSuccess) return -(int)e - 1000;
+  return h->read_status(false);
+}
+
+int bonsai_step_graph(bonsai_handle hh, int nsteps) { return bonsai_step(hh, nsteps, 1); }
+
 int bonsai_bounds_check(unsigned* count, unsigned* first_site, int reset) {
   unsigned tot = 0, first = 0;
 #ifdef BONSAI_CHECKS

@@ -164,6 +164,13 @@ int bonsai_fp32_peak(int device, double *tflops);
 /* Wait for the handle's stream and its copy streams; returns the sticky device
  * status (and clears it). */
 int bonsai_synchronize(bonsai_handle h);
+/* The last error the handle has seen, without clearing anything: a pending
+ * CUDA error (< 0) if there is one, else the sticky device status bits
+ * (BONSAI_STATUS_*, 0 = none) after waiting for the handle's stream.  API
+ * argument and order errors are returned by the call that made them. */
+int bonsai_last_error(bonsai_handle h);
+/* bonsai_step(h, nsteps, 1): nsteps steps replayed as captured CUDA graphs. */
+int bonsai_step_graph(bonsai_handle h, int nsteps);
 /* the copy streams (cudaStream_t) of the asynchronous set / get, for callers
  * that order their own work or events after them */
 int bonsai_copy_streams(bonsai_handle h, void **h2d, void **d2h);

@@ -210,9 +210,13 @@ def test_walk_level_list_overflow_reports_status():
     t.buildTree(1)
     t.computeMultipoles()
     t.makeGroups(5, 64)
+    assert t._L.bonsai_compute_forces(t.handle, 0, None) == 0  # the launch itself is fine
+    assert t._L.bonsai_last_error(t.handle) & 4                # peek: the status stays set
+    assert t._L.bonsai_last_error(t.handle) & 4
     with pytest.raises(B.BonsaiError) as e:
-        B.treecode._check(t._L.bonsai_compute_forces(t.handle, 0, None) or t._L.bonsai_synchronize(t.handle), "walk")
+        B.treecode._check(t._L.bonsai_synchronize(t.handle), "walk")  # reported and cleared
     assert e.value.code & 4
+    assert t._L.bonsai_last_error(t.handle) == 0
     a = t.get_acc()
     assert np.isnan(a[:, 0]).any()
     t.close()
