@@ -152,6 +152,12 @@ struct Treecode<float> {
     check(bonsai_compute_energies(h_, e.data()), "computeEnergies");
     return e;
   }
+  // whole steps (treecode.cu:139-168) replayed as captured CUDA graphs
+  void step(const int nsteps = 1) { check(bonsai_step_graph(h_, nsteps), "step"); }
+  // waits and returns the sticky device status (cleared); throws on errors
+  int synchronize() { return check(bonsai_synchronize(h_), "synchronize"); }
+  // the last error seen, without clearing it (BONSAI_STATUS_* bits or < 0)
+  int last_error() const { return bonsai_last_error(h_); }
   bonsai_handle handle() const { return h_; }
 
  private:
