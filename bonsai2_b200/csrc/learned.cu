@@ -174,6 +174,19 @@ __global__ void __launch_bounds__(256) k_mlp_fwd_bwd(const float* __restrict__ X
                                                      float* __restrict__ G, float* __restrict__ loss,
                                                      float* __restrict__ pred) {
   __shared__ float sh[8][2][kH];
+  // weights staged once per block: W1 and W2 transposed for the forward pass
+  // (lanes read consecutive hidden units), W2 row-major for the backward pass
+  // (lanes read consecutive inputs); the rest as they are
+  __shared__ float sw1t[kF * kH], sw2t[kH * kH], sw2[kH * kH], sb1[kH], sb2[kH], sw3[kH], sb3;
+  for (int t = threadIdx.x; t < kH * kF; t += blockDim.x) sw1t[(t % kF) * kH + t / kF] = w[oW1 + t];
+  for (int t = threadIdx.x; t < kH * kH; t += blockDim.x) {
+    const float v = w[oW2 + t];
+    sw2[t] = v;
+    sw2t[(t % kH) * kH + t / kH] = v;
+  }
+  for (int t = threadIdx.x; t < kH; t += blockDim.x) { sb1[t] = w[oB1 + t]; sb2[t] = w[oB2 + t]; sw3[t] = w[oW3 + t]; }
+  if (threadIdx.x == 0) sb3 = w[oB3];
+  __syncthreads();
   const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < S; s += nw) {
@@ -184,9 +197,9 @@ __global__ void __launch_bounds__(256) k_mlp_fwd_bwd(const float* __restrict__ X
 #pragma unroll
     for (int u = 0; u < 2; u++) {
       const int j = lane + 32 * u;
-      float a = w[oB1 + j];
+      float a = sb1[j];
 #pragma unroll
-      for (int k = 0; k < kF; k++) a = fmaf(w[oW1 + j * kF + k], x[k], a);
+      for (int k = 0; k < kF; k++) a = fmaf(sw1t[k * kH + j], x[k], a);
       h1[u] = tanhf(a);
       sh[wi][0][j] = h1[u];
     }
@@ -194,14 +207,14 @@ __global__ void __launch_bounds__(256) k_mlp_fwd_bwd(const float* __restrict__ X
 #pragma unroll
     for (int u = 0; u < 2; u++) {
       const int j = lane + 32 * u;
-      float a = w[oB2 + j];
-      for (int i = 0; i < kH; i++) a = fmaf(w[oW2 + j * kH + i], sh[wi][0][i], a);
+      float a = sb2[j];
+      for (int i = 0; i < kH; i++) a = fmaf(sw2t[i * kH + j], sh[wi][0][i], a);
       h2[u] = tanhf(a);
     }
-    float z = w[oW3 + lane] * h2[0] + w[oW3 + lane + 32] * h2[1];
+    float z = sw3[lane] * h2[0] + sw3[lane + 32] * h2[1];
 #pragma unroll
     for (int o = 16; o; o >>= 1) z += __shfl_xor_sync(kFull, z, o);
-    z += w[oB3];
+    z += sb3;
     const float sg = 1.0f / (1.0f + expf(-z));
     const float th = lo + (hi - lo) * sg;
     const float e = th - y[s];
@@ -211,7 +224,7 @@ __global__ void __launch_bounds__(256) k_mlp_fwd_bwd(const float* __restrict__ X
 #pragma unroll
     for (int u = 0; u < 2; u++) {
       const int j = lane + 32 * u;
-      d2[u] = gz * w[oW3 + j] * (1.0f - h2[u] * h2[u]);
+      d2[u] = gz * sw3[j] * (1.0f - h2[u] * h2[u]);
       sh[wi][1][j] = d2[u];
     }
     __syncwarp();
@@ -219,7 +232,7 @@ __global__ void __launch_bounds__(256) k_mlp_fwd_bwd(const float* __restrict__ X
     for (int u = 0; u < 2; u++) {
       const int i = lane + 32 * u;
       float a = 0.f;
-      for (int j = 0; j < kH; j++) a = fmaf(w[oW2 + j * kH + i], sh[wi][1][j], a);
+      for (int j = 0; j < kH; j++) a = fmaf(sw2[j * kH + i], sh[wi][1][j], a);
       const float d1 = a * (1.0f - h1[u] * h1[u]);
       H1[(size_t)s * kH + i] = h1[u];
       D1[(size_t)s * kH + i] = d1;
@@ -235,32 +248,45 @@ __global__ void __launch_bounds__(256) k_mlp_fwd_bwd(const float* __restrict__ X
   }
 }
 
-// grad[t] for t in [0, kMlpWeights): fixed-order sums over the samples
+// Weight gradients as fixed-order sums over the samples, in two levels:
+// block (x, c) sums samples [c * chunk, (c + 1) * chunk) in order for 256
+// weights into part[c][t]; k_mlp_grad_fold then adds the chunks in order.
+constexpr int kGradChunks = 32;
 __global__ void __launch_bounds__(256) k_mlp_grad(const float* __restrict__ X, int S, const float* __restrict__ H1,
                                                   const float* __restrict__ D1, const float* __restrict__ H2,
                                                   const float* __restrict__ D2, const float* __restrict__ G,
-                                                  float* __restrict__ grad) {
+                                                  float* __restrict__ part) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= kMlpWeights) return;
+  const int chunk = (S + kGradChunks - 1) / kGradChunks;
+  const int s0 = blockIdx.y * chunk, s1 = min(S, s0 + chunk);
   float acc = 0.f;
   if (t < oB1) {  // W1[j][k] = sum d1[j] x[k]
     const int j = t / kF, k = t % kF;
-    for (int s = 0; s < S; s++) acc = fmaf(D1[(size_t)s * kH + j], X[(size_t)s * kF + k], acc);
+    for (int s = s0; s < s1; s++) acc = fmaf(D1[(size_t)s * kH + j], X[(size_t)s * kF + k], acc);
   } else if (t < oW2) {
     const int j = t - oB1;
-    for (int s = 0; s < S; s++) acc += D1[(size_t)s * kH + j];
+    for (int s = s0; s < s1; s++) acc += D1[(size_t)s * kH + j];
   } else if (t < oB2) {  // W2[j][i] = sum d2[j] h1[i]
     const int j = (t - oW2) / kH, i = (t - oW2) % kH;
-    for (int s = 0; s < S; s++) acc = fmaf(D2[(size_t)s * kH + j], H1[(size_t)s * kH + i], acc);
+    for (int s = s0; s < s1; s++) acc = fmaf(D2[(size_t)s * kH + j], H1[(size_t)s * kH + i], acc);
   } else if (t < oW3) {
     const int j = t - oB2;
-    for (int s = 0; s < S; s++) acc += D2[(size_t)s * kH + j];
+    for (int s = s0; s < s1; s++) acc += D2[(size_t)s * kH + j];
   } else if (t < oB3) {  // w3[j] = sum g h2[j]
     const int j = t - oW3;
-    for (int s = 0; s < S; s++) acc = fmaf(G[s], H2[(size_t)s * kH + j], acc);
+    for (int s = s0; s < s1; s++) acc = fmaf(G[s], H2[(size_t)s * kH + j], acc);
   } else {
-    for (int s = 0; s < S; s++) acc += G[s];
+    for (int s = s0; s < s1; s++) acc += G[s];
   }
+  part[(size_t)blockIdx.y * kMlpWeights + t] = acc;
+}
+
+__global__ void k_mlp_grad_fold(const float* __restrict__ part, float* __restrict__ grad) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= kMlpWeights) return;
+  float acc = 0.f;
+  for (int c = 0; c < kGradChunks; c++) acc += part[(size_t)c * kMlpWeights + t];
   grad[t] = acc;
 }
 
@@ -290,8 +316,9 @@ __global__ void k_sum_f(const float* __restrict__ a, int S, double* __restrict__
   }
 }
 
-// scratch for training: H1, D1, H2, D2 (S x kH each), G, loss, pred (S each)
-size_t mlp_train_scratch_floats(int S) { return (size_t)S * (4 * kH + 3); }
+// scratch for training: H1, D1, H2, D2 (S x kH each), G, loss, pred (S each),
+// the gradient partials (kGradChunks x kMlpWeights)
+size_t mlp_train_scratch_floats(int S) { return (size_t)S * (4 * kH + 3) + (size_t)kGradChunks * kMlpWeights; }
 
 void mlp_loss_grad(const float* X, const float* y, int S, const float* w, float lo, float hi, float over,
                    float* scratch, float* grad, double* loss_out, cudaStream_t st) {
@@ -302,9 +329,11 @@ void mlp_loss_grad(const float* X, const float* y, int S, const float* w, float 
   float* G = D2 + (size_t)S * kH;
   float* L = G + S;
   float* P = L + S;
-  const int blocks = (S + 7) / 8 < 4096 ? (S + 7) / 8 : 4096;
+  float* part = P + S;
+  const int blocks = (S + 7) / 8 < 512 ? (S + 7) / 8 : 512;
   k_mlp_fwd_bwd<<<blocks, 256, 0, st>>>(X, y, S, w, lo, hi, over, H1, D1, H2, D2, G, L, P);
-  k_mlp_grad<<<(kMlpWeights + 255) / 256, 256, 0, st>>>(X, S, H1, D1, H2, D2, G, grad);
+  k_mlp_grad<<<dim3((kMlpWeights + 255) / 256, kGradChunks), 256, 0, st>>>(X, S, H1, D1, H2, D2, G, part);
+  k_mlp_grad_fold<<<(kMlpWeights + 255) / 256, 256, 0, st>>>(part, grad);
   if (loss_out) k_sum_f<<<1, 256, 0, st>>>(L, S, loss_out);
 }
 
@@ -323,7 +352,7 @@ void mlp_predict(const float* X, int S, const float* w, float lo, float hi, floa
   float* D2 = H2 + (size_t)S * kH;
   float* G = D2 + (size_t)S * kH;
   float* L = G + S;
-  const int blocks = (S + 7) / 8 < 4096 ? (S + 7) / 8 : 4096;
+  const int blocks = (S + 7) / 8 < 512 ? (S + 7) / 8 : 512;
   k_mlp_fwd_bwd<<<blocks, 256, 0, st>>>(X, pred, S, w, lo, hi, 0.f, H1, D1, H2, D2, G, L, pred);
 }
 
