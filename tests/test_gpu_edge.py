@@ -171,6 +171,57 @@ def test_full_size_properties(lib):
     assert np.median(err) < 1e-3
 
 
+def test_max_size_2p27_invariants():
+    """N = 2^27 (134M particles, 8x the bench size, ~35 GB on the device): a
+    Plummer profile drawn by inverse transform (fast on the host); sorted keys,
+    permutations, leaf and group coverage, a graph step with no status, and the
+    force error on a sample, so that no index or size overflows 32 bits on the
+    way to the largest systems one B200 holds comfortably."""
+    import bonsai2_b200 as B
+    n = 1 << 27
+    rng = np.random.default_rng(27)
+    u = rng.uniform(1e-6, 0.99, n)
+    r = 1.0 / np.sqrt(u ** (-2.0 / 3.0) - 1.0)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    pos = np.empty((n, 4), np.float32)
+    pos[:, :3] = d * r[:, None]
+    pos[:, 3] = 1.0 / n
+    del u, r, d
+    vel = np.zeros((n, 4), np.float32)
+    t = B.Treecode(eps=0.005, theta=0.6, dt=1.0 / 128)
+    t.alloc(n)
+    t.h_ptclPos[:] = pos
+    t.h_ptclVel[:] = vel
+    t.ptcl_h2d()
+    t.buildTree(16)
+    t.computeMultipoles()
+    t.makeGroups(5, 64)
+    t.computeForces(False)
+    assert t.synchronize() == 0
+    k = t.keys()
+    assert np.all(k["tree_keys"][1:] >= k["tree_keys"][:-1])
+    assert np.all(k["ph_keys"][1:] >= k["ph_keys"][:-1])
+    for perm in (k["tree_perm"], k["ph_perm"]):
+        c = np.bincount(perm, minlength=n)
+        assert c.shape[0] == n and c.min() == 1 and c.max() == 1
+    del k
+    cd = t.cells(multipoles=False)["cell_data"]
+    leaf = cd[:, 1] == 0xFFFFFFFF
+    assert (cd[leaf, 3].astype(np.int64) - cd[leaf, 2]).sum() == n
+    del cd, leaf
+    g = t.groups()
+    assert g[:, 1].astype(np.int64).sum() == n and np.all(g[:, 1] <= 64)
+    acc = t.get_acc().astype(np.float64)
+    samp = np.random.default_rng(11).choice(n, 128, replace=False).astype(np.int32)
+    ref = t.direct_fp64(samp, include_self=True)
+    err = np.linalg.norm(acc[samp, :3] - ref[:, :3], axis=1) / np.linalg.norm(ref[:, :3], axis=1)
+    assert np.median(err) < 1e-3
+    t.step(1, graph=True)
+    assert t.synchronize() == 0
+    t.close()
+
+
 def test_bounded_wait_reports_and_device_stays_usable():
     """A radix-sort pass whose first tile never starts: the next tile's
     look-back waits on a flag nothing sets, ends at its bound and reports
