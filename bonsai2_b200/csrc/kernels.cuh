@@ -146,9 +146,12 @@ void mlp_loss_grad(const float* X, const float* y, int S, const float* w, float 
 void mlp_adam_step(float* w, const float* grad, float* m, float* v, float lr, int step, cudaStream_t st);
 void mlp_predict(const float* X, int S, const float* w, float lo, float hi, float* scratch, float* pred,
                  cudaStream_t st);
+// box: the domain box, or an ensemble's per-system boxes (nsys > 1, with
+// sys_off and the systems' level-1 cell ranges root_beg)
 void launch_group_features(const int2* groups, const TreeInfo* info, const float4* ipos,
                            const unsigned long long* ph_sorted, const MpRec* rec, const Box* box, int n, int ncrit,
-                           float eps, float* feat, int nblocks, cudaStream_t st);
+                           float eps, float* feat, const int* sys_off, int nsys, const int* root_beg, int nblocks,
+                           cudaStream_t st);
 void launch_mlp_infer(const float* feat, const void* wh, const TreeInfo* info, float lo, float hi, float* inv,
                       int nblocks, cudaStream_t st);
 void launch_weights_to_half(const float* w, void* wh, cudaStream_t st);

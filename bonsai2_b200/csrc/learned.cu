@@ -34,22 +34,35 @@ __global__ void __launch_bounds__(256) k_group_features(const int2* __restrict__
                                                         const float4* __restrict__ ipos,
                                                         const unsigned long long* __restrict__ ph_sorted,
                                                         const MpRec* __restrict__ rec, const Box* __restrict__ box,
-                                                        int n, int ncrit, float eps, float* __restrict__ feat) {
+                                                        int n, int ncrit, float eps, float* __restrict__ feat,
+                                                        const int* __restrict__ sys_off, int nsys,
+                                                        const int* __restrict__ root_beg) {
   const int lane = threadIdx.x & 31;
   const int ng = info->ngroups;
-  // system centre of mass and mass from the level-1 cells
-  double M = 0, X = 0, Y = 0, Z = 0;
-  for (int c = info->level_beg[1]; c < info->level_end[1]; c++) {
-    const double m = rec[c].m;
-    M += m; X += m * rec[c].cx; Y += m * rec[c].cy; Z += m * rec[c].cz;
-  }
-  const float mtot = (float)M;
-  const float cx = M > 0 ? (float)(X / M) : 0.f, cy = M > 0 ? (float)(Y / M) : 0.f, cz = M > 0 ? (float)(Z / M) : 0.f;
-  const float hs = box->hsize;
+  // the group's system: its centre of mass and mass from its level-1 cells,
+  // its box and its size (an ensemble's systems each have their own)
+  int sys = -1;
+  float mtot = 0.f, cx = 0.f, cy = 0.f, cz = 0.f, hs = 0.f;
+  int ns = n;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   for (int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < ng; g += nw) {
     const int2 gd = groups[g];
     const int pb = gd.x, np = gd.y;
+    const int s = nsys > 1 ? sys_of(sys_off, nsys, pb) : 0;
+    if (s != sys) {
+      sys = s;
+      const int c0 = nsys > 1 ? root_beg[s] : info->level_beg[1];
+      const int c1 = nsys > 1 ? root_beg[s + 1] : info->level_end[1];
+      double M = 0, X = 0, Y = 0, Z = 0;
+      for (int c = c0; c < c1; c++) {
+        const double m = rec[c].m;
+        M += m; X += m * rec[c].cx; Y += m * rec[c].cy; Z += m * rec[c].cz;
+      }
+      mtot = (float)M;
+      cx = M > 0 ? (float)(X / M) : 0.f; cy = M > 0 ? (float)(Y / M) : 0.f; cz = M > 0 ? (float)(Z / M) : 0.f;
+      hs = box[s].hsize;
+      ns = nsys > 1 ? sys_off[s + 1] - sys_off[s] : n;
+    }
     float mn[3] = {3e38f, 3e38f, 3e38f}, mx[3] = {-3e38f, -3e38f, -3e38f};
     float mg = 0.f;
     for (int i = lane; i < np; i += 32) {
@@ -83,17 +96,21 @@ __global__ void __launch_bounds__(256) k_group_features(const int2* __restrict__
       f[3] = safe_log10(rg / fmaxf(dg, 1e-12f * hs)) / 3.f;
       f[4] = (float)min(lvl, kMaxLevel) / (float)kMaxLevel;
       f[5] = safe_log10(mg / fmaxf(mtot, 1e-30f)) / 8.f;
-      f[6] = safe_log10((float)np / vol * hs * hs * hs / (float)n) / 8.f;
+      f[6] = safe_log10((float)np / vol * hs * hs * hs / (float)ns) / 8.f;
       f[7] = sx / rg; f[8] = sy / rg; f[9] = sz / rg;
-      f[10] = log10f((float)n) / 8.f;
+      f[10] = log10f((float)ns) / 8.f;
       f[11] = safe_log10(fmaxf(eps, 1e-12f) / rg) / 3.f;
       f[12] = safe_log10(fmaxf(eps, 1e-12f) / hs) / 6.f;
       f[13] = dg / (dg + rg);
       f[14] = (md / (float)np) / rg;
       f[15] = 1.0f;
+      // degenerate groups (a one-particle system's box and radius are floored
+      // near 1e-12, so the density's float products under- and overflow) give
+      // inf or NaN; the features are normalised logs well inside [-10, 10], and
+      // fmaxf returns its other operand for a NaN
       float* o = feat + (size_t)g * kF;
 #pragma unroll
-      for (int k = 0; k < kF; k++) o[k] = f[k];
+      for (int k = 0; k < kF; k++) o[k] = fminf(fmaxf(f[k], -10.0f), 10.0f);
     }
   }
 }
@@ -358,8 +375,10 @@ void mlp_predict(const float* X, int S, const float* w, float lo, float hi, floa
 
 void launch_group_features(const int2* groups, const TreeInfo* info, const float4* ipos,
                            const unsigned long long* ph_sorted, const MpRec* rec, const Box* box, int n, int ncrit,
-                           float eps, float* feat, int nblocks, cudaStream_t st) {
-  k_group_features<<<nblocks, 256, 0, st>>>(groups, info, ipos, ph_sorted, rec, box, n, ncrit, eps, feat);
+                           float eps, float* feat, const int* sys_off, int nsys, const int* root_beg, int nblocks,
+                           cudaStream_t st) {
+  k_group_features<<<nblocks, 256, 0, st>>>(groups, info, ipos, ph_sorted, rec, box, n, ncrit, eps, feat, sys_off,
+                                            nsys, root_beg);
 }
 
 void launch_mlp_infer(const float* feat, const void* wh, const TreeInfo* info, float lo, float hi, float* inv,

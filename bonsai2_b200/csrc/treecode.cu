@@ -409,7 +409,7 @@ struct Handle {
     BONSAI_CUDA_TRY(cudaMemcpy(chunks, ch.data(), ch.size() * sizeof(int4), cudaMemcpyHostToDevice));
     BONSAI_CUDA_TRY(cudaMemset(sys_energy, 0, (size_t)ns * 8 * sizeof(double)));
     BONSAI_CUDA_TRY(cudaMemset(root_beg, 0, (size_t)(ns + 1) * sizeof(int)));
-    theta_mode = 0;  // per-group angles, double-single positions, block steps: single systems
+    theta_mode = 0;  // angles are set again for the ensemble; double-single and block steps: single systems
     precision = 0;
     release_lo();
     bts_K = -1;
@@ -465,8 +465,8 @@ struct Handle {
     if (nsys > 1) {
       // ka (8 bytes per particle) is free after the sort: segment flags and indices
       unsigned* flag = reinterpret_cast<unsigned*>(ka);
-      make_groups_sys(pkey, n, ls, ncrit, sys_off, nsys, flag, flag + n, seg_beg, seg_end, nseg, bsum, groups, n, info,
-                      s);
+      make_groups_sys(pkey, n, ls, ncrit, sys_off, nsys, flag, flag + n, seg_beg, seg_end, nseg, bsum, groups,
+                      theta_mode ? gcap : n, info, s);
     } else {
       make_groups(pkey, n, ls, ncrit, g_count, g_seg, g_ng, bsum, groups, theta_mode ? gcap : n, info, s);
     }
@@ -501,7 +501,8 @@ struct Handle {
     cudaMemsetAsync(stats, 0, 4 * sizeof(unsigned long long), st);
     const float* ginv = nullptr;
     if (theta_mode == 1) {
-      launch_group_features(groups, info, pos[par], pkey, rec, box, n, ncrit, prm.eps, group_feat, nsm * 8, st);
+      launch_group_features(groups, info, pos[par], pkey, rec, nsys > 1 ? sys_box : box, n, ncrit, prm.eps,
+                            group_feat, so(), nsys, root_beg, nsm * 8, st);
       launch_mlp_infer(group_feat, mlp_wh, info, theta_lo, theta_hi, group_inv, nsm * 4, st);
       ginv = group_inv;
     } else if (theta_mode == 2) {
@@ -1521,7 +1522,6 @@ int bonsai_set_theta_mode(bonsai_handle hh, int mode, float lo, float hi) {
   if (!h) return BONSAI_ERR_HANDLE;
   if (mode < 0 || mode > 2 || !(lo > 0.f) || !(hi >= lo)) return BONSAI_ERR_ARG;
   if (mode == 1 && !h->mlp_loaded) return BONSAI_ERR_ORDER;
-  if (mode != 0 && h->nsys > 1) return BONSAI_ERR_ARG;  // per-group angles: single systems only
   h->theta_mode = mode;
   h->theta_lo = lo;
   h->theta_hi = hi;
@@ -1570,8 +1570,8 @@ int bonsai_get_group_features(bonsai_handle hh, float* out, int* ngroups) {
   BONSAI_CUDA_TRY(cudaMemcpyAsync(&ng, &h->info->ngroups, sizeof(int), cudaMemcpyDeviceToHost, h->st));
   BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
   if (ng > h->gcap) return BONSAI_STATUS_GROUP_CAPACITY;
-  launch_group_features(h->groups, h->info, h->pos[h->par], h->pkey, h->rec, h->box, h->n, h->cur_ncrit, h->prm.eps,
-                        h->group_feat, h->nsm * 8, h->st);
+  launch_group_features(h->groups, h->info, h->pos[h->par], h->pkey, h->rec, h->nsys > 1 ? h->sys_box : h->box, h->n,
+                        h->cur_ncrit, h->prm.eps, h->group_feat, h->so(), h->nsys, h->root_beg, h->nsm * 8, h->st);
   BONSAI_CUDA_TRY(cudaMemcpyAsync(out, h->group_feat, (size_t)ng * kMlpFeatures * 4, cudaMemcpyDeviceToHost, h->st));
   BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
   *ngroups = ng;

@@ -482,6 +482,7 @@ static int occupancy_of() {
   int nb = occupancy(k_walk<NI, SPLIT, false, false, false>);
   nb = std::min(nb, occupancy(k_walk<NI, SPLIT, true, false, false>));
   nb = std::min(nb, occupancy(k_walk<NI, SPLIT, false, true, false>));
+  nb = std::min(nb, occupancy(k_walk<NI, SPLIT, true, true, false>));
   nb = std::min(nb, occupancy(k_walk<NI, SPLIT, false, false, true>));
   nb = std::min(nb, occupancy(k_walk<NI, SPLIT, true, false, true>));
   return nb < 1 ? 1 : nb;
@@ -513,7 +514,9 @@ void launch_walk(int variant, int nblocks, const int2* groups, const TreeInfo* i
       group_list, group_list_n
 #define BONSAI_WALK(NI, SP)                                                                \
   do {                                                                                     \
-    if (nsys > 1)                                                                          \
+    if (nsys > 1 && group_inv_theta)                                                       \
+      k_walk<NI, SP, true, true, false><<<nblocks, kWalkThreads, 0, s>>>(BONSAI_WALK_ARGS);  \
+    else if (nsys > 1)                                                                     \
       k_walk<NI, SP, false, true, false><<<nblocks, kWalkThreads, 0, s>>>(BONSAI_WALK_ARGS); \
     else if (ipos_lo && group_inv_theta)                                                   \
       k_walk<NI, SP, true, false, true><<<nblocks, kWalkThreads, 0, s>>>(BONSAI_WALK_ARGS);  \

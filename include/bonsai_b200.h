@@ -224,7 +224,9 @@ int bonsai_direct_fp64_noalloc(const float *d_pos4, int n, const int *d_sample, 
 #define BONSAI_MLP_FEATURES 16
 #define BONSAI_MLP_WEIGHTS 5313 /* W1[64][16], b1[64], W2[64][64], b2[64], w3[64], b3 */
 /* mode 0: fixed theta (params); 1: theta_g = lo + (hi-lo)*sigmoid(MLP(features_g))
- * from the weights of bonsai_set_mlp_weights; 2: theta_g from bonsai_set_group_theta. */
+ * from the weights of bonsai_set_mlp_weights; 2: theta_g from bonsai_set_group_theta.
+ * Features are clamped to [-10, 10] (degenerate groups, e.g. of a one-particle
+ * system, would otherwise give inf or NaN). */
 int bonsai_set_theta_mode(bonsai_handle h, int mode, float lo, float hi);
 int bonsai_set_mlp_weights(bonsai_handle h, const float *w, int nw);
 /* host array of ngroups angles for the current groups (after bonsai_make_groups) */
@@ -289,8 +291,11 @@ int bonsai_get_particles_f64(bonsai_handle h, double *pos4, float *vel4, float *
  * handle that holds that system alone with the same parameters.
  * bonsai_compute_energies then sums over all systems; bonsai_get_box returns
  * system 0's box; bonsai_direct_fp64 sums inside each sample's system.
- * Per-group opening angles (bonsai_set_theta_mode != 0) are for single
- * systems only (BONSAI_ERR_ARG).  nsys <= 65536. */
+ * Per-group opening angles (bonsai_set_theta_mode, set after this call) work
+ * inside an ensemble: the network's features are normalised per system, so a
+ * system's angles, and with them its forces, are those it gets alone.
+ * Double-single positions and block time steps are for single systems only
+ * (BONSAI_ERR_ARG).  nsys <= 65536. */
 int bonsai_set_systems(bonsai_handle h, const int *counts, int nsys);
 /* energies of every system, 8 doubles per system in the layout and with the
  * timing rules of bonsai_compute_energies (a single system: its 8 values) */

@@ -107,16 +107,65 @@ def test_ensemble_direct_sum_is_per_system():
     t.close()
 
 
-def test_ensemble_rejects_per_group_theta_and_bad_counts():
+def test_ensemble_rejects_bad_counts_and_double_single():
     import bonsai2_b200 as B
     from bonsai2_b200._lib import BonsaiError
     t = B.Treecode(**PARAMS)
     with pytest.raises(BonsaiError):
         t.set_systems(np.array([10, 0, 5], np.int32))
     t.set_systems(np.array([10, 5], np.int32))
-    # per-group opening angles are a single-system feature
-    assert t._L.bonsai_set_theta_mode(t.handle, 2, 0.25, 1.25) == -4
+    assert t._L.bonsai_set_precision(t.handle, 1) == -4  # double-single positions: single systems
     t.close()
+
+
+def _forces(t, pos, vel, mode=0, theta_g=None, weights=None):
+    """One eager force evaluation with fixed (0), network (1) or given (2) angles."""
+    from bonsai2_b200 import learned
+    t.h_ptclPos[:] = pos
+    t.h_ptclVel[:] = vel
+    t.ptcl_h2d()
+    if mode == 1:
+        learned.set_weights(t, weights)
+    learned.set_theta_mode(t, mode)
+    t.buildTree(t.nLeaf)
+    t.computeMultipoles()
+    t.makeGroups(5, t.nCrit)
+    if mode == 2:
+        learned.set_group_theta(t, np.full(t.groups().shape[0], theta_g, np.float32))
+    t.computeForces(True)
+    assert t.synchronize() == 0
+    return t.get_acc()
+
+
+def test_ensemble_per_group_angles():
+    """Per-group opening angles inside an ensemble: every group at the fixed
+    angle (mode 2) is the fixed-angle walk bit for bit, and network angles
+    (mode 1, features normalised per system) give each system, bit for bit,
+    what it gets alone."""
+    import bonsai2_b200 as B
+    from bonsai2_b200 import learned
+    counts = np.array([300, 1, 4000, 57, 9000, 2], np.int32)
+    pos, vel = _ensemble_inputs(counts, seed=31)
+    off = _offsets(counts)
+    t = B.Treecode(**PARAMS)
+    t.set_systems(counts)  # allocates for sum(counts)
+    a_fixed = _forces(t, pos, vel, 0)
+    a_const = _forces(t, pos, vel, 2, theta_g=PARAMS["theta"])
+    assert np.array_equal(a_fixed.view(np.uint32), a_const.view(np.uint32))
+    w = learned.init_weights(4)
+    a_net = _forces(t, pos, vel, 1, weights=w)
+    th = learned.group_theta(t)
+    # finite everywhere (systems of 1 and 2 particles have degenerate features)
+    # and varying from group to group
+    assert np.isfinite(th).all() and th.std() > 0
+    t.close()
+    for s in range(counts.shape[0]):
+        b, e = off[s], off[s + 1]
+        u = B.Treecode(**PARAMS)
+        u.alloc(int(e - b))
+        a_alone = _forces(u, pos[b:e], vel[b:e], 1, weights=w)
+        u.close()
+        assert np.array_equal(a_net[b:e].view(np.uint32), a_alone.view(np.uint32)), f"system {s}"
 
 
 def test_autotune_restores_state_and_keeps_bit_identity():
