@@ -94,10 +94,11 @@ void launch_scatter_d4(const int* id, int n, const double4* in, double4* out, in
 void launch_move(float4* pos, float4* vel, const float4* acc, int n, float dt, int* closing, float eps, int write,
                  double* partial, int nblocks, unsigned* ticket, double* energies, cudaStream_t s,
                  float4* lo = nullptr);
-// ensemble move: energies per chunk, folded per system and in total
+// ensemble move: energies per chunk, folded per system and in total (lo as launch_move)
 void launch_move_sys(float4* pos, float4* vel, const float4* acc, const int4* chunks, int nchunks,
                      const int* chunk_beg, int nsys, float dt, int* closing, float eps, int write, double* chunk_part,
-                     int nblocks, unsigned* ticket, double* energies, double* sys_energies, cudaStream_t s);
+                     int nblocks, unsigned* ticket, double* energies, double* sys_energies, cudaStream_t s,
+                     float4* lo = nullptr);
 // block time steps (hierarchical levels, kick-drift-kick per particle)
 void launch_bts_open_drift(float4* pos, float4* vel, const float4* acc, const unsigned char* lev, int n, float dt,
                            int K, int s, float4* lo, int nblocks, cudaStream_t st);
@@ -113,9 +114,9 @@ void launch_scatter_u8(const int* id, int n, const unsigned char* in, unsigned c
                        cudaStream_t st);
 // pending closing kick applied in place, then the closing flag cleared
 void launch_closing_kick(float4* vel, const float4* acc, int n, float dt, int* closing, int nblocks, cudaStream_t s);
-// FP64 direct sum inside each sample's own system (one block per sample)
+// FP64 direct sum inside each sample's own system (one block per sample; lo as launch_direct_fp64)
 void launch_direct_fp64_sys(const float4* pos, const int* sys_off, int nsys, const int* sample, int ns, double eps2,
-                            int include_self, double* out, cudaStream_t s);
+                            int include_self, double* out, cudaStream_t s, const float4* lo = nullptr);
 // lo (nullable): double-single low parts, positions taken as hi + lo
 void launch_direct_fp64(const float4* pos, int n, const int* sample, int ns, double eps2, int include_self,
                         double* part, int nsplit, double* out, cudaStream_t s, const float4* lo = nullptr);

@@ -131,7 +131,8 @@ __global__ void __launch_bounds__(256) k_move_sys(float4* __restrict__ pos, floa
                                                   int nchunks, const int* __restrict__ chunk_beg, int nsys, float dt,
                                                   int* __restrict__ closing, float eps, int write,
                                                   double* __restrict__ chunk_part, unsigned* __restrict__ ticket,
-                                                  double* __restrict__ energies, double* __restrict__ sys_energies) {
+                                                  double* __restrict__ energies, double* __restrict__ sys_energies,
+                                                  float4* __restrict__ lo) {
   const float h = 0.5f * dt;
   const float hc = (*closing) ? h : 0.0f;
   const double ieps = eps > 0.f ? 1.0 / (double)eps : 0.0;
@@ -140,7 +141,8 @@ __global__ void __launch_bounds__(256) k_move_sys(float4* __restrict__ pos, floa
   for (int c = blockIdx.x; c < nchunks; c += gridDim.x) {
     const int4 ch = chunks[c];
     EnergySums e;
-    for (int i = ch.x + threadIdx.x; i < ch.y; i += blockDim.x) move_one(pos, vel, acc, i, dt, h, hc, ieps, write, e);
+    for (int i = ch.x + threadIdx.x; i < ch.y; i += blockDim.x)
+      move_one(pos, vel, acc, i, dt, h, hc, ieps, write, e, lo);
     const double x = block_energy_sum(e, sh);
     if (threadIdx.x < kNE) chunk_part[(size_t)c * kNE + threadIdx.x] = x;
   }
@@ -171,9 +173,10 @@ __global__ void __launch_bounds__(256) k_move_sys(float4* __restrict__ pos, floa
 
 void launch_move_sys(float4* pos, float4* vel, const float4* acc, const int4* chunks, int nchunks,
                      const int* chunk_beg, int nsys, float dt, int* closing, float eps, int write, double* chunk_part,
-                     int nblocks, unsigned* ticket, double* energies, double* sys_energies, cudaStream_t s) {
+                     int nblocks, unsigned* ticket, double* energies, double* sys_energies, cudaStream_t s,
+                     float4* lo) {
   k_move_sys<<<nblocks, 256, 0, s>>>(pos, vel, acc, chunks, nchunks, chunk_beg, nsys, dt, closing, eps, write,
-                                     chunk_part, ticket, energies, sys_energies);
+                                     chunk_part, ticket, energies, sys_energies, lo);
 }
 
 void launch_move(float4* pos, float4* vel, const float4* acc, int n, float dt, int* closing, float eps, int write,
@@ -399,12 +402,14 @@ void launch_scatter_u8(const int* id, int n, const unsigned char* in, unsigned c
 }
 
 // Ensemble checker: each sample's force from the particles of its own system
-// only (positions in the caller's order, systems contiguous); one block per
-// sample, fixed-order block reduction.
+// only (positions in the caller's order, systems contiguous; lo, nullable:
+// double-single low parts, positions taken as hi + lo); one block per sample,
+// fixed-order block reduction.
 __global__ void __launch_bounds__(256) k_direct_fp64_sys(const float4* __restrict__ pos,
                                                          const int* __restrict__ sys_off, int nsys,
                                                          const int* __restrict__ sample, int ns, double eps2,
-                                                         int include_self, double* __restrict__ out) {
+                                                         int include_self, double* __restrict__ out,
+                                                         const float4* __restrict__ lo) {
   __shared__ double sh[4][8];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int s = blockIdx.x; s < ns; s += gridDim.x) {
@@ -412,12 +417,21 @@ __global__ void __launch_bounds__(256) k_direct_fp64_sys(const float4* __restric
     const int sy = sys_of(sys_off, nsys, i);
     const int jb = sys_off[sy], je = sys_off[sy + 1];
     const float4 pi = pos[i];
-    const double xi = pi.x, yi = pi.y, zi = pi.z;
+    double xi = pi.x, yi = pi.y, zi = pi.z;
+    if (lo) {
+      const float4 l = lo[i];
+      xi += l.x; yi += l.y; zi += l.z;
+    }
     double a[4] = {0, 0, 0, 0};
     for (int j = jb + threadIdx.x; j < je; j += blockDim.x) {
       if (j == i && !include_self) continue;
       const float4 q = pos[j];
-      const double dx = q.x - xi, dy = q.y - yi, dz = q.z - zi;
+      double qx = q.x, qy = q.y, qz = q.z;
+      if (lo) {
+        const float4 l = lo[j];
+        qx += l.x; qy += l.y; qz += l.z;
+      }
+      const double dx = qx - xi, dy = qy - yi, dz = qz - zi;
       const double r2 = fma(dz, dz, fma(dy, dy, fma(dx, dx, eps2)));
       const double rinv = rsqrt(r2);
       const double mr = q.w * rinv;
@@ -442,8 +456,9 @@ __global__ void __launch_bounds__(256) k_direct_fp64_sys(const float4* __restric
 }
 
 void launch_direct_fp64_sys(const float4* pos, const int* sys_off, int nsys, const int* sample, int ns, double eps2,
-                            int include_self, double* out, cudaStream_t s) {
-  k_direct_fp64_sys<<<ns < 65535 ? ns : 65535, 256, 0, s>>>(pos, sys_off, nsys, sample, ns, eps2, include_self, out);
+                            int include_self, double* out, cudaStream_t s, const float4* lo) {
+  k_direct_fp64_sys<<<ns < 65535 ? ns : 65535, 256, 0, s>>>(pos, sys_off, nsys, sample, ns, eps2, include_self, out,
+                                                            lo);
 }
 
 // out[id[k]] = in[k]

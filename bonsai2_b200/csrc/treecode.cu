@@ -409,7 +409,7 @@ struct Handle {
     BONSAI_CUDA_TRY(cudaMemcpy(chunks, ch.data(), ch.size() * sizeof(int4), cudaMemcpyHostToDevice));
     BONSAI_CUDA_TRY(cudaMemset(sys_energy, 0, (size_t)ns * 8 * sizeof(double)));
     BONSAI_CUDA_TRY(cudaMemset(root_beg, 0, (size_t)(ns + 1) * sizeof(int)));
-    theta_mode = 0;  // angles are set again for the ensemble; double-single and block steps: single systems
+    theta_mode = 0;  // angles and precision are set again for the ensemble; block steps: single systems
     precision = 0;
     release_lo();
     bts_K = -1;
@@ -723,7 +723,7 @@ struct Handle {
 void Handle::launch_move_wrapper(bool write) {
   if (nsys > 1)
     launch_move_sys(pos[par], vel[par], acc, chunks, nchunks, chunk_beg, nsys, prm.dt, closing, prm.eps, write ? 1 : 0,
-                    chunk_energy, move_blocks, move_ticket, energies, sys_energy, st);
+                    chunk_energy, move_blocks, move_ticket, energies, sys_energy, st, precision ? plo[par] : nullptr);
   else
     launch_move(pos[par], vel[par], acc, n, prm.dt, closing, prm.eps, write ? 1 : 0, move_partial, move_blocks,
                 move_ticket, energies, st, precision ? plo[par] : nullptr);
@@ -1095,7 +1095,6 @@ int bonsai_set_precision(bonsai_handle hh, int mode) {
   Handle* h = H(hh);
   if (!h) return BONSAI_ERR_HANDLE;
   if (mode < 0 || mode > 1) return BONSAI_ERR_ARG;
-  if (mode && h->nsys > 1) return BONSAI_ERR_ARG;
   BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
   BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
   h->release_graphs();
@@ -1508,7 +1507,8 @@ int bonsai_direct_fp64(bonsai_handle hh, const int* sample, int ns, int include_
   BONSAI_CUDA_TRY(cudaMemcpyAsync(h->direct_sample, sample, (size_t)ns * 4, cudaMemcpyHostToDevice, h->st));
   const double e2 = (double)h->prm.eps * (double)h->prm.eps;
   if (h->nsys > 1)
-    launch_direct_fp64_sys(tmp, h->sys_off, h->nsys, h->direct_sample, ns, e2, include_self, h->direct_out, h->st);
+    launch_direct_fp64_sys(tmp, h->sys_off, h->nsys, h->direct_sample, ns, e2, include_self, h->direct_out, h->st,
+                           tmp_lo);
   else
     launch_direct_fp64(tmp, h->n, h->direct_sample, ns, e2, include_self, h->direct_part, nsplit, h->direct_out,
                        h->st, tmp_lo);

@@ -483,6 +483,8 @@ static int occupancy_of() {
   nb = std::min(nb, occupancy(k_walk<NI, SPLIT, true, false, false>));
   nb = std::min(nb, occupancy(k_walk<NI, SPLIT, false, true, false>));
   nb = std::min(nb, occupancy(k_walk<NI, SPLIT, true, true, false>));
+  nb = std::min(nb, occupancy(k_walk<NI, SPLIT, false, true, true>));
+  nb = std::min(nb, occupancy(k_walk<NI, SPLIT, true, true, true>));
   nb = std::min(nb, occupancy(k_walk<NI, SPLIT, false, false, true>));
   nb = std::min(nb, occupancy(k_walk<NI, SPLIT, true, false, true>));
   return nb < 1 ? 1 : nb;
@@ -514,7 +516,11 @@ void launch_walk(int variant, int nblocks, const int2* groups, const TreeInfo* i
       group_list, group_list_n
 #define BONSAI_WALK(NI, SP)                                                                \
   do {                                                                                     \
-    if (nsys > 1 && group_inv_theta)                                                       \
+    if (nsys > 1 && ipos_lo && group_inv_theta)                                            \
+      k_walk<NI, SP, true, true, true><<<nblocks, kWalkThreads, 0, s>>>(BONSAI_WALK_ARGS);   \
+    else if (nsys > 1 && ipos_lo)                                                          \
+      k_walk<NI, SP, false, true, true><<<nblocks, kWalkThreads, 0, s>>>(BONSAI_WALK_ARGS);  \
+    else if (nsys > 1 && group_inv_theta)                                                  \
       k_walk<NI, SP, true, true, false><<<nblocks, kWalkThreads, 0, s>>>(BONSAI_WALK_ARGS);  \
     else if (nsys > 1)                                                                     \
       k_walk<NI, SP, false, true, false><<<nblocks, kWalkThreads, 0, s>>>(BONSAI_WALK_ARGS); \

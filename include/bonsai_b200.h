@@ -268,8 +268,9 @@ int bonsai_compute_forces_fp64(bonsai_handle h, double *acc4, unsigned long long
  * particle, (hi - R) + lo, so separations keep FP32 relative precision far
  * from the origin; the drift adds in double-single; the FP64 checker
  * (bonsai_direct_fp64) uses hi + lo.  Interactions stay FP32.  Set it before
- * loading particles (the low parts start at zero); single systems only
- * (BONSAI_ERR_ARG for an ensemble).  mode 0 (default) = float positions. */
+ * loading particles (the low parts start at zero) and, for an ensemble, after
+ * bonsai_set_systems (each system then advances bit for bit as it does
+ * alone).  mode 0 (default) = float positions. */
 int bonsai_set_precision(bonsai_handle h, int mode);
 /* bonsai_set_particles from double positions pos4 = (x, y, z, m): split into
  * hi = (float)x and lo = (float)(x - hi) (lo dropped in mode 0) */
@@ -294,7 +295,8 @@ int bonsai_get_particles_f64(bonsai_handle h, double *pos4, float *vel4, float *
  * Per-group opening angles (bonsai_set_theta_mode, set after this call) work
  * inside an ensemble: the network's features are normalised per system, so a
  * system's angles, and with them its forces, are those it gets alone.
- * Double-single positions and block time steps are for single systems only
+ * Double-single positions (bonsai_set_precision, set after this call) work
+ * inside an ensemble too.  Block time steps are for single systems only
  * (BONSAI_ERR_ARG).  nsys <= 65536. */
 int bonsai_set_systems(bonsai_handle h, const int *counts, int nsys);
 /* energies of every system, 8 doubles per system in the layout and with the

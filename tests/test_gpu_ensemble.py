@@ -107,15 +107,76 @@ def test_ensemble_direct_sum_is_per_system():
     t.close()
 
 
-def test_ensemble_rejects_bad_counts_and_double_single():
+def test_ensemble_rejects_bad_counts_and_block_steps():
     import bonsai2_b200 as B
     from bonsai2_b200._lib import BonsaiError
     t = B.Treecode(**PARAMS)
     with pytest.raises(BonsaiError):
         t.set_systems(np.array([10, 0, 5], np.int32))
     t.set_systems(np.array([10, 5], np.int32))
-    assert t._L.bonsai_set_precision(t.handle, 1) == -4  # double-single positions: single systems
+    assert t._L.bonsai_set_block_steps(t.handle, 2, 0.05) == -4  # block time steps: single systems
     t.close()
+
+
+def _ds_inputs(counts, seed=91):
+    """float64 galaxies, each moved far from the origin by its own offset."""
+    import bonsai2_b200 as B
+    rng = np.random.default_rng(seed)
+    ps, vs = [], []
+    for s, c in enumerate(counts):
+        p, v = B.galaxy(int(c), seed=seed + s)
+        p[:, :3] += rng.uniform(-2.0e4, 2.0e4, 3)
+        ps.append(p)
+        vs.append(v)
+    return np.concatenate(ps), np.concatenate(vs)
+
+
+def _ds_run(t, pos, vel, steps, eager):
+    t.set_precision(1)
+    t.set_particles_f64(pos, vel)
+    if eager:
+        for _ in range(steps):
+            t.buildTree(t.nLeaf)
+            t.computeMultipoles()
+            t.makeGroups(5, t.nCrit)
+            t.computeForces(False)
+            t.moveParticles()
+    else:
+        t.step(steps, graph=True)
+    assert t.synchronize() == 0
+    return t.get_particles_f64()
+
+
+@pytest.mark.parametrize("eager", [False, True])
+def test_ensemble_double_single_bit_identical_to_alone(eager):
+    """Double-single positions inside an ensemble: systems far from the origin,
+    each with its own offset, advance bit for bit as they do alone (positions
+    hi + lo, velocities, accelerations), and the FP64 checker sums each sample
+    over its own system's hi + lo positions."""
+    import bonsai2_b200 as B
+    counts = np.array([1, 2, 700, 5000, 3000], np.int32)
+    pos, vel = _ds_inputs(counts)
+    off = _offsets(counts)
+    t = B.Treecode(**PARAMS)
+    t.set_systems(counts)
+    p, v, a = _ds_run(t, pos, vel, 3, eager)
+    sample = np.array([0, 1, 2, 3, 500, 703, 4000, 8702], np.int32)
+    d_ens = t.direct_fp64(sample, include_self=True)
+    t.close()
+    for s in range(counts.shape[0]):
+        b, e = off[s], off[s + 1]
+        u = B.Treecode(**PARAMS)
+        u.alloc(int(e - b))
+        pa, va, aa = _ds_run(u, pos[b:e], vel[b:e], 3, eager)
+        inside = sample[(sample >= b) & (sample < e)]
+        d_alone = u.direct_fp64((inside - b).astype(np.int32), include_self=True) if inside.size else None
+        u.close()
+        assert np.array_equal(p[b:e].view(np.uint64), pa.view(np.uint64)), f"positions of system {s}"
+        assert np.array_equal(v[b:e].view(np.uint32), va.view(np.uint32)), f"velocities of system {s}"
+        assert np.array_equal(a[b:e].view(np.uint32), aa.view(np.uint32)), f"accelerations of system {s}"
+        if inside.size:
+            k = np.searchsorted(sample, inside)
+            np.testing.assert_allclose(d_ens[k], d_alone, rtol=1e-12, atol=1e-12)
 
 
 def _forces(t, pos, vel, mode=0, theta_g=None, weights=None):

@@ -129,11 +129,15 @@ def test_double_single_drift_keeps_small_steps():
     assert np.all(moved0 == 0.0)  # each step is below half an ulp of the float position
 
 
-def test_precision_rejected_for_ensembles():
+def test_precision_accepted_for_ensembles_and_reset_by_set_systems():
+    """Double-single positions work inside ensembles (bit-identity per system:
+    test_gpu_ensemble.py); a new ensemble layout starts in float positions."""
     import bonsai2_b200 as B
     t = B.Treecode()
     t.set_systems(np.array([100, 200], np.int32))
-    assert t._L.bonsai_set_precision(t.handle, 1) == -4
+    assert t._L.bonsai_set_precision(t.handle, 1) == 0
+    t.set_systems(np.array([50, 50, 200], np.int32))
+    assert t._L.bonsai_set_precision(t.handle, 2) == -4  # modes are 0 and 1
     t.close()
 
 
