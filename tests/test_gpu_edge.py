@@ -144,6 +144,38 @@ def test_energy_drift_short_run(oracle, lib):
     assert abs(t.computeEnergies()[7] - 1.0) < 1e-6
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_leapfrog_time_reversible(precision):
+    """Kick-drift-kick with deterministic forces is time-reversible: K steps,
+    synchronised velocities reversed, K steps back, and the particles return
+    to their start up to rounding (amplified by the dynamics), for float and
+    double-single positions.  Checks the merged kicks, the pending closing
+    kick and its synchronisation together."""
+    import bonsai2_b200 as B
+    p, v = B.plummer(4096, 5)
+    p64 = p.astype(np.float64)
+    t = B.Treecode(eps=0.01, theta=0.5, dt=1.0 / 128)
+    t.set_precision(precision)
+    t.set_particles_f64(p64, v)
+    K = 32
+    t.step(K, graph=True)
+    t.sync_velocities()
+    x1, v1, _ = t.get_particles_f64()
+    t.set_particles_f64(x1, -v1)
+    t.step(K, graph=True)
+    t.sync_velocities()
+    x2, v2, _ = t.get_particles_f64()
+    assert t.synchronize() == 0
+    t.close()
+    moved = np.linalg.norm(x1[:, :3] - p64[:, :3], axis=1)
+    back = np.linalg.norm(x2[:, :3] - p64[:, :3], axis=1)
+    assert np.median(moved) > 1e-2
+    assert np.median(back) < 1e-3 * np.median(moved)
+    assert np.percentile(back, 99) < 1e-2 * np.median(moved)
+    dv = np.linalg.norm(v2[:, :3].astype(np.float64) + v[:, :3], axis=1)
+    assert np.median(dv) < 1e-3 * np.median(np.linalg.norm(v[:, :3], axis=1))
+
+
 def test_full_size_properties(lib):
     # BASELINE's large configuration: N = 2^24 Plummer, theta 0.4, eps 0.005
     import bonsai2_b200 as B
