@@ -81,6 +81,7 @@ def parse():
                     help="systems of the batching form reported beside the headline (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=32)
     ap.add_argument("--batch-autotune", type=int, default=1, help="autotune the ensemble's nLeaf/nCrit/layout (0: keep 16/64)")
+    ap.add_argument("--batch-ds", type=int, default=1, help="also time the ensemble with double-single positions (0: skip)")
     ap.add_argument("--eps", type=float, default=0.005)
     ap.add_argument("--nleaf", type=int, default=16)
     ap.add_argument("--ncrit", type=int, default=64)
@@ -957,6 +958,30 @@ def batching_form(B, L, a, device):
     fin = np.empty((n, 4), np.float32)
     L.bonsai_get_particles(t.handle, _p(fin), None, None)
     t.close()
+    # the same ensemble with double-single positions, every system moved to its
+    # own offset far from the origin (uniform in [-1e4, 1e4]^3), the same tuned
+    # parameters: its throughput and its cost against float positions
+    ds = None
+    if a.batch_ds:
+        shift = np.repeat(np.random.default_rng(7).uniform(-1.0e4, 1.0e4, (len(counts), 3)), counts, axis=0)
+        p64 = pos.astype(np.float64)
+        p64[:, :3] += shift
+        w = B.Treecode(**dict(prm, nleaf=nl, ncrit=nc))
+        w.set_walk_layout(lay)
+        w.set_systems(counts)
+        w.set_precision(1)
+        w.set_particles_f64(p64, vel)
+        w.step(2, graph=True)  # warm-up and graph capture
+        w.set_particles_f64(p64, vel)
+        ph2 = np.zeros(4 * a.batch_steps + 1, np.float32)
+        rc = L.bonsai_step_timed(w.handle, a.batch_steps, _p(ph2))
+        if rc:
+            raise B.BonsaiError(rc, "batching steps, double-single")
+        st2 = w.synchronize()
+        w.close()
+        ms2 = float(ph2[4 * a.batch_steps]) / a.batch_steps
+        ds = {"value": n / (ms2 * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": ms2, "cost_vs_float": ms2 / ms,
+              "status": int(st2), "offsets": "each system moved by U(-1e4, 1e4)^3"}
     off = np.concatenate([[0], np.cumsum(counts)])
     same = []
     for s in (0, int(np.argmax(counts)), len(counts) - 1):
@@ -979,7 +1004,7 @@ def batching_form(B, L, a, device):
             "kernels_per_step": int(nkern), "autotuned": {"nleaf": nl, "ncrit": nc, "walk_layout": lay,
                                                           "seconds": t_tune},
             "median_rel_force_err": float(np.median(err)), "p99_rel_force_err": float(np.percentile(err, 99)),
-            "bit_identical_to_alone": same, "status": int(status),
+            "bit_identical_to_alone": same, "status": int(status), "double_single": ds,
             "config": "512 Plummer spheres, N_s = floor(2^U(10,18)) seed 2024, theta 0.5, eps 0.01, dt 1/64"}
 
 
