@@ -86,7 +86,8 @@ void launch_walk64(int nblocks, const int2* groups, const TreeInfo* info, const 
                    const float4* jpos, const float4* jpos_lo, const uint4* cell_data, const float4* cell_open,
                    const float4* cell_lo, const float2* cell_ls, const float* group_inv_theta, const MpRec* rec,
                    double eps2, double4* acc, int* ring_pool, int ring_cap, unsigned* group_counter,
-                   unsigned long long* stats, int* status, cudaStream_t s);
+                   unsigned long long* stats, int* status, const int* sys_off, int nsys, const int* root_beg,
+                   cudaStream_t s);
 void launch_scatter_d4(const int* id, int n, const double4* in, double4* out, int nblocks, cudaStream_t s);
 
 // move.cu

@@ -1150,7 +1150,6 @@ int bonsai_compute_forces_fp64(bonsai_handle hh, double* acc4, unsigned long lon
   Handle* h = H(hh);
   if (!h) return BONSAI_ERR_HANDLE;
   if (!h->built || !h->mp_done || !h->grouped) return BONSAI_ERR_ORDER;
-  if (h->nsys > 1) return BONSAI_ERR_ARG;
   if (h->theta_mode == 1 && !h->forced) return BONSAI_ERR_ORDER;  // the network's angles come from compute_forces
   if (h->cur_ncrit > 128) return BONSAI_ERR_ARG;
   BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
@@ -1164,7 +1163,8 @@ int bonsai_compute_forces_fp64(bonsai_handle hh, double* acc4, unsigned long lon
   const int nblocks = h->ring_warps / (256 / 32);
   launch_walk64(nblocks, h->groups, h->info, h->pos[h->par], h->precision ? h->plo[h->par] : nullptr, h->jpos,
                 h->jlo, h->cell_data, h->cell_open, h->cell_lo, h->cell_ls, h->theta_mode ? h->group_inv : nullptr,
-                h->rec, e2, h->acc64, h->ring, kRingCap, h->group_counter, h->stats, &h->info->status, h->st);
+                h->rec, e2, h->acc64, h->ring, kRingCap, h->group_counter, h->stats, &h->info->status, h->so(),
+                h->nsys, h->root_beg, h->st);
   if (acc4) {
     launch_scatter_d4(h->id[h->par], h->n, h->acc64, h->acc64_tmp, h->nsm * 8, h->st);
     BONSAI_CUDA_TRY(cudaMemcpyAsync(acc4, h->acc64_tmp, (size_t)h->n * sizeof(double4), cudaMemcpyDeviceToHost, h->st));

@@ -62,12 +62,13 @@ __global__ void __launch_bounds__(kW64Threads) k_walk64(
     const uint4* __restrict__ cell_data, const float4* __restrict__ cell_open, const float4* __restrict__ cell_lo,
     const float2* __restrict__ cell_ls, const float* __restrict__ group_inv_theta, const MpRec* __restrict__ rec,
     double eps2, double4* __restrict__ acc, int* __restrict__ ring_pool, int ring_cap,
-    unsigned* __restrict__ group_counter, unsigned long long* __restrict__ stats, int* __restrict__ status) {
+    unsigned* __restrict__ group_counter, unsigned long long* __restrict__ stats, int* __restrict__ status,
+    const int* __restrict__ sys_off, int nsys, const int* __restrict__ root_beg) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   int* lists = ring_pool + (size_t)(blockIdx.x * kW64Warps + w) * (size_t)ring_cap;
   const int half_cap = ring_cap >> 1;
   const int ngroups = info->ngroups;
-  const int l1b = info->level_beg[1], l1e = info->level_end[1];
+  int l1b = info->level_beg[1], l1e = info->level_end[1];
   [[maybe_unused]] const int ncells = info->ncells, npart = info->npart;
   unsigned long long sum_app = 0, sum_dir = 0;
   unsigned max_app = 0, max_dir = 0;
@@ -82,6 +83,11 @@ __global__ void __launch_bounds__(kW64Threads) k_walk64(
         !BONSAI_IN_RANGE(pbeg, npart, 0x503))
       continue;
     const float inv_theta_g = PERGROUP ? group_inv_theta[g] : 0.0f;
+    if (nsys > 1) {  // an ensemble: the group's own system's level-1 cells
+      const int sy = sys_of(sys_off, nsys, pbeg);
+      l1b = __ldg(root_beg + sy);
+      l1e = __ldg(root_beg + sy + 1);
+    }
     float3 R = make_float3(0.f, 0.f, 0.f);
     if (DS) {
       const float4 r0 = ipos[pbeg];
@@ -226,11 +232,13 @@ void launch_walk64(int nblocks, const int2* groups, const TreeInfo* info, const 
                    const float4* jpos, const float4* jpos_lo, const uint4* cell_data, const float4* cell_open,
                    const float4* cell_lo, const float2* cell_ls, const float* group_inv_theta, const MpRec* rec,
                    double eps2, double4* acc, int* ring_pool, int ring_cap, unsigned* group_counter,
-                   unsigned long long* stats, int* status, cudaStream_t s) {
+                   unsigned long long* stats, int* status, const int* sys_off, int nsys, const int* root_beg,
+                   cudaStream_t s) {
 #define BONSAI_W64(DS, PG)                                                                                         \
   k_walk64<DS, PG><<<nblocks, kW64Threads, 0, s>>>(groups, info, ipos, ipos_lo, jpos, jpos_lo, cell_data,          \
                                                    cell_open, cell_lo, cell_ls, group_inv_theta, rec, eps2, acc,  \
-                                                   ring_pool, ring_cap, group_counter, stats, status)
+                                                   ring_pool, ring_cap, group_counter, stats, status, sys_off,    \
+                                                   nsys, root_beg)
   if (ipos_lo) {
     if (group_inv_theta) BONSAI_W64(true, true); else BONSAI_W64(true, false);
   } else {

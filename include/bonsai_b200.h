@@ -257,7 +257,7 @@ int bonsai_mlp_predict(int device, const float *X, int S, const float *w, float 
  * n x (ax, ay, az, phi) doubles in caller order; stats4 (optional): as
  * bonsai_get_stats.  Against the float walk the difference is rounding alone;
  * against bonsai_direct_fp64 it is multipole truncation alone.  Slow (a
- * checker).  Single systems, nCrit <= 128. */
+ * checker).  nCrit <= 128; in an ensemble each group walks its own system. */
 int bonsai_compute_forces_fp64(bonsai_handle h, double *acc4, unsigned long long *stats4);
 
 /* ---- Double-single positions (precision form) ----

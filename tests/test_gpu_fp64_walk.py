@@ -84,3 +84,40 @@ def test_per_group_angles_in_fp64_walk():
     assert np.array_equal(s_fixed, s_pg)
     assert np.array_equal(a_fixed.view(np.uint64), a_pg.view(np.uint64))
     t.close()
+
+
+def test_fp64_walk_inside_an_ensemble_is_per_system():
+    """In an ensemble every group's FP64 walk starts from its own system's
+    level-1 cells: the interaction lists are the float walk's, and each
+    system's FP64 forces are bit-identical to those it gets alone."""
+    import bonsai2_b200 as B
+    from bonsai2_b200.ensemble import plummer_ensemble
+    counts = np.array([300, 1, 2000, 57, 2], np.int32)
+    pos, vel = plummer_ensemble(counts, base_seed=41)
+    off = np.concatenate([[0], np.cumsum(counts)])
+
+    def run(t, p, v):
+        t.h_ptclPos[:] = p
+        t.h_ptclVel[:] = v
+        t.ptcl_h2d()
+        t.buildTree(16)
+        t.computeMultipoles()
+        t.makeGroups(5, 64)
+        t.computeForces(False)
+        s32 = _stats(t)
+        a64, s64 = t.compute_forces_fp64()
+        assert t.synchronize() == 0
+        assert np.array_equal(s32, s64)
+        return a64
+
+    t = B.Treecode(eps=0.01, theta=0.5)
+    t.set_systems(counts)
+    a_ens = run(t, pos, vel)
+    t.close()
+    for s in range(counts.shape[0]):
+        b, e = off[s], off[s + 1]
+        u = B.Treecode(eps=0.01, theta=0.5)
+        u.alloc(int(e - b))
+        a_alone = run(u, pos[b:e], vel[b:e])
+        u.close()
+        assert np.array_equal(a_ens[b:e].view(np.uint64), a_alone.view(np.uint64)), f"system {s}"
