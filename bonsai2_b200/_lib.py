@@ -53,6 +53,7 @@ SIGNATURES = {
     "bonsai_graph_kernel_count": (I, [P]),
     "bonsai_get_stats": (I, [P, P]),
     "bonsai_fp32_peak": (I, [I, P]),
+    "bonsai_binary_version": (I, [I, P, P]),
     "bonsai_selftest_wait_bound": (I, [I]),
     "bonsai_bounds_check": (I, [P, P, I]),
     "bonsai_bounds_selftest": (I, [I]),

@@ -14,6 +14,12 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+// sm_100a only: the device code uses sm_100 packed FP32 (FFMA2) and
+// redux.sync.f32, and no other target is built.
+#if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ != 1000 || !defined(__CUDA_ARCH_FEAT_SM100_ALL))
+#error "bonsai_b200 device code is compiled for sm_100a only (-gencode arch=compute_100a,code=sm_100a)"
+#endif
+
 namespace bonsai {
 
 constexpr int kMaxLevel = 21;        // 3 bits per level in a 63-bit key

@@ -125,6 +125,7 @@ __global__ void k_scatter_by_id(const int* __restrict__ id, int n, const float4*
                                 float4* __restrict__ out);
 __global__ void k_iota(int* __restrict__ a, int n);
 double fma_probe_tflops(int nsm, cudaStream_t st, float* scratch);
+int kernel_binary_version(int* binary_version, int* ptx_version);
 
 // Bounds-checked builds (-DBONSAI_CHECKS): the violation word (count, first
 // failing site) of each translation unit with guarded accesses; reset clears

@@ -185,7 +185,10 @@ void launch_move(float4* pos, float4* vel, const float4* acc, int n, float dt, i
 }
 
 // FP64 direct summation for sample particles (checker): grid (ceil(ns/256),
-// nsplit); thread = one sample, block = one slice of the sources.
+// nsplit); thread = one sample, block = one slice of the sources.  A sample
+// index outside [0, n) reads nothing: its partial sums are NaN, so its output
+// row is NaN (the allocation-free entry point passes caller device indices
+// that no host code has checked).
 __global__ void __launch_bounds__(256) k_direct_fp64(const float4* __restrict__ pos, int n,
                                                      const int* __restrict__ sample, int ns, double eps2,
                                                      int include_self, double* __restrict__ part,
@@ -194,7 +197,9 @@ __global__ void __launch_bounds__(256) k_direct_fp64(const float4* __restrict__ 
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   const int nsplit = gridDim.y;
   const int jb = (int)((long long)n * blockIdx.y / nsplit), je = (int)((long long)n * (blockIdx.y + 1) / nsplit);
-  const int i = s < ns ? sample[s] : 0;
+  const int si = s < ns ? sample[s] : 0;
+  const bool valid = si >= 0 && si < n;
+  const int i = valid ? si : 0;
   const float4 pi = pos[i];
   double xi = pi.x, yi = pi.y, zi = pi.z;
   if (lo) {
@@ -228,6 +233,7 @@ __global__ void __launch_bounds__(256) k_direct_fp64(const float4* __restrict__ 
     }
   }
   if (s < ns) {
+    if (!valid) ax = ay = az = ph = __longlong_as_double(0x7ff8000000000000LL);
     double* o = part + ((size_t)blockIdx.y * ns + s) * 4;
     o[0] = ax; o[1] = ay; o[2] = az; o[3] = ph;
   }
@@ -539,6 +545,17 @@ double fma_probe_tflops(int nsm, cudaStream_t st, float* scratch) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return best_tf;
+}
+
+// The architecture the loaded device code was compiled for (binaryVersion
+// 100 = sm_100), read from one of this library's kernels at run time.
+int kernel_binary_version(int* binary_version, int* ptx_version) {
+  cudaFuncAttributes a;
+  const cudaError_t e = cudaFuncGetAttributes(&a, k_fma_probe);
+  if (e != cudaSuccess) return -(int)e - 1000;
+  *binary_version = a.binaryVersion;
+  *ptx_version = a.ptxVersion;
+  return 0;
 }
 
 // Self-test of the checked build's machinery: index n of a logical length n,

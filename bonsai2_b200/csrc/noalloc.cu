@@ -13,15 +13,20 @@
 // Limits and sharing:
 //   * capacity kNoAllocDoubles doubles (2 MiB): ns <= 65536 samples; larger
 //     requests return BONSAI_ERR_TOO_LARGE without launching anything;
+//   * sample indices must lie in [0, n); the kernel reads no particle for an
+//     index outside that range and writes a NaN row for it instead;
+//   * with include_self the i == j term is summed, so eps2 must be > 0 (at
+//     eps2 = 0 that term is 0/0): eps2 <= 0 with include_self returns
+//     BONSAI_ERR_ARG;
 //   * all calls share the array.  Every entry a call reads is written by the
 //     same call first, so nothing has to start at zero, but two calls whose
 //     kernels overlap on the GPU (different streams, or different host
 //     threads) race on it and give wrong results: serialise them;
-//   * the first call on a device looks up the array's device address with
-//     cudaGetSymbolAddress (with that device current) and caches it; make that
-//     first call before any stream capture on that device.
-#include <mutex>
-
+//   * every call looks up the array's device address with
+//     cudaGetSymbolAddress on the current device (nothing is cached, so a
+//     device reset or a new context is harmless).  The first call on a device
+//     may load the library's device code there; make it before any stream
+//     capture on that device.
 #include "../../include/bonsai_b200.h"
 #include "common.cuh"
 #include "kernels.cuh"
@@ -30,28 +35,17 @@ namespace {
 
 constexpr int kNoAllocDoubles = 1 << 18;  // 2 MiB of FP64 partial sums
 constexpr int kNoAllocMaxSamples = kNoAllocDoubles / 4;
-constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) double g_direct_scratch[kNoAllocDoubles];
 
-// the array's address on each device (host code cannot use the symbol itself:
-// on the host it only names a stand-in, not device memory)
-double* g_scratch_addr[kMaxDevices] = {nullptr};
-std::mutex g_scratch_mu;
-
+// The array's address on the current device.  Host code cannot pass the
+// symbol itself to a kernel: on the host it only names a stand-in, not device
+// memory.
 int scratch_for_current_device(double** out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_direct_scratch);
   if (e != cudaSuccess) return -(int)e - 1000;
-  if (dev < 0 || dev >= kMaxDevices) return BONSAI_ERR_ARG;
-  std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_direct_scratch);
-    if (e != cudaSuccess) return -(int)e - 1000;
-    g_scratch_addr[dev] = static_cast<double*>(p);
-  }
-  *out = g_scratch_addr[dev];
+  *out = static_cast<double*>(p);
   return 0;
 }
 
@@ -60,6 +54,7 @@ int scratch_for_current_device(double** out) {
 extern "C" int bonsai_direct_fp64_noalloc(const float* d_pos4, int n, const int* d_sample, int ns, double eps2,
                                           int include_self, double* d_out, void* stream) {
   if (!d_pos4 || !d_sample || !d_out || n < 1 || ns < 1 || !(eps2 >= 0.0)) return BONSAI_ERR_ARG;
+  if (include_self && !(eps2 > 0.0)) return BONSAI_ERR_ARG;  // the i == j term would be 0/0
   if (ns > kNoAllocMaxSamples) return BONSAI_ERR_TOO_LARGE;
   double* scratch = nullptr;
   const int rc = scratch_for_current_device(&scratch);

@@ -1732,6 +1732,12 @@ int bonsai_fp32_peak(int device, double* tflops) {
   return last_cuda();
 }
 
+int bonsai_binary_version(int device, int* binary_version, int* ptx_version) {
+  if (!binary_version || !ptx_version) return BONSAI_ERR_ARG;
+  BONSAI_CUDA_TRY(cudaSetDevice(device));
+  return kernel_binary_version(binary_version, ptx_version);
+}
+
 void* bonsai_host_alloc(size_t bytes) {
   void* p = nullptr;
   if (cudaMallocHost(&p, bytes) != cudaSuccess) return nullptr;

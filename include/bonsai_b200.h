@@ -161,6 +161,10 @@ int bonsai_bounds_selftest(int device);
 /* measured FP32 FMA throughput of the device (TFLOP/s; the faster of scalar
  * FFMA and packed FFMA2 chains): the walk's roofline */
 int bonsai_fp32_peak(int device, double *tflops);
+/* the architecture of the device code loaded on `device`, read at run time
+ * from one of the library's kernels (cudaFuncGetAttributes): binary_version
+ * 100 = sm_100 SASS; ptx_version 0 when no PTX was embedded */
+int bonsai_binary_version(int device, int *binary_version, int *ptx_version);
 /* Wait for the handle's stream and its copy streams; returns the sticky device
  * status (and clears it). */
 int bonsai_synchronize(bonsai_handle h);
@@ -208,13 +212,17 @@ int bonsai_direct_fp64(bonsai_handle h, const int *sample, int ns, int include_s
  * (their GPU memory belongs to another framework's allocator, or their loop
  * must not pay cudaMalloc's device-wide synchronisation).  No counterpart in
  * the reference.  All pointers are device memory: d_pos4 = n float4 (x,y,z,m),
- * d_sample = ns particle indices, d_out = double[4*ns] (ax, ay, az, phi);
- * eps2 = softening squared; stream = a cudaStream_t (NULL: the legacy default
- * stream).  Allocates nothing: its scratch is a fixed 2 MiB device array in
- * the library, so ns <= 65536 (larger: BONSAI_ERR_TOO_LARGE).  Calls share
- * that array: calls that overlap on the GPU race and must be serialised.  The
- * first call on a device looks the array up (cudaGetSymbolAddress); make it
- * before any stream capture on that device.  Asynchronous on `stream`. */
+ * d_sample = ns particle indices, each in [0, n) (an index outside that range
+ * reads nothing and gets a NaN output row), d_out = double[4*ns] (ax, ay, az,
+ * phi); eps2 = softening squared, > 0 when include_self is set (the i == j
+ * term; eps2 <= 0 then returns BONSAI_ERR_ARG); stream = a cudaStream_t
+ * (NULL: the legacy default stream).  Allocates nothing: its scratch is a
+ * fixed 2 MiB device array in the library, so ns <= 65536 (larger:
+ * BONSAI_ERR_TOO_LARGE).  Calls share that array: calls that overlap on the
+ * GPU race and must be serialised.  Every call looks the array up on the
+ * current device (cudaGetSymbolAddress); the first call on a device may load
+ * the library's device code, so make it before any stream capture on that
+ * device.  Asynchronous on `stream`. */
 int bonsai_direct_fp64_noalloc(const float *d_pos4, int n, const int *d_sample, int ns, double eps2,
                                int include_self, double *d_out, void *stream);
 

@@ -9,9 +9,16 @@
 # computeMultipoles.cu / computeForces.cu use pre-Volta shuffles and legacy
 # textures).
 # Same flags as the reference's own Makefile for host code (code/Makefile:9-10).
+# This recipe is the one file that names the reference tree's location: the
+# environment variable BONSAI_REFERENCE, else /root/reference.  Without the
+# tree it builds nothing and says so (the GPU box only uses prebuilt files).
 set -e
 REF=${BONSAI_REFERENCE:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
+if [ ! -d "$REF/code" ]; then
+  echo "build_ref.sh: no reference tree at $REF (set BONSAI_REFERENCE); oracle/_ref not built"
+  exit 0
+fi
 mkdir -p "$HERE/_ref"
 g++ -O3 -Wall -I"$REF/code" "$HERE/ref_plummer_main.cpp" -o "$HERE/_ref/ref_plummer"
 echo "built $HERE/_ref/ref_plummer"

@@ -45,11 +45,21 @@ def test_bounds_check_of_normal_build_needs_no_device(lib):
     assert lib.bonsai_error_string(128)
 
 
-def test_library_is_built_for_sm100a(lib):
-    from bonsai2_b200 import _lib
-    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", _lib.LIB_PATH],
-                         capture_output=True, text=True).stdout
-    assert "sm_100a" in out
+def test_library_is_built_for_sm100a_only(lib):
+    # the recipe compiles for sm_100a alone; common.cuh refuses to compile
+    # device code for any other target, so a library that built is sm_100a
+    from bonsai2_b200 import build
+    assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+    guard = open(os.path.join(ROOT, "bonsai2_b200", "csrc", "common.cuh")).read()
+    assert "__CUDA_ARCH_FEAT_SM100_ALL" in guard and "#error" in guard
+
+
+@pytest.mark.gpu
+def test_loaded_device_code_is_sm100(lib):
+    # read at run time from one of the library's own kernels
+    b, p = ctypes.c_int(0), ctypes.c_int(-1)
+    assert lib.bonsai_binary_version(0, ctypes.byref(b), ctypes.byref(p)) == 0
+    assert b.value == 100, b.value
 
 
 def test_create_without_gpu_fails_loudly(lib):
