@@ -31,7 +31,11 @@ state, 1.3 GB, is larger than the 126 MB L2, so no flush is needed).
             of groups extrapolated to all groups.
 
 Multi-GPU (torchrun): independent replicas, one per GPU (the single-system
-step has no exchange step); max of the device times over ranks.
+step has no exchange step); max of the device times over ranks.  Beside it,
+`batching_split`: the batching ensemble's systems partitioned over the ranks
+by estimated work, each rank advancing only its own systems, no data-path
+collective, per-system energies gathered to rank 0 at the end (strong
+scaling of the fixed 512-system ensemble).
 """
 from __future__ import annotations
 
@@ -82,6 +86,8 @@ def parse():
     ap.add_argument("--batch-steps", type=int, default=32)
     ap.add_argument("--batch-autotune", type=int, default=1, help="autotune the ensemble's nLeaf/nCrit/layout (0: keep 16/64)")
     ap.add_argument("--batch-ds", type=int, default=1, help="also time the ensemble with double-single positions (0: skip)")
+    ap.add_argument("--split-emulate", type=int, default=0,
+                    help="on one GPU, run the split batching form's ranks one after another (a check of the split)")
     ap.add_argument("--eps", type=float, default=0.005)
     ap.add_argument("--nleaf", type=int, default=16)
     ap.add_argument("--ncrit", type=int, default=64)
@@ -223,10 +229,11 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU restatement of the reference (oracle/), bounded sample
 # ---------------------------------------------------------------------------
-def cpu_reference_step(O, pos, vel, a, rng):
-    """One step of the reference algorithm on the host cores; the walk runs on
-    a random sample of groups and is extrapolated.  Returns (seconds per full
-    step (estimated), description)."""
+def cpu_reference_step(O, pos, vel, a, rng, full=False):
+    """One step of the reference algorithm on the host cores.  full: the walk
+    covers every group (a measured step); otherwise it runs on a random
+    sample of cpu_group_fraction of the groups and is extrapolated.  Returns
+    (seconds per full step (measured, or estimated), description)."""
     t0 = time.perf_counter()
     S = O.OracleStep(pos, theta=a.theta, eps=a.eps, nleaf=a.nleaf, ncrit=a.ncrit, level_split=a.level_split)
     S.build()
@@ -236,22 +243,30 @@ def cpu_reference_step(O, pos, vel, a, rng):
     S.groups()
     t3 = time.perf_counter()
     G = len(S.gbeg)
-    gs = max(1, int(round(G * a.cpu_group_fraction)))
-    sel = np.sort(rng.choice(G, gs, replace=False)).astype(np.int32)
+    if full:
+        gs, sel = G, None
+    else:
+        gs = max(1, int(round(G * a.cpu_group_fraction)))
+        sel = np.sort(rng.choice(G, gs, replace=False)).astype(np.int32)
     S.forces(gsel=sel)
     t4 = time.perf_counter()
     acc = np.zeros_like(pos)
-    acc[S.ph_perm] = S.acc
+    if full:
+        acc[S.ph_perm] = S.acc
     p2, v2 = pos.copy(), vel.copy()
     O.move(p2, v2, acc, a.dt, True, a.eps)
     t5 = time.perf_counter()
-    frac = S.gnp[sel].sum() / float(pos.shape[0])
+    frac = 1.0 if full else S.gnp[sel].sum() / float(pos.shape[0])
     walk_full = (t4 - t3) / frac
     total = (t1 - t0) + (t2 - t1) + (t3 - t2) + walk_full + (t5 - t4)
-    desc = ("full-N box+keys+sort+tree %.2fs, multipoles %.2fs, groups %.2fs; walk of %d/%d groups "
-            "(%.3f%% of particles) %.2fs extrapolated to %.1fs; move %.2fs"
-            % (t1 - t0, t2 - t1, t3 - t2, gs, G, 100 * frac, t4 - t3, walk_full, t5 - t4))
-    return total, desc
+    if full:
+        desc = ("full-N box+keys+sort+tree %.2fs, multipoles %.2fs, groups %.2fs, walk of all %d groups %.2fs, "
+                "move %.2fs (measured, nothing extrapolated)" % (t1 - t0, t2 - t1, t3 - t2, G, t4 - t3, t5 - t4))
+    else:
+        desc = ("full-N box+keys+sort+tree %.2fs, multipoles %.2fs, groups %.2fs; walk of %d/%d groups "
+                "(%.3f%% of particles) %.2fs extrapolated to %.1fs; move %.2fs"
+                % (t1 - t0, t2 - t1, t3 - t2, gs, G, 100 * frac, t4 - t3, walk_full, t5 - t4))
+    return total, desc, S
 
 
 def reference_gpu_make_groups(O, pos, a, reps=10):
@@ -290,6 +305,55 @@ def reference_gpu_make_groups(O, pos, a, reps=10):
                     % (a.level_split, a.ncrit)}
 
 
+def reference_gpu_walk(S, a, reps=3):
+    """The reference's own multipoles and tree walk (code/computeMultipoles.cu,
+    code/computeForces.cu: the "modified reference" with mechanical sm_100a
+    shims, oracle/_ref/ref_walk), timed with CUDA events around
+    Treecode<float>::computeMultipoles and ::computeForces on the tree of the
+    CPU restatement's step S (the reference's comparison-partition octree and
+    groups, which the reference's CDP build cannot produce on sm_100)."""
+    import tempfile
+    from oracle import ref_walk as RW
+    if not RW.available():
+        return {"unavailable": "oracle/_ref/ref_walk not built (oracle/build_ref.sh needs the reference tree)"}
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return {"unavailable": "no GPU"}
+    except ImportError:
+        return {"unavailable": "no torch to probe for a GPU"}
+    T = S.tree
+    tree = {"cell_data": T.cell_data(), "size": S.size4, "mono": S.mono4, "quad0": S.quad0, "quad1": S.quad1,
+            "l1": (int(T.level_beg[1]), int(T.level_end[1])),
+            "groups": np.stack([S.gbeg, S.gnp], 1).astype(np.int32), "ipos": S.ipos, "jpos": S.jpos}
+    if int(np.max(S.gnp)) > 64:
+        return {"unavailable": "groups larger than the reference walk's 64 particles"}
+    eps2 = float(np.float32(np.float32(a.eps) * np.float32(a.eps)))
+    with tempfile.TemporaryDirectory() as dd:
+        inp = os.path.join(dd, "tree.in")
+        RW.write_input(inp, tree, a.theta, eps2, a.ncrit)
+        info = RW.time_walk(inp, reps)
+    if "unavailable" in info:
+        return info
+    n = S.pos4.shape[0]
+    flops = (20.0 * info["direct_mean"] + 64.0 * info["approx_mean"]) * n
+    return {"walk_ms": info["walk_ms_min"], "walk_ms_median": info["walk_ms_median"],
+            "multipoles_ms": info["multipoles_ms_min"], "walk_tflops": flops / (info["walk_ms_min"] * 1e-3) / 1e12,
+            "interactions_per_particle": {"approx": info["approx_mean"], "direct": info["direct_mean"],
+                                          "max_approx": info["approx_max"], "max_direct": info["direct_max"]},
+            "cells": info["cells"], "groups": info["groups"], "reps": info["reps"],
+            "what": "code/computeForces.cu + code/computeMultipoles.cu with mechanical sm_100a shims (sync "
+                    "shuffles, bounds-checked loads for textures, __syncwarp at warp exchanges), the reference's "
+                    "launch (104 blocks x 128 threads, NI=2), on the comparison-partition tree of the same input; "
+                    "CUDA events around the public Treecode calls, best of %d" % info["reps"]}
+
+
+def bench_config(a, world):
+    """The workload description, the same in both arms."""
+    return {"workload": workload(a), "n_per_gpu": a.n, "parallelism": "replicas x%d" % world,
+            "l2": "no flush: particle state 1.3 GB > 126 MB L2"}
+
+
 def run_reference(a):
     d = Dist("gloo")
     if d.rank != 0:
@@ -302,23 +366,32 @@ def run_reference(a):
     # threads would slow the reference's host-side allocations)
     ref_gpu = reference_gpu_make_groups(O, pos, a)
     rng = np.random.default_rng(1)
-    times = []
-    desc = ""
-    for s in range(a.warmup + a.steps):
-        t, desc = cpu_reference_step(O, pos, vel, a, rng)
-        if s >= a.warmup:
-            times.append(t)
-    tm = statistics.mean(times)
+    # warm-up: sampled steps (the walk of cpu_group_fraction of the groups,
+    # extrapolated), reported beside the measurement as an estimate
+    est = []
+    est_desc = ""
+    for s in range(a.warmup):
+        t, est_desc, _ = cpu_reference_step(O, pos, vel, a, rng)
+        est.append(t)
+    # timed: one full step, every group walked -- the whole configuration,
+    # so one step is what fits the run; steps = full steps timed
+    tm, desc, S = cpu_reference_step(O, pos, vel, a, rng, full=True)
+    ref_walk = reference_gpu_walk(S, a)
     v = a.n / tm / 1e6
     cores = O.num_threads()
-    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": 1, "warmup": a.warmup,
+            "steps_requested": a.steps,
             "ms_per_step": tm * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic: seeded Plummer sphere (plummer.h algorithm)",
-            "config": {"workload": workload(a), "n": a.n}, "impl": "reference",
+            "config": bench_config(a, a.gpus), "impl": "reference",
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": "per step: " + desc},
+                             "sample": "one full step, nothing sampled: " + desc},
+            "cpu_sampled_estimate": ({"value": a.n / statistics.mean(est) / 1e6, "unit": UNIT, "steps": len(est),
+                                      "extrapolated": True, "sample": "warm-up steps: " + est_desc}
+                                     if est else None),
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "reference_gpu_make_groups": ref_gpu}
+            "reference_gpu_make_groups": ref_gpu,
+            "reference_gpu_walk": ref_walk}
     print(json.dumps(line), flush=True)
     d.close()
 
@@ -436,6 +509,12 @@ def run_ours(a):
     # the forms beside the headline run on a single GPU only (under torchrun
     # every rank reports the replicated headline and leaves together)
     solo = d.rank == 0 and d.world == 1
+    # the batching ensemble split across the ranks (every rank takes part)
+    split = None
+    if a.batch_systems > 0 and d.world > 1:
+        split = batching_split_form(B, L, a, d)
+    elif solo and a.batch_systems > 0 and a.split_emulate > 1:
+        split = batching_split_form(B, L, a, d, emulate_world=a.split_emulate)
     sweep = theta_sweep(B, L, pos, vel, a, d.local) if (solo and a.sweep) else None
     learned = learned_theta(B, L, pos, vel, a, d.local, sweep) if (solo and a.learned_target > 0) else None
     batching = batching_form(B, L, a, d.local) if (solo and a.batch_systems > 0) else None
@@ -450,7 +529,7 @@ def run_ours(a):
     if d.rank == 0 and d.world == 1 and not a.no_cpu_baseline:
         from oracle import oracle as O
         O.build()
-        tcpu, desc = cpu_reference_step(O, p0, v0, a, np.random.default_rng(1))
+        tcpu, desc, _ = cpu_reference_step(O, p0, v0, a, np.random.default_rng(1))
         cpu = {"value": n / tcpu / 1e6, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
                "sample": "one step: " + desc}
 
@@ -460,8 +539,8 @@ def run_ours(a):
             "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32",
             "data": "synthetic: seeded Plummer sphere (plummer.h algorithm), N per GPU",
-            "config": {"workload": workload(a), "n_per_gpu": n, "parallelism": "replicas x%d" % d.world,
-                       "l2": "no flush: particle state 1.3 GB > 126 MB L2", "graph": "captured CUDA graphs"},
+            "config": bench_config(a, d.world),
+            "execution": "captured CUDA graphs",
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": float(peak.value), "unit": "TFLOP/s",
                          "frac": achieved / float(peak.value),
                          "traffic": WALK_DRAM_BYTES_2P22 * n / 4194304 if abs(a.theta - 0.6) < 1e-6 else None,
@@ -490,6 +569,7 @@ def run_ours(a):
             "theta_sweep": sweep,
             "learned_theta": learned,
             "batching": batching,
+            "batching_split": split,
             "autotuned_headline": tuned,
             "octree_build": octree,
             "group_formation": grouping,
@@ -1006,6 +1086,74 @@ def batching_form(B, L, a, device):
             "median_rel_force_err": float(np.median(err)), "p99_rel_force_err": float(np.percentile(err, 99)),
             "bit_identical_to_alone": same, "status": int(status), "double_single": ds,
             "config": "512 Plummer spheres, N_s = floor(2^U(10,18)) seed 2024, theta 0.5, eps 0.01, dt 1/64"}
+
+
+def batching_split_form(B, L, a, d, emulate_world=0):
+    """The batching form split across the ranks: the ensemble's systems are
+    partitioned by estimated work (bonsai2_b200.ensemble.partition_systems),
+    every rank generates and advances only its own systems as an ensemble of
+    its own (nLeaf 16, nCrit 64, the half-warp layout on every rank, so that
+    each system's result equals the one-process run), with no data-path
+    collective; the device time is the max over ranks, and the only exchange is
+    the final gather of per-system energies to rank 0.  Fixed total work
+    (strong scaling).  emulate_world > 1 runs that many ranks one after another
+    in this process on one GPU (a check of the split, not a scaling number)."""
+    from bonsai2_b200.ensemble import gather_systems, partition_systems, plummer_ensemble, shard, system_sizes
+    from bonsai2_b200.treecode import _p
+    counts = system_sizes(a.batch_systems, 1 << 10, 1 << 18, seed=2024)
+    world = emulate_world if emulate_world > 1 else d.world
+    parts = partition_systems(counts, world)
+    ranks = range(world) if emulate_world > 1 else [d.rank]
+    prm = dict(eps=0.01, theta=0.5, ncrit=64, nleaf=16, level_split=a.level_split, dt=1.0 / 64,
+               device=d.local)
+    ms_rank, energies, sys_rank = [], [], []
+    for r in ranks:
+        mine = parts[r]
+        cr = counts[mine].astype(np.int32)
+        pos, vel = plummer_ensemble(cr, seeds=a.seed + mine)
+        nr = int(cr.sum())
+        t = B.Treecode(**prm)
+        t.set_systems(cr)
+        L.bonsai_set_particles(t.handle, _p(pos), _p(vel), nr)
+        t.step(max(a.warmup, 1), graph=True)  # warm-up and graph capture
+        L.bonsai_set_particles(t.handle, _p(pos), _p(vel), nr)
+        ph = np.zeros(4 * a.batch_steps + 1, np.float32)
+        if emulate_world <= 1:
+            d.barrier()
+        rc = L.bonsai_step_timed(t.handle, a.batch_steps, _p(ph))
+        st = t.synchronize()
+        if rc or st:
+            raise B.BonsaiError(rc or st, "split batching steps")
+        ms_rank.append(float(ph[4 * a.batch_steps]) / a.batch_steps)
+        t.computeEnergies()
+        energies.append(t.system_energies())
+        sys_rank.append(mine)
+        t.close()
+    if emulate_world > 1:
+        ms = max(ms_rank)
+        E = gather_systems(None, np.concatenate(sys_rank), np.concatenate(energies), len(counts))
+        per_rank = ms_rank
+    else:
+        ms = d.max(ms_rank[0])
+        E = gather_systems(d.pg, sys_rank[0], energies[0], len(counts))
+        per_rank = [None] * d.world
+        if d.pg:
+            d.pg.all_gather_object(per_rank, ms_rank[0])
+        else:
+            per_rank = ms_rank
+    if d.rank != 0:
+        return None
+    W = [float(np.sum(counts[p] * np.log2(np.maximum(counts[p], 2)))) for p in parts]
+    n = int(counts.sum())
+    return {"value": n / (ms * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": ms, "scaling": "strong",
+            "ranks": world, "emulated_on_one_gpu": emulate_world > 1, "systems": int(len(counts)), "particles": n,
+            "systems_per_rank": [int(len(p)) for p in parts],
+            "particles_per_rank": [int(counts[p].sum()) for p in parts],
+            "estimated_work_imbalance": max(W) / (sum(W) / len(W)),
+            "ms_per_step_per_rank": per_rank, "steps": a.batch_steps,
+            "energies_gathered": int(E.shape[0]), "total_energy_sum": float(E[:, 3].sum()),
+            "config": "512 Plummer spheres, N_s = floor(2^U(10,18)) seed 2024, theta 0.5, eps 0.01, dt 1/64, "
+                      "nLeaf 16, nCrit 64; systems partitioned by N log2 N (longest first)"}
 
 
 def main():

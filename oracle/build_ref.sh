@@ -34,3 +34,16 @@ if [ -x "${NVCC:-/usr/local/cuda/bin/nvcc}" ]; then
     "$HERE/ref_groups_main.cu" -o "$HERE/_ref/ref_groups"
   echo "built $HERE/_ref/ref_groups"
 fi
+# The "modified reference" walk and multipoles: code/computeForces.cu and
+# code/computeMultipoles.cu (+ code/cuda_primitives.h), copied into
+# oracle/_ref/modref/ with the mechanical sm_100a shims of make_modref.py, in
+# the harness ref_walk_main.cu.  The reference's nvcc flags for the walk
+# (code/Makefile:53-54: -ftz=true, -rdc=true), sm_100a for sm_35, and -DNDEBUG
+# so that the walk's device assert (computeForces.cu:565) returns its
+# stack-full sentinel instead of trapping.
+if [ -x "${NVCC:-/usr/local/cuda/bin/nvcc}" ]; then
+  "${PYTHON:-python3}" "$HERE/make_modref.py" "$REF/code" "$HERE/_ref/modref"
+  "${NVCC:-/usr/local/cuda/bin/nvcc}" -g -O3 -gencode arch=compute_100a,code=sm_100a -rdc=true -ftz=true -DNDEBUG -w \
+    -I"$REF/code" -I"$HERE" "$HERE/ref_walk_main.cu" -o "$HERE/_ref/ref_walk"
+  echo "built $HERE/_ref/ref_walk"
+fi

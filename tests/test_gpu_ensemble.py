@@ -286,3 +286,46 @@ def test_ensemble_512_systems_spot_check():
         assert np.array_equal(p[b:e].view(np.uint32), pa.view(np.uint32))
         assert np.array_equal(a[b:e].view(np.uint32), aa.view(np.uint32))
     t.close()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_split_ensemble_bit_identical_to_one_process(world):
+    """The multi-GPU split of the batching form, its ranks run one after
+    another on this GPU: each rank's shard (systems partitioned by work,
+    generated by their global seeds) advanced as its own ensemble gives every
+    system, bit for bit, its result in the one-process ensemble; the gathered
+    per-system energies equal the one-process ones to FP64 rounding."""
+    import bonsai2_b200 as B
+    from bonsai2_b200.ensemble import gather_systems, partition_systems, plummer_ensemble, system_sizes
+    counts = np.concatenate([[1, 2], system_sizes(22, 1 << 8, 1 << 14, seed=9)]).astype(np.int32)
+    pos, vel = plummer_ensemble(counts, base_seed=31)
+    steps = 3
+    t = B.Treecode(**PARAMS)
+    t.set_systems(counts)
+    p, v, a, _ = _run(t, pos, vel, steps, eager=False)
+    t.computeEnergies()
+    es = t.system_energies()
+    t.close()
+    off = _offsets(counts)
+    parts = partition_systems(counts, world)
+    rows, owners = [], []
+    for r in range(world):
+        mine = parts[r]
+        cr = counts[mine].astype(np.int32)
+        pr, vr = plummer_ensemble(cr, seeds=31 + mine)
+        u = B.Treecode(**PARAMS)
+        u.set_systems(cr)
+        pu, vu, au, _ = _run(u, pr, vr, steps, eager=False)
+        u.computeEnergies()
+        rows.append(u.system_energies())
+        owners.append(mine)
+        u.close()
+        loff = _offsets(cr)
+        for k, s in enumerate(mine):
+            b, e = off[s], off[s + 1]
+            lb, le = loff[k], loff[k + 1]
+            assert np.array_equal(pu[lb:le].view(np.uint32), p[b:e].view(np.uint32)), f"positions of system {s}"
+            assert np.array_equal(vu[lb:le].view(np.uint32), v[b:e].view(np.uint32)), f"velocities of system {s}"
+            assert np.array_equal(au[lb:le].view(np.uint32), a[b:e].view(np.uint32)), f"accelerations of system {s}"
+    E = gather_systems(None, np.concatenate(owners), np.concatenate(rows), len(counts))
+    np.testing.assert_allclose(E, es, rtol=1e-12, atol=1e-15)
