@@ -70,7 +70,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--particles", type=int, default=1 << 24, dest="n")
     ap.add_argument("--theta", type=float, default=0.6)
-    ap.add_argument("--sweep", default="0.3,0.4,0.5,0.6,0.7,0.8", help="thetas of the sweep reported beside the headline")
+    ap.add_argument("--sweep", default="0.3,0.4,0.5,0.6,0.7,0.8,0.9,1.0",
+                    help="thetas of the sweep reported beside the headline")
     ap.add_argument("--learned-target", type=float, default=1e-3,
                     help="per-group error target of the learned opening angles (0: skip the learned form)")
     ap.add_argument("--precision-n", type=int, default=1 << 26,
@@ -579,8 +580,7 @@ def run_ours(a):
         }
         if learned:
             learned["vs_fixed_headline"] = learned["value"] / value
-            for k in ("fp32", "double_single"):
-                learned["calibrated"][k]["vs_fixed_headline"] = learned["calibrated"][k]["value"] / value
+            learned["double_single"]["vs_fixed_headline"] = learned["double_single"]["value"] / value
         print(json.dumps(line), flush=True)
     for hptr in (hp, hv, ha):
         L.bonsai_host_free(hptr)
@@ -630,23 +630,25 @@ def theta_sweep(B, L, pos, vel, a, device):
 
 
 def learned_theta(B, L, pos, vel, a, device, sweep):
-    """The learned form: per-group opening angles from the MLP, trained on a
-    Plummer sphere of another seed (untimed setup), then timed on the bench
-    system like the headline and judged against the FP64 direct sum; compared
-    with the fixed angles of the sweep at equal median and equal p99 error.
-    Reported raw, and calibrated (one scale on the network's angles, set by
-    bisection on the training system to 0.9 x the target median error) in
-    float and double-single positions."""
+    """The learned form: per-group opening bounds from the MLP (relative
+    accuracy mode, bonsai2_b200.learned), trained on a Plummer sphere of
+    another seed and calibrated there (one shift of the output range, by
+    bisection to 0.9 x the target median error; untimed setup), then timed on
+    the bench system like the headline and judged against the FP64 direct
+    sum; compared with the fixed angles of the sweep at equal median and
+    equal p99 error, with the fastest fixed angle that meets the target, and
+    with the relative mode's single-parameter form (tau = alpha A_g) at the
+    same median.  Float and double-single positions."""
     from bonsai2_b200 import learned as Lr
     n = pos.shape[0]
     t0 = time.perf_counter()
     ptr, vtr = B.plummer(n, a.seed + 1)
-    X, y, _ = Lr.training_set(ptr, vtr, eps=a.eps, target=a.learned_target, max_groups=8192, nleaf=a.nleaf,
-                              ncrit=a.ncrit, level_split=a.level_split, device=device)
-    w, loss = Lr.train(X, y, epochs=3000, lr=3e-3, device=device)
+    X, y, _ = Lr.relative_training_set(ptr, vtr, eps=a.eps, target=a.learned_target, max_groups=8192,
+                                       nleaf=a.nleaf, ncrit=a.ncrit, level_split=a.level_split, device=device)
+    w, loss = Lr.train(X, y, epochs=3000, lr=3e-3, lo=Lr.YLO, hi=Lr.YHI, device=device)
+    c, lo, hi, e_cal = Lr.calibrate_relative(ptr, vtr, w, a.eps, a.learned_target, nleaf=a.nleaf, ncrit=a.ncrit,
+                                             level_split=a.level_split, device=device)
     t_train = time.perf_counter() - t0
-    c, lo, hi, e_cal = Lr.calibrate(ptr, vtr, w, a.eps, a.learned_target, nleaf=a.nleaf, ncrit=a.ncrit,
-                                    level_split=a.level_split, device=device)
     del ptr, vtr
     rng = np.random.default_rng(2048)
     samp = np.ascontiguousarray(np.sort(rng.choice(n, min(2048, n), replace=False)).astype(np.int32))
@@ -658,45 +660,102 @@ def learned_theta(B, L, pos, vel, a, device, sweep):
     ref = t.direct_fp64(samp, include_self=True)
     t.close()
     kw = dict(theta=a.theta, eps=a.eps, device=device, nleaf=a.nleaf, ncrit=a.ncrit, level_split=a.level_split,
-              dt=a.dt, steps=a.steps, weights=w)
-
-    def compare(r):
-        if sweep:
-            em = at_equal(sweep, "value", "median_rel_force_err", r["median_rel_force_err"])
-            ep = at_equal(sweep, "value", "p99_rel_force_err", r["p99_rel_force_err"])
-            r["fixed_theta_value_at_equal_median"] = em
-            r["fixed_theta_value_at_equal_p99"] = ep
-            r["gain_at_equal_median"] = r["value"] / em if em else None
-            r["gain_at_equal_p99"] = r["value"] / ep if ep else None
-        return r
-
-    out = compare(measure(B, L, pos, vel, samp, ref, **kw))
+              dt=a.dt, steps=a.steps)
+    out = compare_to_sweep(measure(B, L, pos, vel, samp, ref, weights=w, y_range=(lo, hi), **kw), sweep,
+                           a.learned_target)
     out["unit"] = UNIT
     out["target"] = a.learned_target
+    out["mode"] = ("relative: a cell passing the geometric test at theta %.2f is opened when M l^3 > tau_g ds^5, "
+                   "tau_g = A_g 10^y_g (A_g: the group's mean |a| of the previous evaluation, y_g: the network)"
+                   % Lr.THETA_BOUND)
     out["training"] = {"system": "Plummer N=%d seed %d" % (n, a.seed + 1), "pairs": int(X.shape[0]),
-                       "final_loss": loss, "seconds": t_train}
-    out["calibrated"] = {
-        "scale": c, "theta_range": [lo, hi], "median_err_on_training_system": e_cal,
-        "fp32": compare(measure(B, L, pos, vel, samp, ref, theta_range=(lo, hi), **kw)),
-        "double_single": compare(measure(B, L, pos, vel, samp, ref, theta_range=(lo, hi), precision=1, **kw)),
-    }
+                       "final_loss": loss, "seconds": t_train, "label": "y at which the group's error meets the target",
+                       "calibration_shift": c, "y_range": [lo, hi], "median_err_on_training_system": e_cal}
+    out["double_single"] = compare_to_sweep(
+        measure(B, L, pos, vel, samp, ref, weights=w, y_range=(lo, hi), precision=1, **kw), sweep, a.learned_target)
+    # the relative mode without the network: one alpha for every group,
+    # bisected on the bench system itself to the learned form's median
+    alpha = relative_alpha_at(B, L, pos, vel, samp, ref, out["median_rel_force_err"], **kw)
+    out["relative_single_alpha"] = compare_to_sweep(
+        measure(B, L, pos, vel, samp, ref, alpha=alpha, **kw), sweep, a.learned_target)
+    out["relative_single_alpha"]["alpha"] = alpha
     return out
 
 
+def compare_to_sweep(r, sweep, target):
+    """Fixed-angle throughput at the same median and p99 error (log-log
+    interpolation over the sweep), and the fastest fixed angle of the sweep
+    whose median error meets the target."""
+    if not sweep:
+        return r
+    em = at_equal(sweep, "value", "median_rel_force_err", r["median_rel_force_err"])
+    ep = at_equal(sweep, "value", "p99_rel_force_err", r["p99_rel_force_err"])
+    r["fixed_theta_value_at_equal_median"] = em
+    r["fixed_theta_value_at_equal_p99"] = ep
+    r["gain_at_equal_median"] = r["value"] / em if em else None
+    r["gain_at_equal_p99"] = r["value"] / ep if ep else None
+    ok = [q for q in sweep if q["median_rel_force_err"] <= target]
+    if ok:
+        best = max(ok, key=lambda q: q["value"])
+        r["best_fixed_meeting_target"] = {"theta": best["theta"], "value": best["value"],
+                                          "median_rel_force_err": best["median_rel_force_err"]}
+        r["vs_best_fixed_meeting_target"] = r["value"] / best["value"]
+    return r
+
+
+def relative_alpha_at(B, L, pos, vel, samp, ref, median, *, theta, eps, device, nleaf, ncrit, level_split, **_):
+    """The single alpha whose relative walk (tau = alpha A_g) has the given
+    median error on this system (bisection in log alpha)."""
+    from bonsai2_b200 import learned as Lr
+    from bonsai2_b200.treecode import _p
+    n = pos.shape[0]
+    t = B.Treecode(eps=eps, theta=theta, ncrit=ncrit, nleaf=nleaf, level_split=level_split, device=device)
+    t.alloc(n)
+    L.bonsai_set_particles(t.handle, _p(pos), _p(vel), n)
+    Lr.set_relative_bound(t, Lr.THETA_BOUND)
+    refn = np.linalg.norm(ref[:, :3], axis=1)
+
+    def med(la):
+        Lr.set_theta_mode(t, 3, 10.0 ** la, 10.0 ** la)
+        Lr.run_relative(t, nleaf, ncrit, level_split, evaluations=2)
+        acc = t.get_acc()[samp].astype(np.float64)
+        return float(np.median(np.linalg.norm(acc[:, :3] - ref[:, :3], axis=1) / refn))
+
+    lo, hi = -4.0, -0.5
+    for _ in range(10):
+        mid = 0.5 * (lo + hi)
+        if med(mid) > median:
+            hi = mid
+        else:
+            lo = mid
+    t.close()
+    return float(10.0 ** lo)
+
+
 def measure(B, L, pos, vel, samp, ref, *, theta, eps, device, nleaf=16, ncrit=64, level_split=5, dt=1.0 / 128,
-            steps=3, precision=0, weights=None, theta_range=None):
-    """One configuration on one system: an eager force evaluation judged at
-    the sample particles against ref (FP64 direct sum), then `steps` timed
-    graph steps from the same initial state.  pos may be float64 (loaded as
-    double-single in precision 1, rounded to float in precision 0)."""
+            steps=3, precision=0, weights=None, y_range=None, alpha=None):
+    """One configuration on one system: force evaluations judged at the
+    sample particles against ref (FP64 direct sum), then `steps` timed graph
+    steps from the same initial state.  weights: the learned form (theta
+    mode 1, output range y_range); alpha: the relative mode with one
+    parameter (theta mode 3).  Both read the previous evaluation's
+    accelerations, so their accuracy is taken at the third evaluation of the
+    same positions (the first is the fixed-angle fallback) and the timing
+    after one untimed step.  pos may be float64 (loaded as double-single in
+    precision 1, rounded to float in precision 0)."""
     from bonsai2_b200 import learned as Lr
     from bonsai2_b200.treecode import _p
     n = pos.shape[0]
     t = B.Treecode(eps=eps, theta=theta, ncrit=ncrit, nleaf=nleaf, level_split=level_split, dt=dt, device=device)
     t.set_precision(precision)
+    relative = weights is not None or alpha is not None
+    if relative:
+        Lr.set_relative_bound(t, Lr.THETA_BOUND)
     if weights is not None:
         Lr.set_weights(t, weights)
-        Lr.set_theta_mode(t, 1, *(theta_range or (Lr.LO, Lr.HI)))
+        Lr.set_theta_mode(t, 1, *(y_range or (Lr.YLO, Lr.YHI)))
+    elif alpha is not None:
+        Lr.set_theta_mode(t, 3, alpha, alpha)
 
     def load():
         if pos.dtype == np.float64:
@@ -707,13 +766,12 @@ def measure(B, L, pos, vel, samp, ref, *, theta, eps, device, nleaf=16, ncrit=64
             L.bonsai_set_particles(t.handle, _p(pos), _p(vel), n)
 
     load()
-    t.buildTree(nleaf)
-    t.computeMultipoles()
-    t.makeGroups(level_split, ncrit)
-    t.computeForces(False)
+    Lr.run_relative(t, nleaf, ncrit, level_split, evaluations=3 if relative else 1)
     acc = t.get_acc()[samp].astype(np.float64)
     err = np.linalg.norm(acc[:, :3] - ref[:, :3], axis=1) / np.linalg.norm(ref[:, :3], axis=1)
-    th = Lr.group_theta(t) if weights is not None else None
+    if relative:
+        cnt = Lr.group_interactions(t)
+        tau = Lr.group_scale(t)
     load()
     t.step(1, graph=True)
     t.synchronize()
@@ -732,9 +790,10 @@ def measure(B, L, pos, vel, samp, ref, *, theta, eps, device, nleaf=16, ncrit=64
            "approx_per_particle": float(st[0]) / n, "direct_per_particle": float(st[1]) / n,
            "median_rel_force_err": float(np.median(err)), "p99_rel_force_err": float(np.percentile(err, 99)),
            "status": int(status)}
-    if th is not None:
-        out["theta_mean"] = float(th.mean())
-        out["theta_p10_p90"] = [float(np.percentile(th, 10)), float(np.percentile(th, 90))]
+    if relative:
+        out["theta"] = Lr.THETA_BOUND
+        out["groups_walked"] = int(cnt.shape[0])
+        out["group_scale_range"] = [float(np.percentile(tau, 10)), float(np.percentile(tau, 90))]
     return out
 
 
@@ -803,22 +862,22 @@ def precision_form(B, L, a, device):
 
 def learned_field_form(B, L, a, device):
     """The learned form on the clustered field (64 Plummer subclusters plus
-    a 20 % uniform background): the network is trained on a field of another
-    seed (untimed), then learned and fixed angles are timed on the bench field
-    and judged against the FP64 direct sum (2048 samples); interactions per
-    particle and throughput at equal median and p99 error."""
+    a 20 % uniform background): the network is trained and calibrated on a
+    field of another seed (untimed), then learned and fixed angles are timed
+    on the bench field and judged against the FP64 direct sum (2048 samples);
+    throughput at equal median and p99 error, and against the fastest fixed
+    angle that meets the target."""
     from bonsai2_b200 import learned as Lr
     n = a.field_n
     eps = 0.001
     pos, vel = B.clustered_field(n, seed=a.seed)
     t0 = time.perf_counter()
     ptr, vtr = B.clustered_field(n, seed=a.seed + 1)
-    X, y, _ = Lr.training_set(ptr, vtr, eps=eps, target=a.learned_target, max_groups=8192, device=device)
-    w, loss = Lr.train(X, y, epochs=3000, lr=3e-3, device=device)
-    t_train = time.perf_counter() - t0
+    X, y, _ = Lr.relative_training_set(ptr, vtr, eps=eps, target=a.learned_target, max_groups=8192, device=device)
+    w, loss = Lr.train(X, y, epochs=3000, lr=3e-3, lo=Lr.YLO, hi=Lr.YHI, device=device)
     # field realisations differ more than Plummer seeds: calibrate to 0.8 x target
-    # (0.9 x target on the training field gave 1.07e-3 on the bench field)
-    c, lo, hi, e_cal = Lr.calibrate(ptr, vtr, w, eps, a.learned_target, fraction=0.8, device=device)
+    c, lo, hi, e_cal = Lr.calibrate_relative(ptr, vtr, w, eps, a.learned_target, fraction=0.8, device=device)
+    t_train = time.perf_counter() - t0
     del ptr, vtr
     rng = np.random.default_rng(2048)
     samp = np.ascontiguousarray(np.sort(rng.choice(n, 2048, replace=False)).astype(np.int32))
@@ -829,31 +888,24 @@ def learned_field_form(B, L, a, device):
     t.ptcl_h2d()
     ref = t.direct_fp64(samp, include_self=True)
     t.close()
-    sweep = [measure(B, L, pos, vel, samp, ref, theta=th, eps=eps, device=device)
-             for th in (0.4, 0.5, 0.6, 0.7, 0.8, 0.9, 1.0)]
-    lrn = measure(B, L, pos, vel, samp, ref, theta=0.5, eps=eps, device=device, weights=w)
-    cal = measure(B, L, pos, vel, samp, ref, theta=0.5, eps=eps, device=device, weights=w, theta_range=(lo, hi))
-    for r in (cal,):
-        em = at_equal(sweep, "value", "median_rel_force_err", r["median_rel_force_err"])
-        ep = at_equal(sweep, "value", "p99_rel_force_err", r["p99_rel_force_err"])
-        r["gain_at_equal_median"] = r["value"] / em if em else None
-        r["gain_at_equal_p99"] = r["value"] / ep if ep else None
-        r["scale"] = c
-        r["calibration_fraction"] = 0.8
-        r["median_err_on_training_field"] = e_cal
-    eq_m = at_equal(sweep, "value", "median_rel_force_err", lrn["median_rel_force_err"])
-    eq_p = at_equal(sweep, "value", "p99_rel_force_err", lrn["p99_rel_force_err"])
-    ip_m = at_equal(sweep, "approx_per_particle", "median_rel_force_err", lrn["median_rel_force_err"])
+    kw = dict(theta=0.5, eps=eps, device=device)
+    sweep = [measure(B, L, pos, vel, samp, ref, **dict(kw, theta=th)) for th in (0.4, 0.5, 0.6, 0.7, 0.8, 0.9, 1.0)]
+    lrn = compare_to_sweep(measure(B, L, pos, vel, samp, ref, weights=w, y_range=(lo, hi), **kw), sweep,
+                           a.learned_target)
+    alpha = relative_alpha_at(B, L, pos, vel, samp, ref, lrn["median_rel_force_err"], nleaf=16, ncrit=64,
+                              level_split=5, **kw)
+    rel = compare_to_sweep(measure(B, L, pos, vel, samp, ref, alpha=alpha, **kw), sweep, a.learned_target)
+    rel["alpha"] = alpha
     return {"config": "clustered field N=%d: 64 Plummer subclusters (masses log-uniform over 2 decades, scale radii "
                       "log-uniform 0.01-0.2, centres uniform in the unit cube) + 20%% uniform background; eps %.3f; "
                       "2048 samples" % (n, eps),
-            "learned": lrn, "learned_calibrated": cal, "fixed_theta_sweep": sweep,
-            "fixed_value_at_equal_median": eq_m, "fixed_value_at_equal_p99": eq_p,
-            "gain_at_equal_median": lrn["value"] / eq_m if eq_m else None,
-            "gain_at_equal_p99": lrn["value"] / eq_p if eq_p else None,
-            "fixed_approx_per_particle_at_equal_median": ip_m,
+            "learned": lrn, "relative_single_alpha": rel, "fixed_theta_sweep": sweep,
+            "gain_at_equal_median": lrn.get("gain_at_equal_median"),
+            "gain_at_equal_p99": lrn.get("gain_at_equal_p99"),
             "training": {"system": "clustered field seed %d" % (a.seed + 1), "pairs": int(X.shape[0]),
-                         "final_loss": loss, "seconds": t_train, "target": a.learned_target}}
+                         "final_loss": loss, "seconds": t_train, "target": a.learned_target,
+                         "calibration_shift": c, "calibration_fraction": 0.8, "y_range": [lo, hi],
+                         "median_err_on_training_field": e_cal}}
 
 
 # the reference's one published number: the standalone octree build of a

@@ -74,6 +74,9 @@ SIGNATURES = {
     "bonsai_set_theta_mode": (I, [P, I, ctypes.c_float, ctypes.c_float]),
     "bonsai_set_mlp_weights": (I, [P, P, I]),
     "bonsai_set_group_theta": (I, [P, P, I]),
+    "bonsai_set_group_tau": (I, [P, P, I]),
+    "bonsai_set_relative_bound": (I, [P, ctypes.c_float]),
+    "bonsai_get_group_scale": (I, [P, P]),
     "bonsai_get_group_features": (I, [P, P, P]),
     "bonsai_get_group_theta": (I, [P, P]),
     "bonsai_get_group_interactions": (I, [P, P]),

@@ -69,6 +69,26 @@ __global__ void k_gather_state(const int* __restrict__ perm, int n, const float4
 __global__ void k_gather_pos(const int* __restrict__ perm, int n, const float4* __restrict__ pos,
                              float4* __restrict__ out);
 
+// Relative accuracy mode (per-group bound tau on a cell's octupole truncation
+// error, M l^3 / ds^5 <= tau) and the statistics the learned features read
+// at the next evaluation.
+struct RelativeArgs {
+  const float* tau = nullptr;  // per-group bounds; null: the geometric test only
+  float4* stats = nullptr;     // per-group statistics written by the walk (null: none)
+  int* part_gid = nullptr;     // group of each particle, written with the statistics
+  int* acc_valid = nullptr;    // set to 1 by the walk once acc holds this evaluation's accelerations
+};
+
+// What the learned features read of the previous evaluation.
+struct PrevEval {
+  const float4* acc = nullptr;    // its accelerations, in its particle order
+  const int* perm = nullptr;      // current position -> index in that order (null: the same order)
+  const int* acc_valid = nullptr; // device flag: acc is valid
+  const int* part_gid = nullptr;  // group of each particle in that evaluation (its order)
+  const float4* stats = nullptr;  // its per-group statistics
+  int stats_cap = 0;              // capacity of stats
+};
+
 // walk.cu
 int walk_variant(int ncrit, int layout);
 int walk_blocks_per_sm(int variant);
@@ -79,13 +99,15 @@ void launch_walk(int variant, int nblocks, const int2* groups, const TreeInfo* i
                  const float2* cell_ls, const float* group_inv_theta, float eps2, float4* acc, int* ring_pool,
                  int ring_cap, unsigned* group_counter, unsigned long long* stats, int* status, const int* sys_off,
                  int nsys, const int* root_beg, const float4* ipos_lo, const float4* jpos_lo, const float4* cell_lo,
-                 uint2* group_counts, const int* group_list, const unsigned* group_list_n, cudaStream_t s);
+                 uint2* group_counts, const int* group_list, const unsigned* group_list_n, const RelativeArgs& rel,
+                 cudaStream_t s);
 
 // walk64.cu: the FP64 checker walk (same interaction lists as the float walk)
 void launch_walk64(int nblocks, const int2* groups, const TreeInfo* info, const float4* ipos, const float4* ipos_lo,
                    const float4* jpos, const float4* jpos_lo, const uint4* cell_data, const float4* cell_open,
-                   const float4* cell_lo, const float2* cell_ls, const float* group_inv_theta, const MpRec* rec,
-                   double eps2, double4* acc, int* ring_pool, int ring_cap, unsigned* group_counter,
+                   const float4* cell_lo, const float2* cell_ls, const float* group_inv_theta,
+                   const float* group_tau, const MpRec* rec, double eps2, double4* acc, int* ring_pool, int ring_cap,
+                   unsigned* group_counter,
                    unsigned long long* stats, int* status, const int* sys_off, int nsys, const int* root_beg,
                    cudaStream_t s);
 void launch_scatter_d4(const int* id, int n, const double4* in, double4* out, int nblocks, cudaStream_t s);
@@ -137,6 +159,7 @@ int bounds_word_groups(unsigned* w, bool reset);
 int bounds_word_walk(unsigned* w, bool reset);
 int bounds_word_walk64(unsigned* w, bool reset);
 int bounds_word_move(unsigned* w, bool reset);
+int bounds_word_learned(unsigned* w, bool reset);
 // checked-build self-test (move.cu): one guarded write at the logical end of
 // a buffer that has a spare element, so the access is inside the allocation
 // in every build; returns the violations it recorded (1 in a checked build)
@@ -151,12 +174,20 @@ void mlp_predict(const float* X, int S, const float* w, float lo, float hi, floa
                  cudaStream_t st);
 // box: the domain box, or an ensemble's per-system boxes (nsys > 1, with
 // sys_off and the systems' level-1 cell ranges root_beg)
+// amag: each group's mean |a| of the previous evaluation (0 without one)
 void launch_group_features(const int2* groups, const TreeInfo* info, const float4* ipos,
                            const unsigned long long* ph_sorted, const MpRec* rec, const Box* box, int n, int ncrit,
-                           float eps, float* feat, const int* sys_off, int nsys, const int* root_beg, int nblocks,
-                           cudaStream_t st);
-void launch_mlp_infer(const float* feat, const void* wh, const TreeInfo* info, float lo, float hi, float* inv,
-                      int nblocks, cudaStream_t st);
+                           float eps, float* feat, const int* sys_off, int nsys, const int* root_beg,
+                           const PrevEval& prev, float* amag, int nblocks, cudaStream_t st);
+// the network's output y in [lo, hi] per group: tau = amag 10^y, 1/theta =
+// inv_bound; without previous accelerations the fixed angle (tau = 0,
+// 1/theta = inv_fixed)
+void launch_mlp_infer(const float* feat, const void* wh, const TreeInfo* info, float lo, float hi, const float* amag,
+                      const int* acc_valid, float inv_bound, float inv_fixed, float* inv, float* tau, int nblocks,
+                      cudaStream_t st);
+// relative mode with one accuracy parameter: tau = alpha amag (fallback as above)
+void launch_relative_tau(const TreeInfo* info, const float* amag, const int* acc_valid, float alpha, float inv_bound,
+                         float inv_fixed, float* inv, float* tau, int nblocks, cudaStream_t st);
 void launch_weights_to_half(const float* w, void* wh, cudaStream_t st);
 void launch_fill_inv_theta(const TreeInfo* info, const float* theta, float c, float* inv, int nblocks,
                            cudaStream_t st);

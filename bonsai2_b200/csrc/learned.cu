@@ -1,18 +1,34 @@
-// learned.cu -- per-group opening angles from a small MLP.
+// learned.cu -- per-group opening bounds from a small MLP.
 //
-// A group's opening angle theta_g trades its force error against its walk
-// cost.  Groups differ (a group in the dense core sees most of its force from
-// nearby cells, one in the halo from far away), so one angle for all groups
-// must suit the worst of them.  Here a 16 -> 64 -> 64 -> 1 network maps cheap
-// group features to theta_g; it is trained on pairs (features, largest theta
-// meeting a per-group error target) that the fixed-angle walk and the FP64
-// direct sum generate (bonsai2_b200/learned.py), with this file's own forward
-// and backward kernels.  The walk then runs with per-group angles
-// (walk.cu, PERGROUP).  Fixed-angle walking stays available (theta mode 0).
+// The walk opens a cell when the group is inside its geometric opening
+// sphere (computeForces.cu:30-54) at the group's angle theta_g, or -- in the
+// relative accuracy mode -- when the cell's octupole truncation error, of
+// order M l^3 / ds^5, exceeds the group's bound tau_g.  A single angle must
+// suit the worst group; per-group angles alone gain little (their best
+// allocation is a few tens of percent and cannot be predicted from group
+// features), while a bound on each cell's truncation error relative to the
+// group's own acceleration puts the error budget where it matters.  Here a
+// 16 -> 64 -> 64 -> 1 network maps group features to y_g = log10(tau_g / A_g),
+// A_g being the group's mean |a| of the previous force evaluation; it is
+// trained on pairs (features, the y at which the group's error against the
+// FP64 direct sum meets the target) that the walk and the direct sum
+// generate (bonsai2_b200/learned.py), with this file's own forward and
+// backward kernels.  theta_g is then a fixed safety bound.  Without previous
+// accelerations (the first evaluation after particles are loaded) every
+// group walks at the fixed angle (theta mode 0's walk, bit for bit).
+//
+// Features (per group, normalised logs clamped to [-10, 10]): size, radius,
+// tree depth (common PH-key prefix), distance from and mass share of its
+// system, density, shape, system size, softening over radius, the previous
+// acceleration scale A_g and its spread over the group, and -- recorded by
+// the previous walk of the group holding the group's middle particle -- the
+// number of cells near the opening boundary, the mass share of the accepted
+// cells near it, and the force-weighted quadrupole norm of the accepted
+// cells.
 //
 // Weight vector layout (kMlpWeights floats): W1[64][16], b1[64], W2[64][64],
 // b2[64], w3[64], b3.  Hidden activations tanh; output
-// theta = lo + (hi - lo) * sigmoid(z).
+// y = lo + (hi - lo) * sigmoid(z).
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -36,9 +52,11 @@ __global__ void __launch_bounds__(256) k_group_features(const int2* __restrict__
                                                         const MpRec* __restrict__ rec, const Box* __restrict__ box,
                                                         int n, int ncrit, float eps, float* __restrict__ feat,
                                                         const int* __restrict__ sys_off, int nsys,
-                                                        const int* __restrict__ root_beg) {
+                                                        const int* __restrict__ root_beg, const PrevEval prev,
+                                                        float* __restrict__ amag) {
   const int lane = threadIdx.x & 31;
   const int ng = info->ngroups;
+  const bool have_prev = prev.acc_valid && *prev.acc_valid;
   // the group's system: its centre of mass and mass from its level-1 cells,
   // its box and its size (an ensemble's systems each have their own)
   int sys = -1;
@@ -64,46 +82,70 @@ __global__ void __launch_bounds__(256) k_group_features(const int2* __restrict__
       ns = nsys > 1 ? sys_off[s + 1] - sys_off[s] : n;
     }
     float mn[3] = {3e38f, 3e38f, 3e38f}, mx[3] = {-3e38f, -3e38f, -3e38f};
-    float mg = 0.f;
+    float mg = 0.f, am = 0.f, al = 0.f, al2 = 0.f;
     for (int i = lane; i < np; i += 32) {
       const float4 p = ipos[pb + i];
       mn[0] = fminf(mn[0], p.x); mn[1] = fminf(mn[1], p.y); mn[2] = fminf(mn[2], p.z);
       mx[0] = fmaxf(mx[0], p.x); mx[1] = fmaxf(mx[1], p.y); mx[2] = fmaxf(mx[2], p.z);
       mg += p.w;
+      if (have_prev) {
+        const int k = pb + i;
+        const int j = prev.perm ? __ldg(prev.perm + k) : k;
+        const float4 a = BONSAI_IN_RANGE(j, n, 0x501) ? __ldg(prev.acc + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float m = sqrtf(a.x * a.x + a.y * a.y + a.z * a.z);
+        const float lm = safe_log10(m);
+        am += m; al += lm; al2 += lm * lm;
+      }
     }
     for (int k = 0; k < 3; k++) { mn[k] = warp_min_f32(mn[k]); mx[k] = warp_max_f32(mx[k]); }
 #pragma unroll
-    for (int o = 16; o; o >>= 1) mg += __shfl_xor_sync(kFull, mg, o);
+    for (int o = 16; o; o >>= 1) {
+      mg += __shfl_xor_sync(kFull, mg, o);
+      am += __shfl_xor_sync(kFull, am, o);
+      al += __shfl_xor_sync(kFull, al, o);
+      al2 += __shfl_xor_sync(kFull, al2, o);
+    }
     const float gx = 0.5f * (mx[0] + mn[0]), gy = 0.5f * (mx[1] + mn[1]), gz = 0.5f * (mx[2] + mn[2]);
     const float sx = 0.5f * (mx[0] - mn[0]), sy = 0.5f * (mx[1] - mn[1]), sz = 0.5f * (mx[2] - mn[2]);
     const float rg = fmaxf(sqrtf(sx * sx + sy * sy + sz * sz), 1e-12f * hs);
-    // mean distance from the group centre (concentration)
-    float md = 0.f;
-    for (int i = lane; i < np; i += 32) {
-      const float4 p = ipos[pb + i];
-      md += sqrtf((p.x - gx) * (p.x - gx) + (p.y - gy) * (p.y - gy) + (p.z - gz) * (p.z - gz));
-    }
-#pragma unroll
-    for (int o = 16; o; o >>= 1) md += __shfl_xor_sync(kFull, md, o);
     if (lane == 0) {
       const float dg = sqrtf((gx - cx) * (gx - cx) + (gy - cy) * (gy - cy) + (gz - cz) * (gz - cz));
       const int lvl = diff_level(ph_sorted[pb], ph_sorted[pb + np - 1]) - 1;  // common PH prefix (levels)
       const float vol = rg * rg * rg;
+      // the previous evaluation: acceleration scale (floored at 1e-4 of the
+      // system's M / hsize^2, so that a group at an exact balance point does not
+      // open everything) and the statistics of the group that held the
+      // group's middle particle
+      const float afloor = 1e-4f * mtot / fmaxf(hs * hs, 1e-30f);
+      float A = 0.f, spread = 0.f;
+      float4 st = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (have_prev) {
+        A = fmaxf(am / (float)np, afloor);
+        const float mu = al / (float)np;
+        spread = sqrtf(fmaxf(al2 / (float)np - mu * mu, 0.f));
+        const int k = pb + np / 2;
+        const int j = prev.perm ? __ldg(prev.perm + k) : k;
+        if (BONSAI_IN_RANGE(j, n, 0x502)) {
+          const int og = __ldg(prev.part_gid + j);
+          if (og >= 0 && og < prev.stats_cap) st = __ldg(prev.stats + og);
+        }
+      }
+      amag[g] = A;
       float f[kF];
-      f[0] = (float)np / (float)ncrit;
-      f[1] = safe_log10(rg / hs) / 6.f;
-      f[2] = safe_log10(dg / hs + 1e-7f) / 6.f;
-      f[3] = safe_log10(rg / fmaxf(dg, 1e-12f * hs)) / 3.f;
-      f[4] = (float)min(lvl, kMaxLevel) / (float)kMaxLevel;
-      f[5] = safe_log10(mg / fmaxf(mtot, 1e-30f)) / 8.f;
-      f[6] = safe_log10((float)np / vol * hs * hs * hs / (float)ns) / 8.f;
-      f[7] = sx / rg; f[8] = sy / rg; f[9] = sz / rg;
-      f[10] = log10f((float)ns) / 8.f;
-      f[11] = safe_log10(fmaxf(eps, 1e-12f) / rg) / 3.f;
-      f[12] = safe_log10(fmaxf(eps, 1e-12f) / hs) / 6.f;
-      f[13] = dg / (dg + rg);
-      f[14] = (md / (float)np) / rg;
-      f[15] = 1.0f;
+      f[0] = (float)np / (float)ncrit;                               // group size
+      f[1] = safe_log10(rg / hs) / 6.f;                              // radius
+      f[2] = (float)min(lvl, kMaxLevel) / (float)kMaxLevel;          // tree depth
+      f[3] = safe_log10(dg / hs + 1e-7f) / 6.f;                      // distance from the system's centre
+      f[4] = safe_log10(mg / fmaxf(mtot, 1e-30f)) / 8.f;             // mass share
+      f[5] = safe_log10((float)np / vol * hs * hs * hs / (float)ns) / 8.f;  // density
+      f[6] = sx / rg; f[7] = sy / rg; f[8] = sz / rg;                // shape
+      f[9] = log10f((float)ns) / 8.f;                                // system size
+      f[10] = safe_log10(fmaxf(eps, 1e-12f) / rg) / 3.f;             // softening / radius
+      f[11] = have_prev ? safe_log10(A * hs * hs / fmaxf(mtot, 1e-30f)) / 3.f : 0.f;  // acceleration scale
+      f[12] = spread;                                                // its spread (dex)
+      f[13] = log10f(1.0f + st.x) / 4.f;                             // cells near the opening boundary
+      f[14] = st.y;                                                  // accepted mass near it
+      f[15] = have_prev ? safe_log10(st.z + 1e-12f) / 3.f : 0.f;     // quadrupole norm of accepted cells
       // degenerate groups (a one-particle system's box and radius are floored
       // near 1e-12, so the density's float products under- and overflow) give
       // inf or NaN; the features are normalised logs well inside [-10, 10], and
@@ -124,7 +166,9 @@ __global__ void __launch_bounds__(256) k_group_features(const int2* __restrict__
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_mlp_infer(const float* __restrict__ feat, const __half* __restrict__ wh,
                                                    const TreeInfo* __restrict__ info, float lo, float hi,
-                                                   float* __restrict__ group_inv_theta) {
+                                                   const float* __restrict__ amag, const int* __restrict__ acc_valid,
+                                                   float inv_bound, float inv_fixed,
+                                                   float* __restrict__ group_inv_theta, float* __restrict__ group_tau) {
   __shared__ __half sw[kMlpWeights + 1];
   __shared__ float sh[8][kH];
   for (int t = threadIdx.x; t < kMlpWeights; t += blockDim.x) {
@@ -160,8 +204,28 @@ __global__ void __launch_bounds__(256) k_mlp_infer(const float* __restrict__ fea
 #pragma unroll
     for (int o = 16; o; o >>= 1) z += __shfl_xor_sync(kFull, z, o);
     z += __half2float(sw[oB3]);
-    if (lane == 0) group_inv_theta[g] = 1.0f / (lo + (hi - lo) / (1.0f + expf(-z)));
+    if (lane == 0) {
+      if (*acc_valid) {
+        const float y = lo + (hi - lo) / (1.0f + expf(-z));
+        group_tau[g] = amag[g] * exp10f(y);
+        group_inv_theta[g] = inv_bound;
+      } else {  // no previous accelerations: the fixed angle
+        group_tau[g] = 0.0f;
+        group_inv_theta[g] = inv_fixed;
+      }
+    }
     __syncwarp();
+  }
+}
+
+__global__ void k_relative_tau(const TreeInfo* __restrict__ info, const float* __restrict__ amag,
+                               const int* __restrict__ acc_valid, float alpha, float inv_bound, float inv_fixed,
+                               float* __restrict__ inv, float* __restrict__ tau) {
+  const int ng = info->ngroups;
+  const bool v = *acc_valid != 0;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
+    tau[g] = v ? alpha * amag[g] : 0.0f;
+    inv[g] = v ? inv_bound : inv_fixed;
   }
 }
 
@@ -375,15 +439,22 @@ void mlp_predict(const float* X, int S, const float* w, float lo, float hi, floa
 
 void launch_group_features(const int2* groups, const TreeInfo* info, const float4* ipos,
                            const unsigned long long* ph_sorted, const MpRec* rec, const Box* box, int n, int ncrit,
-                           float eps, float* feat, const int* sys_off, int nsys, const int* root_beg, int nblocks,
-                           cudaStream_t st) {
+                           float eps, float* feat, const int* sys_off, int nsys, const int* root_beg,
+                           const PrevEval& prev, float* amag, int nblocks, cudaStream_t st) {
   k_group_features<<<nblocks, 256, 0, st>>>(groups, info, ipos, ph_sorted, rec, box, n, ncrit, eps, feat, sys_off,
-                                            nsys, root_beg);
+                                            nsys, root_beg, prev, amag);
 }
 
-void launch_mlp_infer(const float* feat, const void* wh, const TreeInfo* info, float lo, float hi, float* inv,
-                      int nblocks, cudaStream_t st) {
-  k_mlp_infer<<<nblocks, 256, 0, st>>>(feat, static_cast<const __half*>(wh), info, lo, hi, inv);
+void launch_mlp_infer(const float* feat, const void* wh, const TreeInfo* info, float lo, float hi, const float* amag,
+                      const int* acc_valid, float inv_bound, float inv_fixed, float* inv, float* tau, int nblocks,
+                      cudaStream_t st) {
+  k_mlp_infer<<<nblocks, 256, 0, st>>>(feat, static_cast<const __half*>(wh), info, lo, hi, amag, acc_valid,
+                                       inv_bound, inv_fixed, inv, tau);
+}
+
+void launch_relative_tau(const TreeInfo* info, const float* amag, const int* acc_valid, float alpha, float inv_bound,
+                         float inv_fixed, float* inv, float* tau, int nblocks, cudaStream_t st) {
+  k_relative_tau<<<nblocks, 256, 0, st>>>(info, amag, acc_valid, alpha, inv_bound, inv_fixed, inv, tau);
 }
 
 void launch_weights_to_half(const float* w, void* wh, cudaStream_t st) {
@@ -394,5 +465,7 @@ void launch_fill_inv_theta(const TreeInfo* info, const float* theta, float c, fl
                            cudaStream_t st) {
   k_fill_inv_theta<<<nblocks, 256, 0, st>>>(info, theta, c, inv);
 }
+
+BONSAI_BOUNDS_ACCESSOR(bounds_word_learned)
 
 }  // namespace bonsai

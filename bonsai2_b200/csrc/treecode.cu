@@ -79,6 +79,18 @@ struct Handle {
   float theta_lo = 0.25f, theta_hi = 1.25f;
   int gcap = 0;
   float* group_inv = nullptr;
+  // relative accuracy mode: per-group bound on a cell's truncation error,
+  // each group's mean |a| of the previous evaluation, the walk's per-group
+  // statistics and the group of every particle (read by the next
+  // evaluation's features), and the flag that acc holds valid accelerations
+  float* group_tau = nullptr;
+  float* group_amag = nullptr;
+  float4* group_stats = nullptr;
+  int* part_gid = nullptr;
+  int* acc_valid = nullptr;
+  bool tau_on = false;
+  float theta_bound = 1.3f;  // geometric safety bound of the relative modes
+  float rel_alpha = 1e-2f;   // theta mode 3: tau = rel_alpha * A_g
   float* group_feat = nullptr;
   uint2* group_counts = nullptr;  // per-group (approx, direct) counts of the per-group angle walk
   double4 *acc64 = nullptr, *acc64_tmp = nullptr;  // FP64 checker walk output (group order, caller order)
@@ -132,6 +144,19 @@ struct Handle {
   unsigned* walk_list_n = nullptr;
   int* max_lev = nullptr;  // device: largest level present
   bool walk_list_on = false;
+  // acc follows the particles' current (state) order: after a walk, and after
+  // a block-step gather; false once a PH gather reorders the particles
+  bool acc_in_state_order = false;
+  PrevEval prev_eval() const {
+    PrevEval p;
+    p.acc = acc;
+    p.perm = acc_in_state_order ? nullptr : pperm;
+    p.acc_valid = acc_valid;
+    p.part_gid = part_gid;
+    p.stats = group_stats;
+    p.stats_cap = gcap;
+    return p;
+  }
   bool bts_gathering = false;  // inside block_steps: levels and accelerations follow the state
   int nsys = 1, nchunks = 0;
   int *sys_off = nullptr, *chunk_beg = nullptr, *root_beg = nullptr;
@@ -218,7 +243,8 @@ struct Handle {
     dfree(&acc); dfree(&jpos); dfree(&tkey); dfree(&pkey); dfree(&kalt);
     dfree(&tperm); dfree(&pperm); dfree(&valt); dfree(&sort_counts); dfree(&bsum);
     dfree(&kalt2); dfree(&valt2); dfree(&sort_counts2);
-    dfree(&dlev); dfree(&chain); dfree(&hist); dfree(&groups); dfree(&group_inv); dfree(&group_feat);
+    dfree(&dlev); dfree(&chain); dfree(&hist); dfree(&groups); dfree(&group_inv); dfree(&group_tau); dfree(&group_amag);
+    dfree(&group_stats); dfree(&part_gid); dfree(&group_feat);
     dfree(&group_counts); dfree(&acc64); dfree(&acc64_tmp);
     release_cells();
     n = 0;
@@ -234,7 +260,7 @@ struct Handle {
     release_particles();
     dfree(&info); dfree(&g_count); dfree(&g_seg); dfree(&g_ng); dfree(&ring);
     dfree(&group_counter); dfree(&stats); dfree(&move_partial); dfree(&energies);
-    dfree(&move_ticket); dfree(&box_ticket); dfree(&closing); dfree(&box); dfree(&box_partial);
+    dfree(&move_ticket); dfree(&box_ticket); dfree(&closing); dfree(&acc_valid); dfree(&box); dfree(&box_partial);
     dfree(&ph_table); dfree(&direct_part); dfree(&direct_out); dfree(&direct_sample);
     dfree(&mlp_w);
     if (mlp_wh) { cudaFree(mlp_wh); mlp_wh = nullptr; }
@@ -310,6 +336,8 @@ struct Handle {
     BONSAI_CUDA_TRY(cudaMemset(box_ticket, 0, sizeof(unsigned)));
     BONSAI_CUDA_TRY(dalloc(&closing, 1));
     BONSAI_CUDA_TRY(cudaMemset(closing, 0, sizeof(int)));
+    BONSAI_CUDA_TRY(dalloc(&acc_valid, 1));
+    BONSAI_CUDA_TRY(cudaMemset(acc_valid, 0, sizeof(int)));
     BONSAI_CUDA_TRY(dalloc(&box, 1));
     BONSAI_CUDA_TRY(dalloc(&box_partial, (size_t)box_blocks * 6));
     std::vector<uint16_t> tab(384);
@@ -355,6 +383,13 @@ struct Handle {
     // one partial group per PH segment (groups.cu)
     gcap = (int)std::min<long long>(N, (long long)N / std::max(1, prm.ncrit) + (1ll << (3 * kMaxLevelSplit)) + 1);
     BONSAI_CUDA_TRY(dalloc(&group_inv, (size_t)gcap));
+    BONSAI_CUDA_TRY(dalloc(&group_tau, (size_t)gcap));
+    BONSAI_CUDA_TRY(dalloc(&group_amag, (size_t)gcap));
+    BONSAI_CUDA_TRY(dalloc(&group_stats, (size_t)gcap));
+    BONSAI_CUDA_TRY(cudaMemset(group_stats, 0, (size_t)gcap * sizeof(float4)));
+    BONSAI_CUDA_TRY(dalloc(&part_gid, N));
+    BONSAI_CUDA_TRY(cudaMemset(part_gid, 0, N * sizeof(int)));
+    BONSAI_CUDA_TRY(cudaMemset(acc_valid, 0, sizeof(int)));
     BONSAI_CUDA_TRY(dalloc(&group_feat, (size_t)gcap * kMlpFeatures));
     BONSAI_CUDA_TRY(dalloc(&group_counts, (size_t)gcap));
     // the reference reserves nPtcl cells (Treecode.h:192); a Plummer tree at
@@ -473,11 +508,13 @@ struct Handle {
     const int q = par ^ 1;
     k_gather_state<<<nsm * 8, 256, 0, s>>>(pperm, n, pos[par], vel[par], id[par], pos[q], vel[q], id[q]);
     if (precision) k_gather_pos<<<nsm * 8, 256, 0, s>>>(pperm, n, plo[par], plo[q]);
+    acc_in_state_order = false;
     if (bts_K >= 0 && bts_gathering) {
       // levels and the accelerations of inactive particles travel with them
       launch_gather_u8(pperm, n, lev[par], lev[q], nsm * 8, s);
       k_gather_pos<<<nsm * 8, 256, 0, s>>>(pperm, n, acc, acc_alt);
       std::swap(acc, acc_alt);
+      acc_in_state_order = true;
     } else {
       bts_ready = false;  // the levels no longer follow the particle order
     }
@@ -500,18 +537,35 @@ struct Handle {
     cudaMemsetAsync(group_counter, 0, sizeof(unsigned), st);
     cudaMemsetAsync(stats, 0, 4 * sizeof(unsigned long long), st);
     const float* ginv = nullptr;
-    if (theta_mode == 1) {
+    RelativeArgs rel;
+    rel.acc_valid = acc_valid;
+    if (theta_mode == 1 || theta_mode == 3) {
+      // the previous evaluation's accelerations and statistics, through this
+      // step's PH permutation
+      const PrevEval prev = prev_eval();
       launch_group_features(groups, info, pos[par], pkey, rec, nsys > 1 ? sys_box : box, n, ncrit, prm.eps,
-                            group_feat, so(), nsys, root_beg, nsm * 8, st);
-      launch_mlp_infer(group_feat, mlp_wh, info, theta_lo, theta_hi, group_inv, nsm * 4, st);
+                            group_feat, so(), nsys, root_beg, prev, group_amag, nsm * 8, st);
+      if (theta_mode == 1)
+        launch_mlp_infer(group_feat, mlp_wh, info, theta_lo, theta_hi, group_amag, acc_valid, 1.0f / theta_bound,
+                         1.0f / prm.theta, group_inv, group_tau, nsm * 4, st);
+      else
+        launch_relative_tau(info, group_amag, acc_valid, rel_alpha, 1.0f / theta_bound, 1.0f / prm.theta,
+                            group_inv, group_tau, nsm * 4, st);
       ginv = group_inv;
+      rel.tau = group_tau;
     } else if (theta_mode == 2) {
       ginv = group_inv;
+      rel.tau = tau_on ? group_tau : nullptr;
+    }
+    if (ginv) {
+      rel.stats = group_stats;
+      rel.part_gid = part_gid;
     }
     launch_walk(k, walk_blocks[k], groups, info, pos[par], jpos, cell_data, cell_open, cell_q0, cell_q1, cell_ls,
                 ginv, prm.eps * prm.eps, acc, ring, kRingCap, group_counter, stats, &info->status, so(), nsys, root_beg,
                 precision ? plo[par] : nullptr, jlo, cell_lo, ginv ? group_counts : nullptr,
-                walk_list_on ? walk_list : nullptr, walk_list_on ? walk_list_n : nullptr, st);
+                walk_list_on ? walk_list : nullptr, walk_list_on ? walk_list_n : nullptr, rel, st);
+    acc_in_state_order = true;
   }
   void enq_move(bool write) {
     launch_move_wrapper(write);
@@ -601,6 +655,7 @@ struct Handle {
       BONSAI_CUDA_TRY(cudaMemcpyAsync(id[par], si, N * sizeof(int), cudaMemcpyDeviceToDevice, st));
       if (precision) BONSAI_CUDA_TRY(cudaMemcpyAsync(plo[par], sl, N * sizeof(float4), cudaMemcpyDeviceToDevice, st));
       BONSAI_CUDA_TRY(cudaMemcpyAsync(closing, &closing0, sizeof(int), cudaMemcpyHostToDevice, st));
+      BONSAI_CUDA_TRY(cudaMemsetAsync(acc_valid, 0, sizeof(int), st));
       return 0;
     };
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -827,6 +882,7 @@ static int set_particles_impl(Handle* h, const float* pos4, const float* vel4, i
   k_iota<<<h->nsm * 4, 256, 0, h->st>>>(h->id[h->par], n);
   if (h->precision) BONSAI_CUDA_TRY(cudaMemsetAsync(h->plo[h->par], 0, bytes, h->st));  // float input: lo = 0
   BONSAI_CUDA_TRY(cudaMemsetAsync(h->closing, 0, sizeof(int), h->st));
+  BONSAI_CUDA_TRY(cudaMemsetAsync(h->acc_valid, 0, sizeof(int), h->st));  // no previous accelerations
   h->built = h->mp_done = h->grouped = h->forced = h->moved_after_forces = false;
   h->bts_ready = false;
   return last_cuda();
@@ -889,6 +945,7 @@ int bonsai_set_particles_async(bonsai_handle hh, const float* pos4, const float*
   k_iota<<<h->nsm * 4, 256, 0, h->st>>>(h->id[h->par], n);
   if (h->precision) BONSAI_CUDA_TRY(cudaMemsetAsync(h->plo[h->par], 0, bytes, h->st));
   BONSAI_CUDA_TRY(cudaMemsetAsync(h->closing, 0, sizeof(int), h->st));
+  BONSAI_CUDA_TRY(cudaMemsetAsync(h->acc_valid, 0, sizeof(int), h->st));
   h->built = h->mp_done = h->grouped = h->forced = h->moved_after_forces = false;
   h->bts_ready = false;
   return last_cuda();
@@ -1163,6 +1220,7 @@ int bonsai_compute_forces_fp64(bonsai_handle hh, double* acc4, unsigned long lon
   const int nblocks = h->ring_warps / (256 / 32);
   launch_walk64(nblocks, h->groups, h->info, h->pos[h->par], h->precision ? h->plo[h->par] : nullptr, h->jpos,
                 h->jlo, h->cell_data, h->cell_open, h->cell_lo, h->cell_ls, h->theta_mode ? h->group_inv : nullptr,
+                (h->theta_mode == 1 || h->theta_mode == 3 || (h->theta_mode == 2 && h->tau_on)) ? h->group_tau : nullptr,
                 h->rec, e2, h->acc64, h->ring, kRingCap, h->group_counter, h->stats, &h->info->status, h->so(),
                 h->nsys, h->root_beg, h->st);
   if (acc4) {
@@ -1306,7 +1364,7 @@ int bonsai_bounds_check(unsigned* count, unsigned* first_site, int reset) {
   BONSAI_CUDA_TRY(cudaDeviceSynchronize());
   int (*const words[])(unsigned*, bool) = {bounds_word_sort,   bounds_word_tree,   bounds_word_multipoles,
                                            bounds_word_groups, bounds_word_walk,   bounds_word_walk64,
-                                           bounds_word_move};
+                                           bounds_word_move,   bounds_word_learned};
   for (auto f : words) {
     unsigned w[2] = {0u, 0u};
     if (f(w, reset != 0) != 0) return -(int)cudaErrorUnknown - 1000;
@@ -1520,11 +1578,22 @@ int bonsai_direct_fp64(bonsai_handle hh, const int* sample, int ns, int include_
 int bonsai_set_theta_mode(bonsai_handle hh, int mode, float lo, float hi) {
   Handle* h = H(hh);
   if (!h) return BONSAI_ERR_HANDLE;
-  if (mode < 0 || mode > 2 || !(lo > 0.f) || !(hi >= lo)) return BONSAI_ERR_ARG;
+  if (mode < 0 || mode > 3 || !(hi >= lo)) return BONSAI_ERR_ARG;
+  if (mode == 3 && !(lo > 0.f)) return BONSAI_ERR_ARG;  // alpha
   if (mode == 1 && !h->mlp_loaded) return BONSAI_ERR_ORDER;
   h->theta_mode = mode;
   h->theta_lo = lo;
   h->theta_hi = hi;
+  if (mode == 3) h->rel_alpha = lo;
+  h->release_graphs();
+  return 0;
+}
+
+int bonsai_set_relative_bound(bonsai_handle hh, float theta_bound) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (!(theta_bound > 0.f) || !(theta_bound < 100.f)) return BONSAI_ERR_ARG;
+  h->theta_bound = theta_bound;
   h->release_graphs();
   return 0;
 }
@@ -1560,6 +1629,28 @@ int bonsai_set_group_theta(bonsai_handle hh, const float* theta, int ngroups) {
   return last_cuda();
 }
 
+int bonsai_set_group_tau(bonsai_handle hh, const float* tau, int ngroups) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (!tau) {
+    h->tau_on = false;
+    h->release_graphs();
+    return 0;
+  }
+  if (!h->grouped && !h->forced) return BONSAI_ERR_ORDER;
+  if (ngroups < 1 || ngroups > h->gcap) return BONSAI_ERR_ARG;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  int ng = 0;
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(&ng, &h->info->ngroups, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  if (ng != ngroups) return BONSAI_ERR_ARG;
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(h->group_tau, tau, (size_t)ng * 4, cudaMemcpyHostToDevice, h->st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  h->tau_on = true;
+  h->release_graphs();
+  return last_cuda();
+}
+
 int bonsai_get_group_features(bonsai_handle hh, float* out, int* ngroups) {
   Handle* h = H(hh);
   if (!h) return BONSAI_ERR_HANDLE;
@@ -1571,10 +1662,26 @@ int bonsai_get_group_features(bonsai_handle hh, float* out, int* ngroups) {
   BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
   if (ng > h->gcap) return BONSAI_STATUS_GROUP_CAPACITY;
   launch_group_features(h->groups, h->info, h->pos[h->par], h->pkey, h->rec, h->nsys > 1 ? h->sys_box : h->box, h->n,
-                        h->cur_ncrit, h->prm.eps, h->group_feat, h->so(), h->nsys, h->root_beg, h->nsm * 8, h->st);
+                        h->cur_ncrit, h->prm.eps, h->group_feat, h->so(), h->nsys, h->root_beg, h->prev_eval(),
+                        h->group_amag, h->nsm * 8, h->st);
   BONSAI_CUDA_TRY(cudaMemcpyAsync(out, h->group_feat, (size_t)ng * kMlpFeatures * 4, cudaMemcpyDeviceToHost, h->st));
   BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
   *ngroups = ng;
+  return last_cuda();
+}
+
+int bonsai_get_group_scale(bonsai_handle hh, float* out) {
+  Handle* h = H(hh);
+  if (!h) return BONSAI_ERR_HANDLE;
+  if (!out) return BONSAI_ERR_ARG;
+  if (!h->grouped && !h->forced) return BONSAI_ERR_ORDER;
+  BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
+  int ng = 0;
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(&ng, &h->info->ngroups, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
+  if (ng > h->gcap) return BONSAI_STATUS_GROUP_CAPACITY;
+  BONSAI_CUDA_TRY(cudaMemcpyAsync(out, h->group_amag, (size_t)ng * 4, cudaMemcpyDeviceToHost, h->st));
+  BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
   return last_cuda();
 }
 

@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
            int nsys, const int* __restrict__ root_beg, const float4* __restrict__ ipos_lo,
            const float4* __restrict__ jpos_lo, const float4* __restrict__ cell_lo,
            uint2* __restrict__ group_counts, const int* __restrict__ group_list,
-           const unsigned* __restrict__ group_list_n) {
+           const unsigned* __restrict__ group_list_n, const RelativeArgs rel) {
   constexpr int STRIDE = SPLIT ? 16 : 32;
   constexpr int JSTEP = SPLIT ? 2 : 1;
   __shared__ float4 s_a0[kWalkWarps][64];
@@ -220,6 +220,13 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
         !BONSAI_IN_RANGE(pbeg, npart, 0x407))
       continue;
     const float inv_theta_g = PERGROUP ? group_inv_theta[g] : 0.0f;
+    // relative accuracy mode: the group's bound on a cell's truncation error
+    const float tau_g = (PERGROUP && rel.tau) ? rel.tau[g] : 0.0f;
+    // per-group statistics for the next evaluation's features (learned mode):
+    // cells near the opening boundary (count; mass of the accepted ones) and
+    // the force-weighted quadrupole norm of the accepted cells
+    unsigned st_near = 0;
+    float st_mnear = 0.f, st_macc = 0.f, st_qn = 0.f, st_wm = 0.f;
     if (ENS) {
       const int sy = sys_of(sys_off, nsys, pbeg);
       l1b = __ldg(root_beg + sy);
@@ -299,7 +306,25 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
           }
         }
         const bool leaf = cd.y == 0xFFFFFFFFu;
-        const bool split = valid && (open_cell(co, gc, gs) || ((int)(cd.w - cd.z) < 3));
+        bool split = valid && (open_cell(co, gc, gs) || ((int)(cd.w - cd.z) < 3));
+        bool near = false;
+        if (PERGROUP && rel.stats) {
+          // ds within ~20 % of the geometric opening distance
+          const float r = __fdividef(box_dist2(co, gc, gs), fabsf(co.w));
+          near = valid && r > 0.7f && r < 1.45f;
+        }
+        if (PERGROUP && tau_g > 0.0f && valid && !split) {
+          const float m = __ldg(&cell_q0[cell].x), lc = __ldg(&cell_ls[cell].x);
+          split = open_relative(co, gc, gs, m, lc, tau_g);
+          if (rel.stats) {
+            // within a factor 2 of the relative bound (ds within ~15 %)
+            const float ds2 = box_dist2(co, gc, gs);
+            const float rho = __fdividef(__fmul_rn(m, __fmul_rn(lc, __fmul_rn(lc, lc))),
+                                         __fmul_rn(tau_g, __fmul_rn(__fmul_rn(ds2, ds2), __fsqrt_rn(ds2))));
+            near = near || (rho > 0.5f && rho < 2.0f);
+          }
+        }
+        if (PERGROUP && rel.stats) st_near += __popc(__ballot_sync(kFull, near));
 
         // (1) children of opened nodes -> next level
         const int nch = (split && !leaf) ? (int)(cd.y >> 29) + 1 : 0;
@@ -333,6 +358,14 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
           const int slot = (a_head + a_cnt + __popc(bal & lt)) & 63;
           const float4 q1 = __ldg(cell_q1 + cell);
           const float4 q0 = __ldg(cell_q0 + cell);
+          if (PERGROUP && rel.stats) {
+            const float ds2 = fmaxf(box_dist2(co, gc, gs), 1e-30f);
+            const float wf = __fdividef(q0.x, ds2);  // the cell's force share M / ds^2
+            st_macc += q0.x;
+            st_mnear += near ? q0.x : 0.f;
+            st_qn += __fdividef(q1.w * (2.0f / 3.0f), __fmul_rn(ds2, ds2));  // tr I / ds^4 = wf (b / ds)^2
+            st_wm += wf;
+          }
           s_a0[w][slot] = make_float4(co.x, co.y, co.z, q1.w * (-1.0f / 3.0f));
           s_a1[w][slot] = make_float4(q0.x, -q0.y, -q0.z, -q0.w);
           s_a2[w][slot] = make_float4(-q1.x, -q1.y, -q1.z, -q1.w);
@@ -445,11 +478,26 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
     }
     // per-group (approximate, direct) interaction counts, for the per-group angle variant
     if (PERGROUP && group_counts && lane == 0) group_counts[g] = make_uint2(n_app, n_dir);
+    if (PERGROUP && rel.stats) {
+#pragma unroll
+      for (int o = 16; o; o >>= 1) {
+        st_mnear += __shfl_xor_sync(kFull, st_mnear, o);
+        st_macc += __shfl_xor_sync(kFull, st_macc, o);
+        st_qn += __shfl_xor_sync(kFull, st_qn, o);
+        st_wm += __shfl_xor_sync(kFull, st_wm, o);
+      }
+      if (lane == 0)
+        rel.stats[g] = make_float4((float)st_near, st_macc > 0.f ? st_mnear / st_macc : 0.f,
+                                   st_wm > 0.f ? st_qn / st_wm : 0.f, (float)n_app);
+      for (int i = lane; i < np; i += 32) rel.part_gid[pbeg + i] = g;
+    }
     sum_app += (unsigned long long)n_app * (unsigned long long)np;
     sum_dir += (unsigned long long)n_dir * (unsigned long long)np;
     max_app = max(max_app, n_app);
     max_dir = max(max_dir, n_dir);
   }
+  // the accelerations just written are the previous ones of the next evaluation
+  if (rel.acc_valid && blockIdx.x == 0 && threadIdx.x == 0) *rel.acc_valid = 1;
   if (lane == 0) {
     atomicAdd(stats + 0, sum_app);
     atomicAdd(stats + 1, sum_dir);
@@ -509,11 +557,11 @@ void launch_walk(int variant, int nblocks, const int2* groups, const TreeInfo* i
                  float4* acc, int* ring_pool, int ring_cap, unsigned* group_counter, unsigned long long* stats,
                  int* status, const int* sys_off, int nsys, const int* root_beg, const float4* ipos_lo,
                  const float4* jpos_lo, const float4* cell_lo, uint2* group_counts, const int* group_list,
-                 const unsigned* group_list_n, cudaStream_t s) {
+                 const unsigned* group_list_n, const RelativeArgs& rel, cudaStream_t s) {
 #define BONSAI_WALK_ARGS                                                                                          \
   groups, info, ipos, jpos, cell_data, cell_open, cell_q0, cell_q1, cell_ls, group_inv_theta, eps2, acc, ring_pool, \
       ring_cap, group_counter, stats, status, sys_off, nsys, root_beg, ipos_lo, jpos_lo, cell_lo, group_counts,  \
-      group_list, group_list_n
+      group_list, group_list_n, rel
 #define BONSAI_WALK(NI, SP)                                                                \
   do {                                                                                     \
     if (nsys > 1 && ipos_lo && group_inv_theta)                                            \

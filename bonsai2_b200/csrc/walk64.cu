@@ -60,7 +60,8 @@ __global__ void __launch_bounds__(kW64Threads) k_walk64(
     const int2* __restrict__ groups, const TreeInfo* __restrict__ info, const float4* __restrict__ ipos,
     const float4* __restrict__ ipos_lo, const float4* __restrict__ jpos, const float4* __restrict__ jpos_lo,
     const uint4* __restrict__ cell_data, const float4* __restrict__ cell_open, const float4* __restrict__ cell_lo,
-    const float2* __restrict__ cell_ls, const float* __restrict__ group_inv_theta, const MpRec* __restrict__ rec,
+    const float2* __restrict__ cell_ls, const float* __restrict__ group_inv_theta,
+    const float* __restrict__ group_tau, const MpRec* __restrict__ rec,
     double eps2, double4* __restrict__ acc, int* __restrict__ ring_pool, int ring_cap,
     unsigned* __restrict__ group_counter, unsigned long long* __restrict__ stats, int* __restrict__ status,
     const int* __restrict__ sys_off, int nsys, const int* __restrict__ root_beg) {
@@ -83,6 +84,7 @@ __global__ void __launch_bounds__(kW64Threads) k_walk64(
         !BONSAI_IN_RANGE(pbeg, npart, 0x503))
       continue;
     const float inv_theta_g = PERGROUP ? group_inv_theta[g] : 0.0f;
+    const float tau_g = (PERGROUP && group_tau) ? group_tau[g] : 0.0f;
     if (nsys > 1) {  // an ensemble: the group's own system's level-1 cells
       const int sy = sys_of(sys_off, nsys, pbeg);
       l1b = __ldg(root_beg + sy);
@@ -149,7 +151,10 @@ __global__ void __launch_bounds__(kW64Threads) k_walk64(
           }
         }
         const bool leaf = cd.y == 0xFFFFFFFFu;
-        const bool split = valid && (open_cell(co, gc, gs) || ((int)(cd.w - cd.z) < 3));
+        bool split = valid && (open_cell(co, gc, gs) || ((int)(cd.w - cd.z) < 3));
+        // the float walk's relative test on the same float operands
+        if (PERGROUP && tau_g > 0.0f && valid && !split)
+          split = open_relative(co, gc, gs, (float)rec[cell].m, __ldg(&cell_ls[cell].x), tau_g);
         // children of opened nodes -> next level
         const int nch = (split && !leaf) ? (int)(cd.y >> 29) + 1 : 0;
         const int incl = warp_incl_scan(nch);
@@ -230,13 +235,14 @@ __global__ void __launch_bounds__(256) k_scatter_d4(const int* __restrict__ id, 
 
 void launch_walk64(int nblocks, const int2* groups, const TreeInfo* info, const float4* ipos, const float4* ipos_lo,
                    const float4* jpos, const float4* jpos_lo, const uint4* cell_data, const float4* cell_open,
-                   const float4* cell_lo, const float2* cell_ls, const float* group_inv_theta, const MpRec* rec,
-                   double eps2, double4* acc, int* ring_pool, int ring_cap, unsigned* group_counter,
+                   const float4* cell_lo, const float2* cell_ls, const float* group_inv_theta,
+                   const float* group_tau, const MpRec* rec, double eps2, double4* acc, int* ring_pool, int ring_cap, unsigned* group_counter,
                    unsigned long long* stats, int* status, const int* sys_off, int nsys, const int* root_beg,
                    cudaStream_t s) {
 #define BONSAI_W64(DS, PG)                                                                                         \
   k_walk64<DS, PG><<<nblocks, kW64Threads, 0, s>>>(groups, info, ipos, ipos_lo, jpos, jpos_lo, cell_data,          \
-                                                   cell_open, cell_lo, cell_ls, group_inv_theta, rec, eps2, acc,  \
+                                                   cell_open, cell_lo, cell_ls, group_inv_theta, group_tau, rec,  \
+                                                   eps2, acc,                                                     \
                                                    ring_pool, ring_cap, group_counter, stats, status, sys_off,    \
                                                    nsys, root_beg)
   if (ipos_lo) {

@@ -1,15 +1,24 @@
-"""Learned per-group opening angles: training-set generation, training and
+"""Learned per-group opening bounds: training-set generation, training and
 use of the 16 -> 64 -> 64 -> 1 network of csrc/learned.cu.
 
-Training pairs come from the plain method and the FP64 direct sum, both on
-the GPU: for a random subset of groups and a few particles in each, the walk
-runs with every group at each angle of a grid (theta mode 2) and the largest
-angle whose error (geometric mean over the group's sampled particles of
-|da|/|a| against the direct sum) stays below the target is the label.  The
-network is trained with the library's own forward/backward kernels
-(bonsai_mlp_train, Adam, full batch) and used in theta mode 1, where a
-feature kernel and an FP16-weight inference kernel set each group's angle
-inside the step.
+The learned form walks in the relative accuracy mode: a cell that passes the
+geometric test at the safety angle theta_bound is still opened when its
+octupole truncation error M l^3 / ds^5 exceeds the group's bound
+tau_g = A_g 10^y_g, A_g being the group's mean |a| of the previous force
+evaluation and y_g the network's output.  Training pairs come from the walk
+and the FP64 direct sum, both on the GPU: for a random subset of groups and a
+few particles in each, the walk runs with every group at each y of a grid
+(theta mode 2 with host bounds) and the largest y whose error (geometric mean
+over the group's sampled particles of |da|/|a| against the direct sum) stays
+below the target is the label.  The network is trained with the library's
+own forward/backward kernels (bonsai_mlp_train, Adam, full batch) and used in
+theta mode 1, where a feature kernel and an FP16-weight inference kernel set
+each group's bound inside the step.  calibrate_relative then shifts the
+output range by one constant so that the median error on a training system
+is a chosen fraction of the target.
+
+The per-group geometric angle (theta mode 2 without bounds) stays available;
+training_tables / allocation_labels analyse it.
 """
 from __future__ import annotations
 
@@ -22,7 +31,15 @@ from .treecode import Treecode, _check, _p
 
 NFEAT = 16
 NWEIGHTS = 5313
+# output range of the per-group angle (geometric per-group analysis)
 LO, HI, OVER = 0.25, 1.25, 3.0
+# the learned form: output range of y = log10(tau / A), the safety angle, the
+# grid of y the training tables cover, and the bound of the walk that
+# precedes feature extraction in the tables
+YLO, YHI = -4.0, -0.5
+THETA_BOUND = 1.3
+Y_GRID = tuple(np.round(np.arange(-3.6, -0.79, 0.2), 2))
+ALPHA0 = 1e-2
 
 
 def init_weights(seed: int = 0) -> np.ndarray:
@@ -75,8 +92,35 @@ def set_group_theta(t: Treecode, theta):
     _check(t._L.bonsai_set_group_theta(t.handle, _p(th), th.shape[0]), "set_group_theta")
 
 
-def set_theta_mode(t: Treecode, mode: int, lo=LO, hi=HI):
+def set_theta_mode(t: Treecode, mode: int, lo=None, hi=None):
+    """0: fixed angle; 1: the learned form (lo, hi: output range of
+    y = log10(tau / A), default (YLO, YHI)); 2: per-group angles and bounds
+    from the host; 3: relative mode with one parameter alpha = lo."""
+    if lo is None:
+        lo, hi = (YLO, YHI) if mode == 1 else (LO, HI)
+    if hi is None:
+        hi = lo
     _check(t._L.bonsai_set_theta_mode(t.handle, mode, lo, hi), "set_theta_mode")
+
+
+def set_relative_bound(t: Treecode, theta_bound: float):
+    _check(t._L.bonsai_set_relative_bound(t.handle, float(theta_bound)), "set_relative_bound")
+
+
+def set_group_tau(t: Treecode, tau):
+    if tau is None:
+        _check(t._L.bonsai_set_group_tau(t.handle, None, 0), "set_group_tau")
+        return
+    tau = np.ascontiguousarray(tau, np.float32)
+    _check(t._L.bonsai_set_group_tau(t.handle, _p(tau), tau.shape[0]), "set_group_tau")
+
+
+def group_scale(t: Treecode) -> np.ndarray:
+    """A_g of the current groups (mean |a| of the previous evaluation)."""
+    G = t.tree_info()["ngroups"]
+    out = np.empty(max(G, 1), np.float32)
+    _check(t._L.bonsai_get_group_scale(t.handle, _p(out)), "get_group_scale")
+    return out[:G]
 
 
 def set_weights(t: Treecode, w):
@@ -231,29 +275,101 @@ def allocation_labels(E, C, sizes, thetas, target, fraction=0.9):
     return th[j].astype(np.float32), info
 
 
-def training_set(pos, vel, eps, thetas=DEFAULT_GRID, target=5e-4, samples_per_group=8, max_groups=8192, seed=0,
-                 nleaf=16, ncrit=64, level_split=5, device=0, labels="crossing"):
-    """(features, label theta, error table) for a random subset of groups.
-    labels = "crossing": the angle at which the group's error reaches the
-    target; "allocation": the cost-optimal allocation (allocation_labels)."""
-    F, E, C, sizes = training_tables(pos, vel, eps, thetas, samples_per_group, max_groups, seed, nleaf, ncrit,
-                                     level_split, device)
-    if labels == "allocation":
-        y, _ = allocation_labels(E, C, sizes, thetas, target)
-    else:
-        y = crossing_labels(E, thetas, target)
-    return F, y, E
+# ---------------------------------------------------------------------------
+# the learned form: relative accuracy mode
+# ---------------------------------------------------------------------------
+def _prepare_relative(t: Treecode, nleaf, ncrit, level_split, alpha0, theta_bound):
+    """A relative walk at alpha0 (after the fixed-angle first evaluation) so
+    that acc and the walk statistics are those of a relative walk, then the
+    tree rebuilt from the same positions (same groups, identity
+    permutation): the state the learned features see inside a run."""
+    set_relative_bound(t, theta_bound)
+    set_theta_mode(t, 3, alpha0, alpha0)
+    for _ in range(2):
+        t.buildTree(nleaf)
+        t.computeMultipoles()
+        t.makeGroups(level_split, ncrit)
+        t.computeForces(False)
+    t.buildTree(nleaf)
+    t.computeMultipoles()
+    t.makeGroups(level_split, ncrit)
 
 
-def calibrate(pos, vel, w, eps, target, fraction=0.9, samples=2048, iters=10, nleaf=16, ncrit=64, level_split=5,
-              seed=0, device=0):
-    """Scale c of the network's angle range (every group's angle becomes c
-    times the network's), found by bisection on log c so that the median
-    |da|/|a| of the system (pos, vel) against the FP64 direct sum is
-    fraction * target.  Returns (c, lo * c, hi * c, median error at c).  The
-    network's raw output sits below the target by design (its loss penalises
-    too-large angles more); this one scalar moves it onto the target on a
-    training system."""
+def relative_tables(pos, vel, eps, ys=Y_GRID, samples_per_group=8, max_groups=8192, seed=0, nleaf=16, ncrit=64,
+                    level_split=5, alpha0=ALPHA0, theta_bound=THETA_BOUND, device=0):
+    """For a random subset of groups: features F (g, 16) as the learned walk
+    sees them; the group scale A (g,); error table E (g, k) = geometric mean
+    over the group's sampled particles of |da|/|a| against the FP64 direct sum
+    with every group at tau = A 10^ys[k]; cost table C (g, k) = 64 n_approx +
+    20 n_direct; group sizes (g,)."""
+    n = pos.shape[0]
+    t = Treecode(eps=eps, theta=0.5, ncrit=ncrit, nleaf=nleaf, level_split=level_split, device=device)
+    try:
+        t.alloc(n)
+        t.h_ptclPos[:] = pos
+        t.h_ptclVel[:] = vel
+        t.ptcl_h2d()
+        _prepare_relative(t, nleaf, ncrit, level_split, alpha0, theta_bound)
+        F = group_features(t)
+        A = group_scale(t).astype(np.float64)
+        groups = t.groups()
+        G = groups.shape[0]
+        ids = t.walk_arrays()["ids"]
+        rng = np.random.default_rng(seed)
+        gsel = np.sort(rng.choice(G, min(max_groups, G), replace=False))
+        spos, owner = [], []
+        for k, g in enumerate(gsel):
+            pb, np_ = groups[g]
+            take = rng.choice(np_, min(samples_per_group, np_), replace=False)
+            spos.extend(pb + take)
+            owner.extend([k] * len(take))
+        spos = np.asarray(spos, np.int64)
+        owner = np.asarray(owner, np.int64)
+        ref = t.direct_fp64(ids[spos].astype(np.int32), include_self=True)
+        refn = np.linalg.norm(ref[:, :3], axis=1)
+        set_theta_mode(t, 2)
+        set_group_theta(t, np.full(G, theta_bound, np.float32))
+        E = np.zeros((gsel.shape[0], len(ys)))
+        C = np.zeros((gsel.shape[0], len(ys)))
+        for j, y in enumerate(ys):
+            set_group_tau(t, (A * 10.0 ** y).astype(np.float32))
+            t.computeForces(False)
+            acc = t.walk_arrays()["acc"][spos].astype(np.float64)
+            err = np.linalg.norm(acc[:, :3] - ref[:, :3], axis=1) / refn
+            le = np.log(np.maximum(err, 1e-30))
+            E[:, j] = np.exp(np.bincount(owner, weights=le, minlength=gsel.shape[0]) /
+                             np.bincount(owner, minlength=gsel.shape[0]))
+            cnt = group_interactions(t)[gsel].astype(np.float64)
+            C[:, j] = 64.0 * cnt[:, 0] + 20.0 * cnt[:, 1]
+        set_group_tau(t, None)
+        return F[gsel], A[gsel], E, C, groups[gsel, 1].astype(np.float64)
+    finally:
+        t.close()
+
+
+def relative_training_set(pos, vel, eps, target, ys=Y_GRID, **kw):
+    """(features, label y) pairs: per group the y at which its error reaches
+    the target (crossing_labels over the y grid; larger y is less accurate)."""
+    F, A, E, C, sizes = relative_tables(pos, vel, eps, ys=ys, **kw)
+    return F, crossing_labels(E, ys, target), E
+
+
+def run_relative(t: Treecode, nleaf, ncrit, level_split, evaluations=3):
+    """Force evaluations at the current positions: the first one after
+    loading is the fixed-angle fallback; the later ones use the previous
+    evaluation's accelerations and statistics, as inside a run."""
+    for _ in range(evaluations):
+        t.buildTree(nleaf)
+        t.computeMultipoles()
+        t.makeGroups(level_split, ncrit)
+        t.computeForces(False)
+
+
+def calibrate_relative(pos, vel, w, eps, target, fraction=0.9, samples=2048, iters=10, nleaf=16, ncrit=64,
+                       level_split=5, theta_bound=THETA_BOUND, seed=0, device=0):
+    """Shift c of the network's output range ((YLO + c, YHI + c)), found by
+    bisection so that the median |da|/|a| of the system (pos, vel) against the
+    FP64 direct sum is fraction * target.  Returns (c, lo, hi, median error)."""
     n = pos.shape[0]
     t = Treecode(eps=eps, theta=0.5, ncrit=ncrit, nleaf=nleaf, level_split=level_split, device=device)
     try:
@@ -266,29 +382,27 @@ def calibrate(pos, vel, w, eps, target, fraction=0.9, samples=2048, iters=10, nl
         ref = t.direct_fp64(samp, include_self=True)
         refn = np.linalg.norm(ref[:, :3], axis=1)
         set_weights(t, w)
-        t.buildTree(nleaf)
-        t.computeMultipoles()
-        t.makeGroups(level_split, ncrit)
+        set_relative_bound(t, theta_bound)
 
         def median_err(c):
-            set_theta_mode(t, 1, LO * c, HI * c)
-            t.computeForces(False)
+            set_theta_mode(t, 1, YLO + c, YHI + c)
+            run_relative(t, nleaf, ncrit, level_split, evaluations=2)
             acc = t.get_acc()[samp].astype(np.float64)
             return float(np.median(np.linalg.norm(acc[:, :3] - ref[:, :3], axis=1) / refn))
 
         goal = fraction * target
-        lo_c, hi_c = 0.5, 2.0
+        lo_c, hi_c = -1.5, 1.5
         e_lo, e_hi = median_err(lo_c), median_err(hi_c)
         if e_lo > goal:
-            return lo_c, LO * lo_c, HI * lo_c, e_lo
+            return lo_c, YLO + lo_c, YHI + lo_c, e_lo
         if e_hi < goal:
-            return hi_c, LO * hi_c, HI * hi_c, e_hi
+            return hi_c, YLO + hi_c, YHI + hi_c, e_hi
         for _ in range(iters):
-            mid = float(np.sqrt(lo_c * hi_c))
+            mid = 0.5 * (lo_c + hi_c)
             if median_err(mid) > goal:
                 hi_c = mid
             else:
                 lo_c = mid
-        return lo_c, LO * lo_c, HI * lo_c, median_err(lo_c)
+        return lo_c, YLO + lo_c, YHI + lo_c, median_err(lo_c)
     finally:
         t.close()

@@ -226,25 +226,47 @@ int bonsai_direct_fp64(bonsai_handle h, const int *sample, int ns, int include_s
 int bonsai_direct_fp64_noalloc(const float *d_pos4, int n, const int *d_sample, int ns, double eps2,
                                int include_self, double *d_out, void *stream);
 
-/* ---- per-group opening angles (learned form; no counterpart in the
+/* ---- per-group opening criteria (learned form; no counterpart in the
  * reference, whose angle is one number baked into every cell's opening size,
- * computeMultipoles.cu:168-177) ---- */
+ * computeMultipoles.cu:168-177) ----
+ * The walk opens a cell when the group's box is inside its geometric opening
+ * sphere at the group's angle theta_g (split_node_grav_impbh,
+ * computeForces.cu:30-54), and -- in the relative modes -- also when the cell's
+ * octupole truncation error, M l^3 / ds^5 (M = cell mass, l = cell size,
+ * ds = box-to-centre-of-mass distance), exceeds the group's bound tau_g.
+ * Relative modes take tau_g from A_g, the group's mean |a| of the previous
+ * force evaluation (read through this step's PH permutation); while there is
+ * none (the first evaluation after particles are loaded) every group walks at
+ * the fixed angle, exactly as mode 0.  theta_g is then the safety bound of
+ * bonsai_set_relative_bound. */
 #define BONSAI_MLP_FEATURES 16
 #define BONSAI_MLP_WEIGHTS 5313 /* W1[64][16], b1[64], W2[64][64], b2[64], w3[64], b3 */
-/* mode 0: fixed theta (params); 1: theta_g = lo + (hi-lo)*sigmoid(MLP(features_g))
- * from the weights of bonsai_set_mlp_weights; 2: theta_g from bonsai_set_group_theta.
+/* mode 0: fixed theta (params);
+ * 1 (learned): tau_g = A_g 10^y_g, y_g = lo + (hi-lo)*sigmoid(MLP(features_g))
+ *   from the weights of bonsai_set_mlp_weights;
+ * 2: theta_g from bonsai_set_group_theta, tau_g from bonsai_set_group_tau;
+ * 3 (relative, one parameter): tau_g = lo * A_g (lo = alpha > 0; hi >= lo).
  * Features are clamped to [-10, 10] (degenerate groups, e.g. of a one-particle
  * system, would otherwise give inf or NaN). */
 int bonsai_set_theta_mode(bonsai_handle h, int mode, float lo, float hi);
+/* geometric bound theta_g of the relative modes 1 and 3 (default 1.3) */
+int bonsai_set_relative_bound(bonsai_handle h, float theta_bound);
 int bonsai_set_mlp_weights(bonsai_handle h, const float *w, int nw);
 /* host array of ngroups angles for the current groups (after bonsai_make_groups) */
 int bonsai_set_group_theta(bonsai_handle h, const float *theta, int ngroups);
+/* theta mode 2: host array of ngroups bounds tau_g for the current groups
+ * (tau = NULL: the geometric test only) */
+int bonsai_set_group_tau(bonsai_handle h, const float *tau, int ngroups);
 /* features of the current groups, host float[ngroups * 16] */
 int bonsai_get_group_features(bonsai_handle h, float *out, int *ngroups);
-/* angles used by the last walk in mode 1 or 2, host float[ngroups] */
+/* A_g of the current groups as the last feature computation (a relative-mode
+ * walk or bonsai_get_group_features) found it, host float[ngroups]; 0 when
+ * there were no previous accelerations */
+int bonsai_get_group_scale(bonsai_handle h, float *out);
+/* angles used by the last walk in mode 1, 2 or 3, host float[ngroups] */
 int bonsai_get_group_theta(bonsai_handle h, float *out);
-/* per-group interaction counts of the last walk with per-group angles (theta
- * mode 1 or 2): out[2g] = approximate (cell) and out[2g+1] = direct (particle)
+/* per-group interaction counts of the last walk with per-group criteria (theta
+ * mode 1, 2 or 3): out[2g] = approximate (cell) and out[2g+1] = direct (particle)
  * interactions of group g (the per-group form of computeForces.cu:568-609) */
 int bonsai_get_group_interactions(bonsai_handle h, unsigned *out);
 /* MLP on the GPU, host arrays: loss (mean of 0.5 (theta - y)^2 (1 + over [theta > y]))

@@ -180,7 +180,10 @@ def test_ensemble_double_single_bit_identical_to_alone(eager):
 
 
 def _forces(t, pos, vel, mode=0, theta_g=None, weights=None):
-    """One eager force evaluation with fixed (0), network (1) or given (2) angles."""
+    """Eager force evaluation with fixed (0), network (1) or given (2) angles.
+    The network's relative mode reads the previous evaluation's accelerations:
+    the first evaluation after loading is its fixed-angle fallback, the second
+    uses the network."""
     from bonsai2_b200 import learned
     t.h_ptclPos[:] = pos
     t.h_ptclVel[:] = vel
@@ -188,21 +191,23 @@ def _forces(t, pos, vel, mode=0, theta_g=None, weights=None):
     if mode == 1:
         learned.set_weights(t, weights)
     learned.set_theta_mode(t, mode)
-    t.buildTree(t.nLeaf)
-    t.computeMultipoles()
-    t.makeGroups(5, t.nCrit)
-    if mode == 2:
-        learned.set_group_theta(t, np.full(t.groups().shape[0], theta_g, np.float32))
-    t.computeForces(True)
+    for _ in range(2 if mode == 1 else 1):
+        t.buildTree(t.nLeaf)
+        t.computeMultipoles()
+        t.makeGroups(5, t.nCrit)
+        if mode == 2:
+            learned.set_group_theta(t, np.full(t.groups().shape[0], theta_g, np.float32))
+        t.computeForces(True)
     assert t.synchronize() == 0
     return t.get_acc()
 
 
 def test_ensemble_per_group_angles():
-    """Per-group opening angles inside an ensemble: every group at the fixed
-    angle (mode 2) is the fixed-angle walk bit for bit, and network angles
-    (mode 1, features normalised per system) give each system, bit for bit,
-    what it gets alone."""
+    """Per-group opening criteria inside an ensemble: every group at the fixed
+    angle (mode 2) is the fixed-angle walk bit for bit, and the network's
+    bounds (mode 1: features normalised per system, each group's scale from
+    its system's previous accelerations) give each system, bit for bit, what
+    it gets alone."""
     import bonsai2_b200 as B
     from bonsai2_b200 import learned
     counts = np.array([300, 1, 4000, 57, 9000, 2], np.int32)
@@ -215,10 +220,11 @@ def test_ensemble_per_group_angles():
     assert np.array_equal(a_fixed.view(np.uint32), a_const.view(np.uint32))
     w = learned.init_weights(4)
     a_net = _forces(t, pos, vel, 1, weights=w)
-    th = learned.group_theta(t)
-    # finite everywhere (systems of 1 and 2 particles have degenerate features)
-    # and varying from group to group
-    assert np.isfinite(th).all() and th.std() > 0
+    sc = learned.group_scale(t)
+    # finite everywhere (systems of 1 and 2 particles have degenerate features
+    # and no acceleration but the floor) and varying from group to group
+    assert np.isfinite(sc).all() and (sc > 0).all() and sc.std() > 0
+    assert not np.array_equal(a_net.view(np.uint32), a_fixed.view(np.uint32))
     t.close()
     for s in range(counts.shape[0]):
         b, e = off[s], off[s + 1]
