@@ -669,7 +669,8 @@ def learned_theta(B, L, pos, vel, a, device, sweep):
                    "tau_g = A_g 10^y_g (A_g: the group's mean |a| of the previous evaluation, y_g: the network)"
                    % Lr.THETA_BOUND)
     out["training"] = {"system": "Plummer N=%d seed %d" % (n, a.seed + 1), "pairs": int(X.shape[0]),
-                       "final_loss": loss, "seconds": t_train, "label": "y at which the group's error meets the target",
+                       "final_loss": loss, "seconds": t_train,
+                       "label": "cost-optimal y per group for a geometric-mean error of 0.9 x target (allocation)",
                        "calibration_shift": c, "y_range": [lo, hi], "median_err_on_training_system": e_cal}
     out["double_single"] = compare_to_sweep(
         measure(B, L, pos, vel, samp, ref, weights=w, y_range=(lo, hi), precision=1, **kw), sweep, a.learned_target)

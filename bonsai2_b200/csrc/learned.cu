@@ -10,10 +10,11 @@
 // group's own acceleration puts the error budget where it matters.  Here a
 // 16 -> 64 -> 64 -> 1 network maps group features to y_g = log10(tau_g / A_g),
 // A_g being the group's mean |a| of the previous force evaluation; it is
-// trained on pairs (features, the y at which the group's error against the
-// FP64 direct sum meets the target) that the walk and the direct sum
-// generate (bonsai2_b200/learned.py), with this file's own forward and
-// backward kernels.  theta_g is then a fixed safety bound.  Without previous
+// trained on pairs (features, y label) that the walk and the FP64 direct sum
+// generate (bonsai2_b200/learned.py: each group's error and cost over a grid
+// of y; the label is the cost-optimal y for the error budget, or the y at
+// which the group's error meets the target), with this file's own forward
+// and backward kernels.  theta_g is then a fixed safety bound.  Without previous
 // accelerations (the first evaluation after particles are loaded) every
 // group walks at the fixed angle (theta mode 0's walk, bit for bit).
 //

@@ -41,6 +41,8 @@ struct BoxOf<true> {
   typedef double T;
 };
 
+constexpr int kMpBatch = 4;  // leaf particles loaded ahead of their sums
+
 template <bool DS>
 __device__ __forceinline__ void store_cell(int c, const MpRec& r, const typename BoxOf<DS>::T* bmin,
                                            const typename BoxOf<DS>::T* bmax, float inv_theta, MpRec* __restrict__ rec,
@@ -186,23 +188,35 @@ __global__ void __launch_bounds__(256) k_multipoles(const int* __restrict__ leaf
       }
     }
     double m = 0, s1x = 0, s1y = 0, s1z = 0, q[6] = {0, 0, 0, 0, 0, 0};
-    for (int i = b; i < e; i++) {
-      const float4 p = __ldg(jpos + i);
-      double px = p.x, py = p.y, pz = p.z;
-      if (DS) {
-        const float4 l = __ldg(jlo + i);
-        px += l.x; py += l.y; pz += l.z;
-        mn[0] = (B)fmin((double)mn[0], px); mn[1] = (B)fmin((double)mn[1], py); mn[2] = (B)fmin((double)mn[2], pz);
-        mx[0] = (B)fmax((double)mx[0], px); mx[1] = (B)fmax((double)mx[1], py); mx[2] = (B)fmax((double)mx[2], pz);
-      } else {
-        mn[0] = (B)fminf((float)mn[0], p.x); mn[1] = (B)fminf((float)mn[1], p.y); mn[2] = (B)fminf((float)mn[2], p.z);
-        mx[0] = (B)fmaxf((float)mx[0], p.x); mx[1] = (B)fmaxf((float)mx[1], p.y); mx[2] = (B)fmaxf((float)mx[2], p.z);
+    // four particles' loads in flight before they are summed (in order)
+    for (int i0 = b; i0 < e; i0 += kMpBatch) {
+      float4 pb[kMpBatch], lb[kMpBatch];
+#pragma unroll
+      for (int u = 0; u < kMpBatch; u++) {
+        const int i = min(i0 + u, e - 1);
+        pb[u] = __ldg(jpos + i);
+        if (DS) lb[u] = __ldg(jlo + i);
       }
-      const double w = p.w, dx = px - x0, dy = py - y0, dz = pz - z0;
-      m += w;
-      s1x += w * dx; s1y += w * dy; s1z += w * dz;
-      q[0] += w * dx * dx; q[1] += w * dy * dy; q[2] += w * dz * dz;
-      q[3] += w * dx * dy; q[4] += w * dx * dz; q[5] += w * dy * dz;
+#pragma unroll
+      for (int u = 0; u < kMpBatch; u++) {
+        if (i0 + u >= e) break;
+        const float4 p = pb[u];
+        double px = p.x, py = p.y, pz = p.z;
+        if (DS) {
+          const float4 l = lb[u];
+          px += l.x; py += l.y; pz += l.z;
+          mn[0] = (B)fmin((double)mn[0], px); mn[1] = (B)fmin((double)mn[1], py); mn[2] = (B)fmin((double)mn[2], pz);
+          mx[0] = (B)fmax((double)mx[0], px); mx[1] = (B)fmax((double)mx[1], py); mx[2] = (B)fmax((double)mx[2], pz);
+        } else {
+          mn[0] = (B)fminf((float)mn[0], p.x); mn[1] = (B)fminf((float)mn[1], p.y); mn[2] = (B)fminf((float)mn[2], p.z);
+          mx[0] = (B)fmaxf((float)mx[0], p.x); mx[1] = (B)fmaxf((float)mx[1], p.y); mx[2] = (B)fmaxf((float)mx[2], p.z);
+        }
+        const double w = p.w, dx = px - x0, dy = py - y0, dz = pz - z0;
+        m += w;
+        s1x += w * dx; s1y += w * dy; s1z += w * dz;
+        q[0] += w * dx * dx; q[1] += w * dy * dy; q[2] += w * dz * dz;
+        q[3] += w * dx * dy; q[4] += w * dx * dz; q[5] += w * dy * dz;
+      }
     }
     if (m > 0.0) {
       const double ux = s1x / m, uy = s1y / m, uz = s1z / m;

@@ -89,7 +89,7 @@ struct Handle {
   int* part_gid = nullptr;
   int* acc_valid = nullptr;
   bool tau_on = false;
-  float theta_bound = 1.3f;  // geometric safety bound of the relative modes
+  float theta_bound = 2.0f;  // geometric safety bound of the relative modes
   float rel_alpha = 1e-2f;   // theta mode 3: tau = rel_alpha * A_g
   float* group_feat = nullptr;
   uint2* group_counts = nullptr;  // per-group (approx, direct) counts of the per-group angle walk

@@ -8,9 +8,11 @@ tau_g = A_g 10^y_g, A_g being the group's mean |a| of the previous force
 evaluation and y_g the network's output.  Training pairs come from the walk
 and the FP64 direct sum, both on the GPU: for a random subset of groups and a
 few particles in each, the walk runs with every group at each y of a grid
-(theta mode 2 with host bounds) and the largest y whose error (geometric mean
-over the group's sampled particles of |da|/|a| against the direct sum) stays
-below the target is the label.  The network is trained with the library's
+(theta mode 2 with host bounds), giving each group's error (geometric mean
+over its sampled particles of |da|/|a| against the direct sum) and cost
+(interaction counts) per y; the label is the cost-optimal y for the error
+budget (allocation_labels), or the y at which the group's error reaches the
+target.  The network is trained with the library's
 own forward/backward kernels (bonsai_mlp_train, Adam, full batch) and used in
 theta mode 1, where a feature kernel and an FP16-weight inference kernel set
 each group's bound inside the step.  calibrate_relative then shifts the
@@ -37,7 +39,7 @@ LO, HI, OVER = 0.25, 1.25, 3.0
 # grid of y the training tables cover, and the bound of the walk that
 # precedes feature extraction in the tables
 YLO, YHI = -4.0, -0.5
-THETA_BOUND = 1.3
+THETA_BOUND = 2.0
 Y_GRID = tuple(np.round(np.arange(-3.6, -0.79, 0.2), 2))
 ALPHA0 = 1e-2
 
@@ -347,11 +349,18 @@ def relative_tables(pos, vel, eps, ys=Y_GRID, samples_per_group=8, max_groups=81
         t.close()
 
 
-def relative_training_set(pos, vel, eps, target, ys=Y_GRID, **kw):
-    """(features, label y) pairs: per group the y at which its error reaches
-    the target (crossing_labels over the y grid; larger y is less accurate)."""
+def relative_training_set(pos, vel, eps, target, ys=Y_GRID, labels="allocation", **kw):
+    """(features, label y, error table) pairs.  labels = "allocation": the
+    cost-optimal per-group y for a geometric-mean error of 0.9 * target
+    (allocation_labels on the y grid: where a group's cost falls faster than
+    its error grows it gets a larger y); "crossing": the y at which the
+    group's own error reaches the target (every group equally accurate)."""
     F, A, E, C, sizes = relative_tables(pos, vel, eps, ys=ys, **kw)
-    return F, crossing_labels(E, ys, target), E
+    if labels == "allocation":
+        y, _ = allocation_labels(E, C, sizes, ys, target)
+    else:
+        y = crossing_labels(E, ys, target)
+    return F, y, E
 
 
 def run_relative(t: Treecode, nleaf, ncrit, level_split, evaluations=3):

@@ -249,7 +249,7 @@ int bonsai_direct_fp64_noalloc(const float *d_pos4, int n, const int *d_sample, 
  * Features are clamped to [-10, 10] (degenerate groups, e.g. of a one-particle
  * system, would otherwise give inf or NaN). */
 int bonsai_set_theta_mode(bonsai_handle h, int mode, float lo, float hi);
-/* geometric bound theta_g of the relative modes 1 and 3 (default 1.3) */
+/* geometric bound theta_g of the relative modes 1 and 3 (default 2.0) */
 int bonsai_set_relative_bound(bonsai_handle h, float theta_bound);
 int bonsai_set_mlp_weights(bonsai_handle h, const float *w, int nw);
 /* host array of ngroups angles for the current groups (after bonsai_make_groups) */
