@@ -13,7 +13,7 @@
 //   M, COM; Q = second moment about the COM per unit mass (:148-158);
 //   particle bounding box -> l = max(2 max h, 1e-6), s = |cvec - COM|,
 //   cellOp = l/theta + s, stored squared (:168-177).
-// cell_ls = (l, s) lets a walk with per-group opening angles form
+// cell_ls = (l, s, M l^3, 0) lets a walk with per-group opening angles form
 // (l/theta_g + s)^2.  Stored for the walk (mass-weighted, pre-scaled so the
 // force kernel needs fewer operations):  cell_q0 = (M, 3Ixx, 3Iyy, 3Izz),
 // cell_q1 = (3Ixy, 3Ixz, 3Iyz, 1.5 tr I), with I = M Q.
@@ -48,7 +48,7 @@ __device__ __forceinline__ void store_cell(int c, const MpRec& r, const typename
                                            const typename BoxOf<DS>::T* bmax, float inv_theta, MpRec* __restrict__ rec,
                                            typename BoxOf<DS>::T* __restrict__ box, float4* __restrict__ cell_open,
                                            float4* __restrict__ cell_q0, float4* __restrict__ cell_q1,
-                                           float2* __restrict__ cell_ls, float4* __restrict__ cell_lo) {
+                                           float4* __restrict__ cell_ls, float4* __restrict__ cell_lo) {
   rec[c] = r;
   for (int k = 0; k < 3; k++) { box[6 * (size_t)c + k] = bmin[k]; box[6 * (size_t)c + 3 + k] = bmax[k]; }
   const float cx = (float)r.cx, cy = (float)r.cy, cz = (float)r.cz;
@@ -78,7 +78,10 @@ __device__ __forceinline__ void store_cell(int c, const MpRec& r, const typename
   }
   const float op = __fmaf_rn(l, inv_theta, s);
   cell_open[c] = make_float4(cx, cy, cz, __fmul_rn(op, op));
-  cell_ls[c] = make_float2(l, s);  // per-group opening angles recompute (l/theta_g + s)^2
+  // per-group opening angles recompute (l/theta_g + s)^2; the relative test
+  // compares M l^3 (formed once here, in float) with tau ds^5
+  const float mf = (float)r.m;
+  cell_ls[c] = make_float4(l, s, __fmul_rn(mf, __fmul_rn(l, __fmul_rn(l, l))), 0.0f);
   const double tr = r.ixx + r.iyy + r.izz;
   cell_q0[c] = make_float4((float)r.m, (float)(3.0 * r.ixx), (float)(3.0 * r.iyy), (float)(3.0 * r.izz));
   cell_q1[c] = make_float4((float)(3.0 * r.ixy), (float)(3.0 * r.ixz), (float)(3.0 * r.iyz), (float)(1.5 * tr));
@@ -100,7 +103,7 @@ __device__ void climb(int c, [[maybe_unused]] int ncells, const uint4* __restric
                       const int* __restrict__ cell_parent,
                       float inv_theta, MpRec* __restrict__ rec, typename BoxOf<DS>::T* __restrict__ box,
                       float4* __restrict__ cell_open, float4* __restrict__ cell_q0, float4* __restrict__ cell_q1,
-                      float2* __restrict__ cell_ls, int* __restrict__ mp_count, float4* __restrict__ cell_lo) {
+                      float4* __restrict__ cell_ls, int* __restrict__ mp_count, float4* __restrict__ cell_lo) {
   typedef typename BoxOf<DS>::T B;
   while (true) {
     const int p = cell_parent[c];
@@ -159,7 +162,7 @@ __global__ void __launch_bounds__(256) k_multipoles(const int* __restrict__ leaf
                                                     const float4* __restrict__ jpos, float inv_theta,
                                                     MpRec* __restrict__ rec, typename BoxOf<DS>::T* __restrict__ box,
                                                     float4* __restrict__ cell_open, float4* __restrict__ cell_q0,
-                                                    float4* __restrict__ cell_q1, float2* __restrict__ cell_ls,
+                                                    float4* __restrict__ cell_q1, float4* __restrict__ cell_ls,
                                                     int* __restrict__ mp_count, int cell_cap,
                                                     const float4* __restrict__ jlo, float4* __restrict__ cell_lo) {
   typedef typename BoxOf<DS>::T B;
@@ -269,7 +272,7 @@ __global__ void __launch_bounds__(256) k_multipoles(const int* __restrict__ leaf
 
 void launch_multipoles(const int* leaf_list, const TreeInfo* info, const uint4* cell_data, const int* cell_parent,
                        const float4* jpos, float inv_theta, MpRec* rec, void* box, float4* cell_open,
-                       float4* cell_q0, float4* cell_q1, float2* cell_ls, int* mp_count, int cell_cap,
+                       float4* cell_q0, float4* cell_q1, float4* cell_ls, int* mp_count, int cell_cap,
                        const float4* jlo, float4* cell_lo, int nblocks, cudaStream_t s) {
   if (jlo)
     k_multipoles<true><<<nblocks, 256, 0, s>>>(leaf_list, info, cell_data, cell_parent, jpos, inv_theta, rec,

@@ -32,7 +32,6 @@ constexpr int kTreeItems = 16;
 constexpr int kTreeTile = kTreeThreads * kTreeItems;  // 4096
 constexpr int kHalo = 64;                              // max nLeaf
 constexpr int kNL = kMaxLevel + 1;                     // rows 0..21 (row 0 unused)
-constexpr int kNodeScan = 384;  // node runs up to this long are resolved from the tile's d values
 
 int tree_tiles(int n) { return (n + kTreeTile - 1) / kTreeTile; }
 
@@ -335,23 +334,7 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_cells(
           if ((int)sd[loc + j] <= L) { pend = i + j; small_leaf = true; break; }
         }
       }
-      // A node's run [i, pend) ends at the first later position whose d is
-      // <= L, and its children start at i and at every position inside with
-      // d == L + 1: for runs that end inside this tile's window the d values
-      // in shared memory give both (d is 0 at n and at system starts, so the
-      // scan stops there too); longer runs are searched in the keys.
-      int nbound = 0;  // children after the first (at most 7)
-      bool scanned = false;
-      if (!leaf) {
-        const int jmax = min(kTreeTile + 2 * kHalo, loc + 1 + kNodeScan);
-        for (int j = loc + 1; j < jmax; j++) {
-          const int dj = (int)sd[j];
-          if (dj <= L) { pend = i + (j - loc); scanned = true; break; }
-          nbound += (dj == L + 1);
-        }
-        nbound = min(nbound, 7);
-      }
-      if (!small_leaf && !scanned) {
+      if (!small_leaf) {
         // keys increase only inside a system: search up to the system's end
         const int send = nsys > 1 ? sys_off[sys_of(sys_off, nsys, i) + 1] : n;
         pend = gallop_u64(keys, min(i + nleaf + 1, send), send, (pre + 1ull) << sh);
@@ -369,45 +352,32 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_cells(
         int lc1 = 0;
         for (int q = 0; q < k; q++) lc1 += (ca[q] && ca[q] <= L + 1 && L + 1 <= cb[q]);
         const int first = (int)(boff[0][L + 1] + cpre[L + 1][threadIdx.x]) + lc1;
-        int nch = 0;
-        if (scanned) {
-          // children start at i and at the scanned boundaries, in key order;
-          // each child's own thread writes its range
-          for (int c = 0; c <= nbound; c++) {
-            if (BONSAI_IN_RANGE(first + c, ncells, 0x106)) {
-              cell_data[first + c].x = (unsigned)cidx | ((unsigned)(L + 1) << 27);
-              cell_parent[first + c] = cidx;
-            }
-          }
-          nch = nbound + 1;
-        } else {
-          // the 7 inner octant boundaries are independent lower bounds over
-          // [i, pend): searched in lock-step, 7 loads in flight per step
-          int bl[8], bh[8];
+        // the 7 inner octant boundaries are independent lower bounds over
+        // [i, pend): searched in lock-step, 7 loads in flight per step
+        int bl[8], bh[8];
 #pragma unroll
-          for (int o = 1; o < 8; o++) { bl[o] = i; bh[o] = pend; }
-          for (int span = pend - i; span > 0; span >>= 1) {
+        for (int o = 1; o < 8; o++) { bl[o] = i; bh[o] = pend; }
+        for (int span = pend - i; span > 0; span >>= 1) {
 #pragma unroll
-            for (int o = 1; o < 8; o++) {
-              if (bl[o] < bh[o]) {
-                const int mid = (bl[o] + bh[o]) >> 1;
-                if (__ldg(keys + mid) < (((pre << 3) | (unsigned long long)o) << (sh - 3))) bl[o] = mid + 1;
-                else bh[o] = mid;
-              }
+          for (int o = 1; o < 8; o++) {
+            if (bl[o] < bh[o]) {
+              const int mid = (bl[o] + bh[o]) >> 1;
+              if (__ldg(keys + mid) < (((pre << 3) | (unsigned long long)o) << (sh - 3))) bl[o] = mid + 1;
+              else bh[o] = mid;
             }
           }
-          int lo = i;
-          for (int o = 1; o <= 8; o++) {
-            const int bnd = (o == 8) ? pend : bl[o];
-            if (bnd > lo) {
-              if (BONSAI_IN_RANGE(first + nch, ncells, 0x103)) {
-                cell_data[first + nch].x = (unsigned)cidx | ((unsigned)(L + 1) << 27);
-                cell_parent[first + nch] = cidx;
-              }
-              nch++;
+        }
+        int nch = 0, lo = i;
+        for (int o = 1; o <= 8; o++) {
+          const int bnd = (o == 8) ? pend : bl[o];
+          if (bnd > lo) {
+            if (BONSAI_IN_RANGE(first + nch, ncells, 0x103)) {
+              cell_data[first + nch].x = (unsigned)cidx | ((unsigned)(L + 1) << 27);
+              cell_parent[first + nch] = cidx;
             }
-            lo = bnd;
+            nch++;
           }
+          lo = bnd;
         }
         ywd = (unsigned)first | ((unsigned)(nch - 1) << 29);
       }

@@ -73,7 +73,7 @@ struct Handle {
   int *cell_parent = nullptr, *leaf_list = nullptr, *mp_count = nullptr;
   MpRec* rec = nullptr;
   double* cell_box = nullptr;  // 6 per cell: floats (float positions) or doubles (double-single)
-  float2* cell_ls = nullptr;
+  float4* cell_ls = nullptr;
   // per-group opening angles (theta mode 1: MLP, 2: caller's array)
   int theta_mode = 0;
   float theta_lo = 0.25f, theta_hi = 1.25f;

@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
     k_walk(const int2* __restrict__ groups, const TreeInfo* __restrict__ info, const float4* __restrict__ ipos,
            const float4* __restrict__ jpos, const uint4* __restrict__ cell_data,
            const float4* __restrict__ cell_open, const float4* __restrict__ cell_q0,
-           const float4* __restrict__ cell_q1, const float2* __restrict__ cell_ls,
+           const float4* __restrict__ cell_q1, const float4* __restrict__ cell_ls,
            const float* __restrict__ group_inv_theta, float eps2, float4* __restrict__ acc,
            int* __restrict__ ring_pool, int ring_cap, unsigned* __restrict__ group_counter,
            unsigned long long* __restrict__ stats, int* __restrict__ status, const int* __restrict__ sys_off,
@@ -290,6 +290,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
         const bool valid = inlist && BONSAI_IN_RANGE(cell, ncells, 0x404);
         uint4 cd = make_uint4(0u, 0xFFFFFFFFu, 0u, 0u);
         float4 co = make_float4(0.f, 0.f, 0.f, 0.f);
+        float mk = 0.f;  // M l^3 (relative test)
         if (valid) {
           cd = __ldg(cell_data + cell);
           co = __ldg(cell_open + cell);
@@ -300,9 +301,10 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
             co.z = __fadd_rn(__fsub_rn(co.z, R.z), cl.z);
           }
           if (PERGROUP) {
-            const float2 ls = __ldg(cell_ls + cell);
+            const float4 ls = __ldg(cell_ls + cell);
             const float op = __fmaf_rn(ls.x, inv_theta_g, ls.y);
             co.w = __fmul_rn(op, op);
+            mk = ls.z;
           }
         }
         const bool leaf = cd.y == 0xFFFFFFFFu;
@@ -314,13 +316,11 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
           near = valid && r > 0.7f && r < 1.45f;
         }
         if (PERGROUP && tau_g > 0.0f && valid && !split) {
-          const float m = __ldg(&cell_q0[cell].x), lc = __ldg(&cell_ls[cell].x);
-          split = open_relative(co, gc, gs, m, lc, tau_g);
+          split = open_relative(co, gc, gs, mk, tau_g);
           if (rel.stats) {
             // within a factor 2 of the relative bound (ds within ~15 %)
             const float ds2 = box_dist2(co, gc, gs);
-            const float rho = __fdividef(__fmul_rn(m, __fmul_rn(lc, __fmul_rn(lc, lc))),
-                                         __fmul_rn(tau_g, __fmul_rn(__fmul_rn(ds2, ds2), __fsqrt_rn(ds2))));
+            const float rho = __fdividef(mk, __fmul_rn(tau_g, __fmul_rn(__fmul_rn(ds2, ds2), __fsqrt_rn(ds2))));
             near = near || (rho > 0.5f && rho < 2.0f);
           }
         }
@@ -553,7 +553,7 @@ int walk_blocks_per_sm(int variant) {
 
 void launch_walk(int variant, int nblocks, const int2* groups, const TreeInfo* info, const float4* ipos,
                  const float4* jpos, const uint4* cell_data, const float4* cell_open, const float4* cell_q0,
-                 const float4* cell_q1, const float2* cell_ls, const float* group_inv_theta, float eps2,
+                 const float4* cell_q1, const float4* cell_ls, const float* group_inv_theta, float eps2,
                  float4* acc, int* ring_pool, int ring_cap, unsigned* group_counter, unsigned long long* stats,
                  int* status, const int* sys_off, int nsys, const int* root_beg, const float4* ipos_lo,
                  const float4* jpos_lo, const float4* cell_lo, uint2* group_counts, const int* group_list,

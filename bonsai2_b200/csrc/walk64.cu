@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(kW64Threads) k_walk64(
     const int2* __restrict__ groups, const TreeInfo* __restrict__ info, const float4* __restrict__ ipos,
     const float4* __restrict__ ipos_lo, const float4* __restrict__ jpos, const float4* __restrict__ jpos_lo,
     const uint4* __restrict__ cell_data, const float4* __restrict__ cell_open, const float4* __restrict__ cell_lo,
-    const float2* __restrict__ cell_ls, const float* __restrict__ group_inv_theta,
+    const float4* __restrict__ cell_ls, const float* __restrict__ group_inv_theta,
     const float* __restrict__ group_tau, const MpRec* __restrict__ rec,
     double eps2, double4* __restrict__ acc, int* __restrict__ ring_pool, int ring_cap,
     unsigned* __restrict__ group_counter, unsigned long long* __restrict__ stats, int* __restrict__ status,
@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(kW64Threads) k_walk64(
             co.z = __fadd_rn(__fsub_rn(co.z, R.z), cl.z);
           }
           if (PERGROUP) {
-            const float2 ls = __ldg(cell_ls + cell);
+            const float4 ls = __ldg(cell_ls + cell);
             const float op = __fmaf_rn(ls.x, inv_theta_g, ls.y);
             co.w = __fmul_rn(op, op);
           }
@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(kW64Threads) k_walk64(
         bool split = valid && (open_cell(co, gc, gs) || ((int)(cd.w - cd.z) < 3));
         // the float walk's relative test on the same float operands
         if (PERGROUP && tau_g > 0.0f && valid && !split)
-          split = open_relative(co, gc, gs, (float)rec[cell].m, __ldg(&cell_ls[cell].x), tau_g);
+          split = open_relative(co, gc, gs, __ldg(&cell_ls[cell].z), tau_g);
         // children of opened nodes -> next level
         const int nch = (split && !leaf) ? (int)(cd.y >> 29) + 1 : 0;
         const int incl = warp_incl_scan(nch);
@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(256) k_scatter_d4(const int* __restrict__ id, 
 
 void launch_walk64(int nblocks, const int2* groups, const TreeInfo* info, const float4* ipos, const float4* ipos_lo,
                    const float4* jpos, const float4* jpos_lo, const uint4* cell_data, const float4* cell_open,
-                   const float4* cell_lo, const float2* cell_ls, const float* group_inv_theta,
+                   const float4* cell_lo, const float4* cell_ls, const float* group_inv_theta,
                    const float* group_tau, const MpRec* rec, double eps2, double4* acc, int* ring_pool, int ring_cap, unsigned* group_counter,
                    unsigned long long* stats, int* status, const int* sys_off, int nsys, const int* root_beg,
                    cudaStream_t s) {

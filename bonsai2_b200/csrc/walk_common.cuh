@@ -27,12 +27,12 @@ __device__ __forceinline__ bool open_cell(const float4 co, const float3 gc, cons
 // passes the geometric test is still opened when the octupole truncation
 // error of its quadrupole expansion, of order M l^3 / ds^5, exceeds the
 // group's bound tau (tau = alpha |a| of the group: the relative error
-// criterion of tree codes with a relative opening rule).
-__device__ __forceinline__ bool open_relative(const float4 co, const float3 gc, const float3 gs, float m, float l,
-                                              float tau) {
+// criterion of tree codes with a relative opening rule).  mk = M l^3 as the
+// multipole kernel stored it (cell_ls.z).
+__device__ __forceinline__ bool open_relative(const float4 co, const float3 gc, const float3 gs, float mk, float tau) {
   const float ds2 = box_dist2(co, gc, gs);
   const float ds5 = __fmul_rn(__fmul_rn(ds2, ds2), __fsqrt_rn(ds2));
-  return __fmul_rn(m, __fmul_rn(l, __fmul_rn(l, l))) > __fmul_rn(tau, ds5);
+  return mk > __fmul_rn(tau, ds5);
 }
 
 // binary search over the warp's inclusive scan: the lane whose range holds s
