@@ -21,6 +21,8 @@
 // box is a separate array, float for float positions and double (DS) for
 // double-single positions, where particles enter the FP64 sums as hi + lo,
 // extents are exact, and the COM is stored as hi (cell_open) plus lo (cell_lo).
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -28,6 +30,13 @@ namespace bonsai {
 
 // leaf moments in one pass over the particles (1) or two (0: centre of mass,
 // then central moments)
+// parents level by level, one launch per level from the deepest (0: 6.55 ms
+// build phase at N = 2^24), or by the last-arriving child's climb with an
+// arrival counter per cell (1: 6.99 ms; fences and atomics serialise its
+// tail through the top levels); both bit-identical
+#ifndef BONSAI_MP_CLIMB
+#define BONSAI_MP_CLIMB 0
+#endif
 #ifndef BONSAI_MP_ONE_PASS
 #define BONSAI_MP_ONE_PASS 1
 #endif
@@ -97,6 +106,51 @@ __device__ __forceinline__ bool arrive_last(int* p, int nch) {
   return true;
 }
 
+// A parent's moments from its nch contiguous children (parallel-axis
+// theorem, FP64), the children taken in index order.
+template <bool DS>
+__device__ void combine_children(int p, int first, int nch, float inv_theta, MpRec* __restrict__ rec,
+                                 typename BoxOf<DS>::T* __restrict__ box, float4* __restrict__ cell_open,
+                                 float4* __restrict__ cell_q0, float4* __restrict__ cell_q1,
+                                 float4* __restrict__ cell_ls, float4* __restrict__ cell_lo) {
+  typedef typename BoxOf<DS>::T B;
+  double M = 0, X = 0, Y = 0, Z = 0;
+  B bmn[3] = {(B)3.0e38, (B)3.0e38, (B)3.0e38}, bmx[3] = {(B)-3.0e38, (B)-3.0e38, (B)-3.0e38};
+  for (int k = 0; k < nch; k++) {
+    const MpRec* ck = rec + first + k;
+    const double mk = __ldcg(&ck->m);
+    M += mk;
+    X += mk * __ldcg(&ck->cx); Y += mk * __ldcg(&ck->cy); Z += mk * __ldcg(&ck->cz);
+    const B* bk = box + 6 * (size_t)(first + k);
+    for (int a = 0; a < 3; a++) {
+      bmn[a] = DS ? (B)fmin((double)bmn[a], (double)__ldcg(bk + a)) : (B)fminf((float)bmn[a], (float)__ldcg(bk + a));
+      bmx[a] = DS ? (B)fmax((double)bmx[a], (double)__ldcg(bk + 3 + a))
+                  : (B)fmaxf((float)bmx[a], (float)__ldcg(bk + 3 + a));
+    }
+  }
+  MpRec P;
+  if (M > 0.0) { P.cx = X / M; P.cy = Y / M; P.cz = Z / M; }
+  else {
+    P.cx = 0.5 * ((double)bmn[0] + bmx[0]); P.cy = 0.5 * ((double)bmn[1] + bmx[1]);
+    P.cz = 0.5 * ((double)bmn[2] + bmx[2]);
+  }
+  double I[6] = {0, 0, 0, 0, 0, 0};
+  for (int k = 0; k < nch; k++) {
+    const MpRec* ck = rec + first + k;
+    const double mk = __ldcg(&ck->m);
+    const double dx = __ldcg(&ck->cx) - P.cx, dy = __ldcg(&ck->cy) - P.cy, dz = __ldcg(&ck->cz) - P.cz;
+    I[0] += __ldcg(&ck->ixx) + mk * dx * dx;
+    I[1] += __ldcg(&ck->iyy) + mk * dy * dy;
+    I[2] += __ldcg(&ck->izz) + mk * dz * dz;
+    I[3] += __ldcg(&ck->ixy) + mk * dx * dy;
+    I[4] += __ldcg(&ck->ixz) + mk * dx * dz;
+    I[5] += __ldcg(&ck->iyz) + mk * dy * dz;
+  }
+  P.m = M;
+  P.ixx = I[0]; P.iyy = I[1]; P.izz = I[2]; P.ixy = I[3]; P.ixz = I[4]; P.iyz = I[5];
+  store_cell<DS>(p, P, bmn, bmx, inv_theta, rec, box, cell_open, cell_q0, cell_q1, cell_ls, cell_lo);
+}
+
 // Combines parents bottom-up while this thread is the last child to arrive.
 template <bool DS>
 __device__ void climb(int c, [[maybe_unused]] int ncells, const uint4* __restrict__ cell_data,
@@ -104,7 +158,6 @@ __device__ void climb(int c, [[maybe_unused]] int ncells, const uint4* __restric
                       float inv_theta, MpRec* __restrict__ rec, typename BoxOf<DS>::T* __restrict__ box,
                       float4* __restrict__ cell_open, float4* __restrict__ cell_q0, float4* __restrict__ cell_q1,
                       float4* __restrict__ cell_ls, int* __restrict__ mp_count, float4* __restrict__ cell_lo) {
-  typedef typename BoxOf<DS>::T B;
   while (true) {
     const int p = cell_parent[c];
     if (p < 0) break;
@@ -113,49 +166,36 @@ __device__ void climb(int c, [[maybe_unused]] int ncells, const uint4* __restric
     const int first = (int)(y & 0x1FFFFFFFu), nch = (int)(y >> 29) + 1;
     if (!BONSAI_IN_RANGE(first + nch - 1, ncells, 0x304) || !BONSAI_IN_RANGE(c - first, nch, 0x305)) break;
     if (!arrive_last(mp_count + p, nch)) break;
-    double M = 0, X = 0, Y = 0, Z = 0;
-    B bmn[3] = {(B)3.0e38, (B)3.0e38, (B)3.0e38}, bmx[3] = {(B)-3.0e38, (B)-3.0e38, (B)-3.0e38};
-    for (int k = 0; k < nch; k++) {
-      const MpRec* ck = rec + first + k;
-      const double mk = __ldcg(&ck->m);
-      M += mk;
-      X += mk * __ldcg(&ck->cx); Y += mk * __ldcg(&ck->cy); Z += mk * __ldcg(&ck->cz);
-      const B* bk = box + 6 * (size_t)(first + k);
-      for (int a = 0; a < 3; a++) {
-        bmn[a] = DS ? (B)fmin((double)bmn[a], (double)__ldcg(bk + a)) : (B)fminf((float)bmn[a], (float)__ldcg(bk + a));
-        bmx[a] = DS ? (B)fmax((double)bmx[a], (double)__ldcg(bk + 3 + a))
-                    : (B)fmaxf((float)bmx[a], (float)__ldcg(bk + 3 + a));
-      }
-    }
-    MpRec P;
-    if (M > 0.0) { P.cx = X / M; P.cy = Y / M; P.cz = Z / M; }
-    else {
-      P.cx = 0.5 * ((double)bmn[0] + bmx[0]); P.cy = 0.5 * ((double)bmn[1] + bmx[1]);
-      P.cz = 0.5 * ((double)bmn[2] + bmx[2]);
-    }
-    double I[6] = {0, 0, 0, 0, 0, 0};
-    for (int k = 0; k < nch; k++) {
-      const MpRec* ck = rec + first + k;
-      const double mk = __ldcg(&ck->m);
-      const double dx = __ldcg(&ck->cx) - P.cx, dy = __ldcg(&ck->cy) - P.cy, dz = __ldcg(&ck->cz) - P.cz;
-      I[0] += __ldcg(&ck->ixx) + mk * dx * dx;
-      I[1] += __ldcg(&ck->iyy) + mk * dy * dy;
-      I[2] += __ldcg(&ck->izz) + mk * dz * dz;
-      I[3] += __ldcg(&ck->ixy) + mk * dx * dy;
-      I[4] += __ldcg(&ck->ixz) + mk * dx * dz;
-      I[5] += __ldcg(&ck->iyz) + mk * dy * dz;
-    }
-    P.m = M;
-    P.ixx = I[0]; P.iyy = I[1]; P.izz = I[2]; P.ixy = I[3]; P.ixz = I[4]; P.iyz = I[5];
-    store_cell<DS>(p, P, bmn, bmx, inv_theta, rec, box, cell_open, cell_q0, cell_q1, cell_ls, cell_lo);
+    combine_children<DS>(p, first, nch, inv_theta, rec, box, cell_open, cell_q0, cell_q1, cell_ls, cell_lo);
     c = p;
+  }
+}
+
+// The nodes of one level from their children, one thread per cell (leaves
+// were done by the leaf pass): the level-by-level form of the climb.
+template <bool DS>
+__global__ void __launch_bounds__(256) k_mp_level(int L, const TreeInfo* __restrict__ info,
+                                                  const uint4* __restrict__ cell_data, float inv_theta,
+                                                  MpRec* __restrict__ rec, typename BoxOf<DS>::T* __restrict__ box,
+                                                  float4* __restrict__ cell_open, float4* __restrict__ cell_q0,
+                                                  float4* __restrict__ cell_q1, float4* __restrict__ cell_ls,
+                                                  int cell_cap, float4* __restrict__ cell_lo) {
+  if (info->ncells > cell_cap) return;
+  [[maybe_unused]] const int ncells = info->ncells;
+  const int b = info->level_beg[L], e = info->level_end[L];
+  for (int c = b + blockIdx.x * blockDim.x + threadIdx.x; c < e; c += gridDim.x * blockDim.x) {
+    const unsigned y = cell_data[c].y;
+    if (y == 0xFFFFFFFFu) continue;
+    const int first = (int)(y & 0x1FFFFFFFu), nch = (int)(y >> 29) + 1;
+    if (!BONSAI_IN_RANGE(first + nch - 1, ncells, 0x307)) continue;
+    combine_children<DS>(c, first, nch, inv_theta, rec, box, cell_open, cell_q0, cell_q1, cell_ls, cell_lo);
   }
 }
 
 // One thread per leaf: the leaf's moments (one pass by default), then the
 // bottom-up climb.  (Half-warp-cooperative leaves
 // with shuffle reductions were measured 13x slower on the B200.)
-template <bool DS>
+template <bool DS, bool CLIMB>
 __global__ void __launch_bounds__(256) k_multipoles(const int* __restrict__ leaf_list, const TreeInfo* __restrict__ info,
                                                     const uint4* __restrict__ cell_data,
                                                     const int* __restrict__ cell_parent,
@@ -266,7 +306,9 @@ __global__ void __launch_bounds__(256) k_multipoles(const int* __restrict__ leaf
     r.m = m;
     r.ixx = q[0]; r.iyy = q[1]; r.izz = q[2]; r.ixy = q[3]; r.ixz = q[4]; r.iyz = q[5];
     store_cell<DS>(c, r, mn, mx, inv_theta, rec, box, cell_open, cell_q0, cell_q1, cell_ls, cell_lo);
-    climb<DS>(c, ncells, cell_data, cell_parent, inv_theta, rec, box, cell_open, cell_q0, cell_q1, cell_ls, mp_count, cell_lo);
+    if (CLIMB)
+      climb<DS>(c, ncells, cell_data, cell_parent, inv_theta, rec, box, cell_open, cell_q0, cell_q1, cell_ls, mp_count,
+                cell_lo);
   }
 }
 
@@ -274,14 +316,34 @@ void launch_multipoles(const int* leaf_list, const TreeInfo* info, const uint4* 
                        const float4* jpos, float inv_theta, MpRec* rec, void* box, float4* cell_open,
                        float4* cell_q0, float4* cell_q1, float4* cell_ls, int* mp_count, int cell_cap,
                        const float4* jlo, float4* cell_lo, int nblocks, cudaStream_t s) {
+#if BONSAI_MP_CLIMB
   if (jlo)
-    k_multipoles<true><<<nblocks, 256, 0, s>>>(leaf_list, info, cell_data, cell_parent, jpos, inv_theta, rec,
-                                               static_cast<double*>(box), cell_open, cell_q0, cell_q1, cell_ls,
-                                               mp_count, cell_cap, jlo, cell_lo);
+    k_multipoles<true, true><<<nblocks, 256, 0, s>>>(leaf_list, info, cell_data, cell_parent, jpos, inv_theta, rec,
+                                                     static_cast<double*>(box), cell_open, cell_q0, cell_q1, cell_ls,
+                                                     mp_count, cell_cap, jlo, cell_lo);
   else
-    k_multipoles<false><<<nblocks, 256, 0, s>>>(leaf_list, info, cell_data, cell_parent, jpos, inv_theta, rec,
-                                                static_cast<float*>(box), cell_open, cell_q0, cell_q1, cell_ls,
-                                                mp_count, cell_cap, nullptr, nullptr);
+    k_multipoles<false, true><<<nblocks, 256, 0, s>>>(leaf_list, info, cell_data, cell_parent, jpos, inv_theta, rec,
+                                                      static_cast<float*>(box), cell_open, cell_q0, cell_q1, cell_ls,
+                                                      mp_count, cell_cap, nullptr, nullptr);
+#else
+  // leaves, then the nodes level by level from the deepest (levels 20 .. 1)
+  const int lb = std::max(1, nblocks / 4);
+  if (jlo) {
+    k_multipoles<true, false><<<nblocks, 256, 0, s>>>(leaf_list, info, cell_data, cell_parent, jpos, inv_theta, rec,
+                                                      static_cast<double*>(box), cell_open, cell_q0, cell_q1, cell_ls,
+                                                      mp_count, cell_cap, jlo, cell_lo);
+    for (int L = kMaxLevel - 1; L >= 1; L--)
+      k_mp_level<true><<<lb, 256, 0, s>>>(L, info, cell_data, inv_theta, rec, static_cast<double*>(box), cell_open,
+                                          cell_q0, cell_q1, cell_ls, cell_cap, cell_lo);
+  } else {
+    k_multipoles<false, false><<<nblocks, 256, 0, s>>>(leaf_list, info, cell_data, cell_parent, jpos, inv_theta,
+                                                       rec, static_cast<float*>(box), cell_open, cell_q0, cell_q1,
+                                                       cell_ls, mp_count, cell_cap, nullptr, nullptr);
+    for (int L = kMaxLevel - 1; L >= 1; L--)
+      k_mp_level<false><<<lb, 256, 0, s>>>(L, info, cell_data, inv_theta, rec, static_cast<float*>(box), cell_open,
+                                           cell_q0, cell_q1, cell_ls, cell_cap, nullptr);
+  }
+#endif
 }
 
 // Reference-layout view of the multipoles (debug/parity getter):
