@@ -21,7 +21,11 @@
 // per-level histogram; launch 2 scans the histograms (one block); launch 3
 // writes the cells level-major, key order inside a level (the canonical form
 // of the reference's cell order), with children contiguous, the leaf list,
-// parent links and the level ranges.
+// parent links (a cell's parent is the last cell of the level above that
+// starts at or before it, counted from the same prefix sums) and the level
+// ranges; then one short launch per level, from the top, gives every cell its
+// run end (its next sibling's start, or its parent's end for a last child)
+// and every node its child count -- no searches over the keys.
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -221,27 +225,6 @@ __global__ void __launch_bounds__(1024) k_tree_scan(unsigned* __restrict__ hist,
   }
 }
 
-__device__ __forceinline__ int lower_bound_u64(const unsigned long long* __restrict__ k, int lo, int hi,
-                                               unsigned long long t) {
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (__ldg(k + mid) < t) lo = mid + 1; else hi = mid;
-  }
-  return lo;
-}
-
-// first j >= lo with k[j] >= t, galloping from lo (k[lo-1] < t is known)
-__device__ __forceinline__ int gallop_u64(const unsigned long long* __restrict__ k, int lo, int n,
-                                          unsigned long long t) {
-  int step = 1, hi = lo;
-  while (hi < n && __ldg(k + hi) < t) {
-    lo = hi + 1;
-    hi += step;
-    step <<= 1;
-  }
-  return lower_bound_u64(k, lo, min(hi, n), t);
-}
-
 __global__ void __launch_bounds__(kTreeThreads) k_tree_cells(
     const unsigned long long* __restrict__ keys, const uint8_t* __restrict__ dlev,
     const uint16_t* __restrict__ chain, const unsigned* __restrict__ hist, int n, int nleaf, int nb, int cell_cap,
@@ -307,7 +290,6 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_cells(
     const int a = ca[k], b = cb[k];
     if (!a) continue;
     const int loc = kHalo + (i - t0);
-    const unsigned long long ki = keys[i];
     // leaf index
     {
       int lk = 0;
@@ -318,75 +300,72 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_cells(
       if (BONSAI_IN_RANGE(leaf_idx, nleaves, 0x101)) leaf_list[leaf_idx] = (int)(boff[0][b] + cpre[b][threadIdx.x]) + lc;
     }
     for (int L = a; L <= b; L++) {
-      int lc = 0;
-      for (int q = 0; q < k; q++) lc += (ca[q] && ca[q] <= L && L <= cb[q]);
+      int lc = 0, lcp = 0, lc1 = 0;
+      for (int q = 0; q < k; q++) {
+        const bool any = ca[q] != 0;
+        lc += (any && ca[q] <= L && L <= cb[q]);
+        lcp += (any && ca[q] <= L - 1 && L - 1 <= cb[q]);
+        lc1 += (any && ca[q] <= L + 1 && L + 1 <= cb[q]);
+      }
       const int cidx = (int)(boff[0][L] + cpre[L][threadIdx.x]) + lc;
       if (!BONSAI_IN_RANGE(cidx, ncells, 0x102)) continue;
       const bool leaf = (L == b);
-      const int sh = 63 - 3 * L;
-      const unsigned long long pre = ki >> sh;
-      int pend;
-      bool small_leaf = false;
-      if (leaf) {
-        // count <= nleaf unless this is a fat level-21 leaf
-        for (int j = 1; j <= nleaf; j++) {
-          if (i + j >= n) { pend = n; small_leaf = true; break; }
-          if ((int)sd[loc + j] <= L) { pend = i + j; small_leaf = true; break; }
-        }
-      }
-      if (!small_leaf) {
-        // keys increase only inside a system: search up to the system's end
-        const int send = nsys > 1 ? sys_off[sys_of(sys_off, nsys, i) + 1] : n;
-        pend = gallop_u64(keys, min(i + nleaf + 1, send), send, (pre + 1ull) << sh);
-      }
-      uint4* cd = cell_data + cidx;
+      uint4 cd;
+      int parent = -1;
       if (L == 1) {
-        cd->x = (unsigned)(1 << 27);  // level-1 cells: parent 0, as the reference stores them
-        cell_parent[cidx] = -1;
+        cd.x = (unsigned)(1 << 27);  // level-1 cells: parent 0, as the reference stores them
         // a system's first level-1 cell starts at the system's first particle
         if (nsys > 1 && sd[loc] == 0) root_beg[sys_of(sys_off, nsys, i)] = cidx;
+      } else {
+        // the parent is the last level-(L-1) cell starting at or before i:
+        // the one starting at i when the chain here covers level L-1, else
+        // the one before the first level-(L-1) cell that starts after i
+        parent = (int)(boff[0][L - 1] + cpre[L - 1][threadIdx.x]) + lcp - (a <= L - 1 ? 0 : 1);
+        cd.x = (unsigned)parent | ((unsigned)L << 27);
       }
-      unsigned ywd = 0xFFFFFFFFu;
-      if (!leaf) {
-        // children: runs of distinct level-(L+1) digit inside [i, pend)
-        int lc1 = 0;
-        for (int q = 0; q < k; q++) lc1 += (ca[q] && ca[q] <= L + 1 && L + 1 <= cb[q]);
-        const int first = (int)(boff[0][L + 1] + cpre[L + 1][threadIdx.x]) + lc1;
-        // the 7 inner octant boundaries are independent lower bounds over
-        // [i, pend): searched in lock-step, 7 loads in flight per step
-        int bl[8], bh[8];
-#pragma unroll
-        for (int o = 1; o < 8; o++) { bl[o] = i; bh[o] = pend; }
-        for (int span = pend - i; span > 0; span >>= 1) {
-#pragma unroll
-          for (int o = 1; o < 8; o++) {
-            if (bl[o] < bh[o]) {
-              const int mid = (bl[o] + bh[o]) >> 1;
-              if (__ldg(keys + mid) < (((pre << 3) | (unsigned long long)o) << (sh - 3))) bl[o] = mid + 1;
-              else bh[o] = mid;
-            }
-          }
-        }
-        int nch = 0, lo = i;
-        for (int o = 1; o <= 8; o++) {
-          const int bnd = (o == 8) ? pend : bl[o];
-          if (bnd > lo) {
-            if (BONSAI_IN_RANGE(first + nch, ncells, 0x103)) {
-              cell_data[first + nch].x = (unsigned)cidx | ((unsigned)(L + 1) << 27);
-              cell_parent[first + nch] = cidx;
-            }
-            nch++;
-          }
-          lo = bnd;
-        }
-        ywd = (unsigned)first | ((unsigned)(nch - 1) << 29);
-      }
-      if (!BONSAI_IN_RANGE(pend - 1, n, 0x104) || !BONSAI_IN_RANGE(i, pend, 0x105)) pend = min(max(pend, i + 1), n);
-      cd->y = ywd;
-      cd->z = (unsigned)i;
-      cd->w = (unsigned)pend;
+      // nodes: the first child (children are contiguous at level L + 1); the
+      // child count and every cell's run end follow in the level passes
+      cd.y = leaf ? 0xFFFFFFFFu : (unsigned)((int)(boff[0][L + 1] + cpre[L + 1][threadIdx.x]) + lc1);
+      cd.z = (unsigned)i;
+      cd.w = (unsigned)i;
+      cell_data[cidx] = cd;
+      cell_parent[cidx] = parent;
       mp_count[cidx] = 0;
     }
+  }
+}
+
+// Run ends and child counts, level by level from the top.  A cell's run ends
+// where its next sibling starts (the next cell of the level with the same
+// parent) or, for a last child, where its parent's run ends; the last child
+// of a node writes the node's child count.  Level-1 cells partition their
+// system: a run ends at the next level-1 cell's start (the next system's
+// first particle for a system's last cell) or at n.
+__global__ void __launch_bounds__(kTreeThreads) k_tree_pass(int L, const TreeInfo* __restrict__ info,
+                                                            uint4* __restrict__ cell_data,
+                                                            const int* __restrict__ cell_parent, int n,
+                                                            int cell_cap) {
+  if (info->ncells > cell_cap || info->nleaves > cell_cap) return;
+  [[maybe_unused]] const int ncells = info->ncells;
+  const int b = info->level_beg[L], e = info->level_end[L];
+  for (int c = b + blockIdx.x * blockDim.x + threadIdx.x; c < e; c += gridDim.x * blockDim.x) {
+    const bool more = c + 1 < e;
+    int pend;
+    if (L == 1) {
+      pend = more ? (int)cell_data[c + 1].z : n;
+    } else {
+      const int par = cell_parent[c];
+      if (!BONSAI_IN_RANGE(par, ncells, 0x107)) continue;
+      const bool sib = more && cell_parent[c + 1] == par;
+      pend = sib ? (int)cell_data[c + 1].z : (int)cell_data[par].w;
+      if (!sib) {
+        const unsigned first = cell_data[par].y & 0x1FFFFFFFu;
+        cell_data[par].y = first | ((unsigned)(c - (int)first) << 29);
+      }
+    }
+    const int i = (int)cell_data[c].z;
+    if (!BONSAI_IN_RANGE(pend - 1, n, 0x104) || !BONSAI_IN_RANGE(i, pend, 0x105)) pend = min(max(pend, i + 1), n);
+    cell_data[c].w = (unsigned)pend;
   }
 }
 
@@ -400,6 +379,9 @@ void build_tree(const unsigned long long* sorted_keys, int n, int nleaf, int cel
   k_tree_scan<<<1, 1024, 0, s>>>(hist, nb, cell_cap, leaf_cap, n, info);
   k_tree_cells<<<nb, kTreeThreads, 0, s>>>(sorted_keys, dlev, chain, hist, n, nleaf, nb, cell_cap, info, cell_data,
                                            cell_parent, leaf_list, mp_count, sys_off, nsys, root_beg);
+  const int pb = nb < 512 ? nb : 512;
+  for (int L = 1; L <= kMaxLevel; L++)
+    k_tree_pass<<<pb, kTreeThreads, 0, s>>>(L, info, cell_data, cell_parent, n, cell_cap);
 }
 
 BONSAI_BOUNDS_ACCESSOR(bounds_word_tree)
