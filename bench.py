@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--particles", type=int, default=1 << 24, dest="n")
     ap.add_argument("--theta", type=float, default=0.6)
+    ap.add_argument("--relative-alpha", type=float, default=0.0,
+                    help="run the headline steps in the relative opening mode with this alpha (0: fixed theta)")
     ap.add_argument("--sweep", default="0.3,0.4,0.5,0.6,0.7,0.8,0.9,1.0",
                     help="thetas of the sweep reported beside the headline")
     ap.add_argument("--learned-target", type=float, default=1e-3,
@@ -138,8 +140,12 @@ def hbm_roofline(n, info, stage_ms):
 
 
 def workload(a):
-    return ("plummer N=%d theta=%g eps=%g nleaf=%d ncrit=%d levelSplit=%d dt=1/%d seed=%d, fixed-theta FP32"
-            % (a.n, a.theta, a.eps, a.nleaf, a.ncrit, a.level_split, round(1 / a.dt), a.seed))
+    alpha = getattr(a, "relative_alpha", 0.0)
+    how = ("fixed-theta FP32" if not alpha else
+           "relative opening test alpha=%g (safety angle 2.0, theta the first evaluation's fallback), FP32"
+           % alpha)
+    return ("plummer N=%d theta=%g eps=%g nleaf=%d ncrit=%d levelSplit=%d dt=1/%d seed=%d, %s"
+            % (a.n, a.theta, a.eps, a.nleaf, a.ncrit, a.level_split, round(1 / a.dt), a.seed, how))
 
 
 # ---------------------------------------------------------------------------
@@ -434,6 +440,10 @@ def run_ours(a):
     t = B.Treecode(eps=a.eps, theta=a.theta, ncrit=a.ncrit, nleaf=a.nleaf, level_split=a.level_split, dt=a.dt,
                    device=d.local)
     t.alloc(n)
+    if a.relative_alpha:
+        from bonsai2_b200 import learned as Lr
+        Lr.set_relative_bound(t, Lr.THETA_BOUND)
+        Lr.set_theta_mode(t, 3, a.relative_alpha, a.relative_alpha)
     if L.bonsai_set_particles(t.handle, _p(pos), _p(vel), n):
         raise RuntimeError("set_particles")
     nkern = L.bonsai_graph_kernel_count(t.handle)
