@@ -116,16 +116,32 @@ __device__ void combine_children(int p, int first, int nch, float inv_theta, MpR
   typedef typename BoxOf<DS>::T B;
   double M = 0, X = 0, Y = 0, Z = 0;
   B bmn[3] = {(B)3.0e38, (B)3.0e38, (B)3.0e38}, bmx[3] = {(B)-3.0e38, (B)-3.0e38, (B)-3.0e38};
-  for (int k = 0; k < nch; k++) {
-    const MpRec* ck = rec + first + k;
-    const double mk = __ldcg(&ck->m);
-    M += mk;
-    X += mk * __ldcg(&ck->cx); Y += mk * __ldcg(&ck->cy); Z += mk * __ldcg(&ck->cz);
-    const B* bk = box + 6 * (size_t)(first + k);
-    for (int a = 0; a < 3; a++) {
-      bmn[a] = DS ? (B)fmin((double)bmn[a], (double)__ldcg(bk + a)) : (B)fminf((float)bmn[a], (float)__ldcg(bk + a));
-      bmx[a] = DS ? (B)fmax((double)bmx[a], (double)__ldcg(bk + 3 + a))
-                  : (B)fmaxf((float)bmx[a], (float)__ldcg(bk + 3 + a));
+  // the children's records are loaded a batch ahead of their sums, which
+  // stay in child order (the moments are the same to the bit)
+  constexpr int kB = 4;
+  for (int k0 = 0; k0 < nch; k0 += kB) {
+    double mb[kB], xb[kB], yb[kB], zb[kB];
+    B lo[kB][3], hi[kB][3];
+#pragma unroll
+    for (int u = 0; u < kB; u++) {
+      const int k = min(k0 + u, nch - 1);
+      const MpRec* ck = rec + first + k;
+      mb[u] = __ldcg(&ck->m); xb[u] = __ldcg(&ck->cx); yb[u] = __ldcg(&ck->cy); zb[u] = __ldcg(&ck->cz);
+      const B* bk = box + 6 * (size_t)(first + k);
+#pragma unroll
+      for (int a = 0; a < 3; a++) { lo[u][a] = __ldcg(bk + a); hi[u][a] = __ldcg(bk + 3 + a); }
+    }
+#pragma unroll
+    for (int u = 0; u < kB; u++) {
+      if (k0 + u >= nch) break;
+      const double mk = mb[u];
+      M += mk;
+      X += mk * xb[u]; Y += mk * yb[u]; Z += mk * zb[u];
+#pragma unroll
+      for (int a = 0; a < 3; a++) {
+        bmn[a] = DS ? (B)fmin((double)bmn[a], (double)lo[u][a]) : (B)fminf((float)bmn[a], (float)lo[u][a]);
+        bmx[a] = DS ? (B)fmax((double)bmx[a], (double)hi[u][a]) : (B)fmaxf((float)bmx[a], (float)hi[u][a]);
+      }
     }
   }
   MpRec P;
@@ -135,16 +151,28 @@ __device__ void combine_children(int p, int first, int nch, float inv_theta, MpR
     P.cz = 0.5 * ((double)bmn[2] + bmx[2]);
   }
   double I[6] = {0, 0, 0, 0, 0, 0};
-  for (int k = 0; k < nch; k++) {
-    const MpRec* ck = rec + first + k;
-    const double mk = __ldcg(&ck->m);
-    const double dx = __ldcg(&ck->cx) - P.cx, dy = __ldcg(&ck->cy) - P.cy, dz = __ldcg(&ck->cz) - P.cz;
-    I[0] += __ldcg(&ck->ixx) + mk * dx * dx;
-    I[1] += __ldcg(&ck->iyy) + mk * dy * dy;
-    I[2] += __ldcg(&ck->izz) + mk * dz * dz;
-    I[3] += __ldcg(&ck->ixy) + mk * dx * dy;
-    I[4] += __ldcg(&ck->ixz) + mk * dx * dz;
-    I[5] += __ldcg(&ck->iyz) + mk * dy * dz;
+  constexpr int kB2 = 2;
+  for (int k0 = 0; k0 < nch; k0 += kB2) {
+    MpRec cb[kB2];
+#pragma unroll
+    for (int u = 0; u < kB2; u++) {
+      const MpRec* ck = rec + first + min(k0 + u, nch - 1);
+      cb[u].m = __ldcg(&ck->m); cb[u].cx = __ldcg(&ck->cx); cb[u].cy = __ldcg(&ck->cy); cb[u].cz = __ldcg(&ck->cz);
+      cb[u].ixx = __ldcg(&ck->ixx); cb[u].iyy = __ldcg(&ck->iyy); cb[u].izz = __ldcg(&ck->izz);
+      cb[u].ixy = __ldcg(&ck->ixy); cb[u].ixz = __ldcg(&ck->ixz); cb[u].iyz = __ldcg(&ck->iyz);
+    }
+#pragma unroll
+    for (int u = 0; u < kB2; u++) {
+      if (k0 + u >= nch) break;
+      const double mk = cb[u].m;
+      const double dx = cb[u].cx - P.cx, dy = cb[u].cy - P.cy, dz = cb[u].cz - P.cz;
+      I[0] += cb[u].ixx + mk * dx * dx;
+      I[1] += cb[u].iyy + mk * dy * dy;
+      I[2] += cb[u].izz + mk * dz * dz;
+      I[3] += cb[u].ixy + mk * dx * dy;
+      I[4] += cb[u].ixz + mk * dx * dz;
+      I[5] += cb[u].iyz + mk * dy * dz;
+    }
   }
   P.m = M;
   P.ixx = I[0]; P.iyy = I[1]; P.izz = I[2]; P.ixy = I[3]; P.ixz = I[4]; P.iyz = I[5];
@@ -327,7 +355,7 @@ void launch_multipoles(const int* leaf_list, const TreeInfo* info, const uint4* 
                                                       mp_count, cell_cap, nullptr, nullptr);
 #else
   // leaves, then the nodes level by level from the deepest (levels 20 .. 1)
-  const int lb = std::max(1, nblocks / 4);
+  const int lb = nblocks;
   if (jlo) {
     k_multipoles<true, false><<<nblocks, 256, 0, s>>>(leaf_list, info, cell_data, cell_parent, jpos, inv_theta, rec,
                                                       static_cast<double*>(box), cell_open, cell_q0, cell_q1, cell_ls,
