@@ -444,7 +444,7 @@ struct Handle {
     BONSAI_CUDA_TRY(cudaMemcpy(chunks, ch.data(), ch.size() * sizeof(int4), cudaMemcpyHostToDevice));
     BONSAI_CUDA_TRY(cudaMemset(sys_energy, 0, (size_t)ns * 8 * sizeof(double)));
     BONSAI_CUDA_TRY(cudaMemset(root_beg, 0, (size_t)(ns + 1) * sizeof(int)));
-    theta_mode = 0;  // angles and precision are set again for the ensemble; block steps: single systems
+    theta_mode = 0;  // angles, precision and block steps are set again for the ensemble
     precision = 0;
     release_lo();
     bts_K = -1;
@@ -1253,7 +1253,6 @@ int bonsai_set_block_steps(bonsai_handle hh, int max_level, float eta) {
   Handle* h = H(hh);
   if (!h) return BONSAI_ERR_HANDLE;
   if (max_level > 16 || (max_level >= 0 && !(eta > 0.f))) return BONSAI_ERR_ARG;
-  if (max_level >= 0 && h->nsys > 1) return BONSAI_ERR_ARG;
   BONSAI_CUDA_TRY(cudaSetDevice(h->dev));
   BONSAI_CUDA_TRY(cudaStreamSynchronize(h->st));
   h->bts_K = max_level < 0 ? -1 : max_level;

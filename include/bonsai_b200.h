@@ -326,8 +326,8 @@ int bonsai_get_particles_f64(bonsai_handle h, double *pos4, float *vel4, float *
  * inside an ensemble: the network's features are normalised per system, so a
  * system's angles, and with them its forces, are those it gets alone.
  * Double-single positions (bonsai_set_precision, set after this call) work
- * inside an ensemble too.  Block time steps are for single systems only
- * (BONSAI_ERR_ARG).  nsys <= 65536. */
+ * inside an ensemble too, and so do block time steps (bonsai_set_block_steps,
+ * set after this call).  nsys <= 65536. */
 int bonsai_set_systems(bonsai_handle h, const int *counts, int nsys);
 /* energies of every system, 8 doubles per system in the layout and with the
  * timing rules of bonsai_compute_energies (a single system: its 8 values) */
@@ -382,7 +382,10 @@ int bonsai_sync_velocities(bonsai_handle h);
  * per particle; its level is the smallest k with dt/2^k <= eta sqrt(eps/|a|),
  * taken at the end of each of its steps, never before its boundary (a step
  * starts where a step of its length may) and at most doubling the step at a
- * time.  max_level < 0 turns them off.  Single systems only. */
+ * time.  max_level < 0 turns them off.  In an ensemble (set after
+ * bonsai_set_systems) every particle keeps its own level and each system
+ * advances as it does alone; a substep rebuilds the tree when a particle of
+ * any system ends a step there. */
 int bonsai_set_block_steps(bonsai_handle h, int max_level, float eta);
 /* nsteps big steps of dt, each 2^K substeps: per substep the opening kicks of
  * the particles whose step starts, the drift of all particles, a tree of all

@@ -85,13 +85,54 @@ def test_levels_follow_the_criterion_and_energy_is_kept():
     t.close()
 
 
-def test_block_steps_rejected_for_ensembles_and_before_enabling():
+def test_block_steps_accepted_for_ensembles_rejected_before_enabling():
     import bonsai2_b200 as B
     t = B.Treecode(**PRM)
     t.set_systems(np.array([100, 200], np.int32))
-    assert t._L.bonsai_set_block_steps(t.handle, 2, 0.2) == -4
+    assert t._L.bonsai_set_block_steps(t.handle, 2, 0.2) == 0
+    assert t._L.bonsai_set_block_steps(t.handle, 2, 0.0) == -4  # eta must be > 0
     u = B.Treecode(**PRM)
     u.alloc(100)
     assert u._L.bonsai_block_step(u.handle, 1) == -3
     t.close()
     u.close()
+
+
+def test_block_steps_in_an_ensemble_are_each_system_alone():
+    """Block time steps inside an ensemble: every system's positions,
+    velocities and levels after two big steps equal, bit for bit, those of the
+    system stepped alone (a substep rebuilds the tree when any system has a
+    particle ending a step there; the others only drift, as they do alone)."""
+    import bonsai2_b200 as B
+    from bonsai2_b200.ensemble import plummer_ensemble
+    counts = np.array([3000, 7000, 2, 4500], np.int32)
+    pos, vel = plummer_ensemble(counts, base_seed=41)
+    prm = dict(PRM, dt=1.0 / 16)
+    t = B.Treecode(**prm)
+    t.set_systems(counts)
+    t.h_ptclPos[:] = pos
+    t.h_ptclVel[:] = vel
+    t.ptcl_h2d()
+    t.set_block_steps(2, 0.4)
+    t.block_step(2)
+    assert t.synchronize() == 0
+    t.ptcl_d2h()
+    lev = t.levels()
+    es = t.system_energies()
+    P, V = t.h_ptclPos.copy(), t.h_ptclVel.copy()
+    t.close()
+    assert len(np.unique(lev)) >= 2  # particles on different levels
+    off = np.concatenate([[0], np.cumsum(counts)])
+    for s in range(len(counts)):
+        b, e = int(off[s]), int(off[s + 1])
+        u = B.Treecode(**prm)
+        _load(u, np.ascontiguousarray(pos[b:e]), np.ascontiguousarray(vel[b:e]))
+        u.set_block_steps(2, 0.4)
+        u.block_step(2)
+        assert u.synchronize() == 0
+        u.ptcl_d2h()
+        assert np.array_equal(u.h_ptclPos.view(np.uint32), P[b:e].view(np.uint32)), f"positions of system {s}"
+        assert np.array_equal(u.h_ptclVel.view(np.uint32), V[b:e].view(np.uint32)), f"velocities of system {s}"
+        assert np.array_equal(u.levels(), lev[b:e]), f"levels of system {s}"
+        np.testing.assert_allclose(u.computeEnergies(), es[s], rtol=1e-12, atol=1e-15)
+        u.close()
