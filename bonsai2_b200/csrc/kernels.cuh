@@ -76,14 +76,15 @@ struct RelativeArgs {
   const float* tau = nullptr;  // per-group bounds; null: the geometric test only
   float4* stats = nullptr;     // per-group statistics written by the walk (null: none)
   int* part_gid = nullptr;     // group of each particle, written with the statistics
-  int* acc_valid = nullptr;    // set to 1 by the walk once acc holds this evaluation's accelerations
+  int* acc_valid = nullptr;    // [0] set to 1 by the walk once acc holds this evaluation's
+                               // accelerations, [1] to whether it wrote the statistics too
 };
 
 // What the learned features read of the previous evaluation.
 struct PrevEval {
   const float4* acc = nullptr;    // its accelerations, in its particle order
   const int* perm = nullptr;      // current position -> index in that order (null: the same order)
-  const int* acc_valid = nullptr; // device flag: acc is valid
+  const int* acc_valid = nullptr; // device flags: [0] acc is valid, [1] stats and part_gid came with it
   const int* part_gid = nullptr;  // group of each particle in that evaluation (its order)
   const float4* stats = nullptr;  // its per-group statistics
   int stats_cap = 0;              // capacity of stats

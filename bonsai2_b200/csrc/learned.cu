@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(256) k_group_features(const int2* __restrict__
         spread = sqrtf(fmaxf(al2 / (float)np - mu * mu, 0.f));
         const int k = pb + np / 2;
         const int j = prev.perm ? __ldg(prev.perm + k) : k;
-        if (BONSAI_IN_RANGE(j, n, 0x502)) {
+        if (prev.acc_valid[1] && BONSAI_IN_RANGE(j, n, 0x502)) {
           const int og = __ldg(prev.part_gid + j);
           if (og >= 0 && og < prev.stats_cap) st = __ldg(prev.stats + og);
         }

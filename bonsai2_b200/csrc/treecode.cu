@@ -87,7 +87,7 @@ struct Handle {
   float* group_amag = nullptr;
   float4* group_stats = nullptr;
   int* part_gid = nullptr;
-  int* acc_valid = nullptr;
+  int* acc_valid = nullptr;  // device: [0] acc is this state's, [1] the walk statistics came with it
   bool tau_on = false;
   float theta_bound = 2.0f;  // geometric safety bound of the relative modes
   float rel_alpha = 1e-2f;   // theta mode 3: tau = rel_alpha * A_g
@@ -336,8 +336,8 @@ struct Handle {
     BONSAI_CUDA_TRY(cudaMemset(box_ticket, 0, sizeof(unsigned)));
     BONSAI_CUDA_TRY(dalloc(&closing, 1));
     BONSAI_CUDA_TRY(cudaMemset(closing, 0, sizeof(int)));
-    BONSAI_CUDA_TRY(dalloc(&acc_valid, 1));
-    BONSAI_CUDA_TRY(cudaMemset(acc_valid, 0, sizeof(int)));
+    BONSAI_CUDA_TRY(dalloc(&acc_valid, 2));
+    BONSAI_CUDA_TRY(cudaMemset(acc_valid, 0, 2 * sizeof(int)));
     BONSAI_CUDA_TRY(dalloc(&box, 1));
     BONSAI_CUDA_TRY(dalloc(&box_partial, (size_t)box_blocks * 6));
     std::vector<uint16_t> tab(384);
@@ -389,7 +389,7 @@ struct Handle {
     BONSAI_CUDA_TRY(cudaMemset(group_stats, 0, (size_t)gcap * sizeof(float4)));
     BONSAI_CUDA_TRY(dalloc(&part_gid, N));
     BONSAI_CUDA_TRY(cudaMemset(part_gid, 0, N * sizeof(int)));
-    BONSAI_CUDA_TRY(cudaMemset(acc_valid, 0, sizeof(int)));
+    BONSAI_CUDA_TRY(cudaMemset(acc_valid, 0, 2 * sizeof(int)));
     BONSAI_CUDA_TRY(dalloc(&group_feat, (size_t)gcap * kMlpFeatures));
     BONSAI_CUDA_TRY(dalloc(&group_counts, (size_t)gcap));
     // the reference reserves nPtcl cells (Treecode.h:192); a Plummer tree at
@@ -557,7 +557,9 @@ struct Handle {
       ginv = group_inv;
       rel.tau = tau_on ? group_tau : nullptr;
     }
-    if (ginv) {
+    if (ginv && theta_mode != 3) {
+      // the per-group statistics feed the learned form's next features (mode
+      // 3 has one parameter and no features; mode 2 records them for training)
       rel.stats = group_stats;
       rel.part_gid = part_gid;
     }
@@ -655,7 +657,7 @@ struct Handle {
       BONSAI_CUDA_TRY(cudaMemcpyAsync(id[par], si, N * sizeof(int), cudaMemcpyDeviceToDevice, st));
       if (precision) BONSAI_CUDA_TRY(cudaMemcpyAsync(plo[par], sl, N * sizeof(float4), cudaMemcpyDeviceToDevice, st));
       BONSAI_CUDA_TRY(cudaMemcpyAsync(closing, &closing0, sizeof(int), cudaMemcpyHostToDevice, st));
-      BONSAI_CUDA_TRY(cudaMemsetAsync(acc_valid, 0, sizeof(int), st));
+      BONSAI_CUDA_TRY(cudaMemsetAsync(acc_valid, 0, 2 * sizeof(int), st));
       return 0;
     };
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -882,7 +884,7 @@ static int set_particles_impl(Handle* h, const float* pos4, const float* vel4, i
   k_iota<<<h->nsm * 4, 256, 0, h->st>>>(h->id[h->par], n);
   if (h->precision) BONSAI_CUDA_TRY(cudaMemsetAsync(h->plo[h->par], 0, bytes, h->st));  // float input: lo = 0
   BONSAI_CUDA_TRY(cudaMemsetAsync(h->closing, 0, sizeof(int), h->st));
-  BONSAI_CUDA_TRY(cudaMemsetAsync(h->acc_valid, 0, sizeof(int), h->st));  // no previous accelerations
+  BONSAI_CUDA_TRY(cudaMemsetAsync(h->acc_valid, 0, 2 * sizeof(int), h->st));  // no previous accelerations
   h->built = h->mp_done = h->grouped = h->forced = h->moved_after_forces = false;
   h->bts_ready = false;
   return last_cuda();
@@ -945,7 +947,7 @@ int bonsai_set_particles_async(bonsai_handle hh, const float* pos4, const float*
   k_iota<<<h->nsm * 4, 256, 0, h->st>>>(h->id[h->par], n);
   if (h->precision) BONSAI_CUDA_TRY(cudaMemsetAsync(h->plo[h->par], 0, bytes, h->st));
   BONSAI_CUDA_TRY(cudaMemsetAsync(h->closing, 0, sizeof(int), h->st));
-  BONSAI_CUDA_TRY(cudaMemsetAsync(h->acc_valid, 0, sizeof(int), h->st));
+  BONSAI_CUDA_TRY(cudaMemsetAsync(h->acc_valid, 0, 2 * sizeof(int), h->st));
   h->built = h->mp_done = h->grouped = h->forced = h->moved_after_forces = false;
   h->bts_ready = false;
   return last_cuda();

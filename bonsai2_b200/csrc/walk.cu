@@ -308,21 +308,22 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
           }
         }
         const bool leaf = cd.y == 0xFFFFFFFFu;
-        bool split = valid && (open_cell(co, gc, gs) || ((int)(cd.w - cd.z) < 3));
+        // the squared box-to-COM distance, shared by the geometric test (the
+        // same value open_cell forms), the relative test and the statistics
+        const float ds2 = box_dist2(co, gc, gs);
+        bool split = valid && (ds2 < fabsf(co.w) || ((int)(cd.w - cd.z) < 3));
         bool near = false;
         if (PERGROUP && rel.stats) {
           // ds within ~20 % of the geometric opening distance
-          const float r = __fdividef(box_dist2(co, gc, gs), fabsf(co.w));
-          near = valid && r > 0.7f && r < 1.45f;
+          const float w = fabsf(co.w);
+          near = valid && ds2 > 0.7f * w && ds2 < 1.45f * w;
         }
         if (PERGROUP && tau_g > 0.0f && valid && !split) {
-          split = open_relative(co, gc, gs, mk, tau_g);
-          if (rel.stats) {
-            // within a factor 2 of the relative bound (ds within ~15 %)
-            const float ds2 = box_dist2(co, gc, gs);
-            const float rho = __fdividef(mk, __fmul_rn(tau_g, __fmul_rn(__fmul_rn(ds2, ds2), __fsqrt_rn(ds2))));
-            near = near || (rho > 0.5f && rho < 2.0f);
-          }
+          // open_relative on the shared ds2
+          const float tds5 = __fmul_rn(tau_g, __fmul_rn(__fmul_rn(ds2, ds2), __fsqrt_rn(ds2)));
+          split = mk > tds5;
+          // within a factor 2 of the relative bound (ds within ~15 %)
+          if (rel.stats) near = near || (mk > 0.5f * tds5 && mk < 2.0f * tds5);
         }
         if (PERGROUP && rel.stats) st_near += __popc(__ballot_sync(kFull, near));
 
@@ -359,12 +360,11 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
           const float4 q1 = __ldg(cell_q1 + cell);
           const float4 q0 = __ldg(cell_q0 + cell);
           if (PERGROUP && rel.stats) {
-            const float ds2 = fmaxf(box_dist2(co, gc, gs), 1e-30f);
-            const float wf = __fdividef(q0.x, ds2);  // the cell's force share M / ds^2
+            const float inv = __frcp_rn(fmaxf(ds2, 1e-30f));
             st_macc += q0.x;
             st_mnear += near ? q0.x : 0.f;
-            st_qn += __fdividef(q1.w * (2.0f / 3.0f), __fmul_rn(ds2, ds2));  // tr I / ds^4 = wf (b / ds)^2
-            st_wm += wf;
+            st_qn += q1.w * (2.0f / 3.0f) * inv * inv;  // tr I / ds^4 = (M / ds^2) (b / ds)^2
+            st_wm += q0.x * inv;                         // the cell's force share M / ds^2
           }
           s_a0[w][slot] = make_float4(co.x, co.y, co.z, q1.w * (-1.0f / 3.0f));
           s_a1[w][slot] = make_float4(q0.x, -q0.y, -q0.z, -q0.w);
@@ -497,7 +497,10 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
     max_dir = max(max_dir, n_dir);
   }
   // the accelerations just written are the previous ones of the next evaluation
-  if (rel.acc_valid && blockIdx.x == 0 && threadIdx.x == 0) *rel.acc_valid = 1;
+  if (rel.acc_valid && blockIdx.x == 0 && threadIdx.x == 0) {
+    rel.acc_valid[0] = 1;
+    rel.acc_valid[1] = rel.stats != nullptr;
+  }
   if (lane == 0) {
     atomicAdd(stats + 0, sum_app);
     atomicAdd(stats + 1, sum_dir);

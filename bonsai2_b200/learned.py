@@ -281,17 +281,27 @@ def allocation_labels(E, C, sizes, thetas, target, fraction=0.9):
 # the learned form: relative accuracy mode
 # ---------------------------------------------------------------------------
 def _prepare_relative(t: Treecode, nleaf, ncrit, level_split, alpha0, theta_bound):
-    """A relative walk at alpha0 (after the fixed-angle first evaluation) so
-    that acc and the walk statistics are those of a relative walk, then the
-    tree rebuilt from the same positions (same groups, identity
-    permutation): the state the learned features see inside a run."""
+    """A relative walk at alpha0 (theta mode 2 with host bounds alpha0 A_g,
+    after the fixed-angle first evaluation that gives A_g) so that acc and the
+    walk statistics are those of a relative walk, then the tree rebuilt from
+    the same positions (same groups, identity permutation): the state the
+    learned features see inside a run."""
     set_relative_bound(t, theta_bound)
-    set_theta_mode(t, 3, alpha0, alpha0)
-    for _ in range(2):
-        t.buildTree(nleaf)
-        t.computeMultipoles()
-        t.makeGroups(level_split, ncrit)
-        t.computeForces(False)
+    set_theta_mode(t, 0)
+    t.buildTree(nleaf)
+    t.computeMultipoles()
+    t.makeGroups(level_split, ncrit)
+    t.computeForces(False)
+    t.buildTree(nleaf)
+    t.computeMultipoles()
+    t.makeGroups(level_split, ncrit)
+    group_features(t)  # computes A_g from the previous accelerations
+    A = group_scale(t).astype(np.float64)
+    set_theta_mode(t, 2)
+    set_group_theta(t, np.full(A.shape[0], theta_bound, np.float32))
+    set_group_tau(t, (alpha0 * A).astype(np.float32))
+    t.computeForces(False)
+    set_group_tau(t, None)
     t.buildTree(nleaf)
     t.computeMultipoles()
     t.makeGroups(level_split, ncrit)

@@ -107,14 +107,15 @@ def test_ensemble_direct_sum_is_per_system():
     t.close()
 
 
-def test_ensemble_rejects_bad_counts_and_block_steps():
+def test_ensemble_rejects_bad_counts():
     import bonsai2_b200 as B
     from bonsai2_b200._lib import BonsaiError
     t = B.Treecode(**PARAMS)
     with pytest.raises(BonsaiError):
         t.set_systems(np.array([10, 0, 5], np.int32))
     t.set_systems(np.array([10, 5], np.int32))
-    assert t._L.bonsai_set_block_steps(t.handle, 2, 0.05) == -4  # block time steps: single systems
+    assert t._L.bonsai_set_block_steps(t.handle, 2, 0.05) == 0  # block time steps inside an ensemble
+    assert t._L.bonsai_set_block_steps(t.handle, 17, 0.05) != 0  # more levels than the 16 supported
     t.close()
 
 
