@@ -49,7 +49,7 @@ void build_tree(const unsigned long long* sorted_keys, int n, int nleaf, int cel
 // double-single positions)
 void launch_multipoles(const int* leaf_list, const TreeInfo* info, const uint4* cell_data, const int* cell_parent,
                        const float4* jpos, float inv_theta, MpRec* rec, void* box, float4* cell_open,
-                       float4* cell_q0, float4* cell_q1, float4* cell_ls, int* mp_count, int cell_cap,
+                       float4* cell_stage, float4* cell_ls, int* mp_count, int cell_cap,
                        const float4* jlo, float4* cell_lo, int nblocks, cudaStream_t s);
 __global__ void k_multipoles_ref_layout(const TreeInfo* __restrict__ info, const float4* __restrict__ cell_open,
                                         const MpRec* __restrict__ rec, float4* __restrict__ size,
@@ -96,7 +96,7 @@ int walk_blocks_per_sm(int variant);
 // group_inv_theta == nullptr: the fixed opening angle baked into cell_open.w;
 // else 1/theta per group with (l, s) from cell_ls
 void launch_walk(int variant, int nblocks, const int2* groups, const TreeInfo* info, const float4* ipos, const float4* jpos,
-                 const uint4* cell_data, const float4* cell_open, const float4* cell_q0, const float4* cell_q1,
+                 const uint4* cell_data, const float4* cell_open, const float4* cell_stage,
                  const float4* cell_ls, const float* group_inv_theta, float eps2, float4* acc, int* ring_pool,
                  int ring_cap, unsigned* group_counter, unsigned long long* stats, int* status, const int* sys_off,
                  int nsys, const int* root_beg, const float4* ipos_lo, const float4* jpos_lo, const float4* cell_lo,

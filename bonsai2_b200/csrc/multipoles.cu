@@ -13,10 +13,13 @@
 //   M, COM; Q = second moment about the COM per unit mass (:148-158);
 //   particle bounding box -> l = max(2 max h, 1e-6), s = |cvec - COM|,
 //   cellOp = l/theta + s, stored squared (:168-177).
-// cell_ls = (l, s, M l^3, 0) lets a walk with per-group opening angles form
-// (l/theta_g + s)^2.  Stored for the walk (mass-weighted, pre-scaled so the
-// force kernel needs fewer operations):  cell_q0 = (M, 3Ixx, 3Iyy, 3Izz),
-// cell_q1 = (3Ixy, 3Ixz, 3Iyz, 1.5 tr I), with I = M Q.
+// cell_ls = (l, s, M l^3, 1.5 tr I) lets a walk with per-group opening angles
+// form (l/theta_g + s)^2.  Stored for the walk as three float4 per cell, in
+// the form the force kernel stages them (mass-weighted, pre-scaled and
+// negated so that it needs fewer operations; I = M Q):
+//   cell_stage[3c]     = (COM, -0.5 tr I)
+//   cell_stage[3c + 1] = (M, -3Ixx, -3Iyy, -3Izz)
+//   cell_stage[3c + 2] = (-3Ixy, -3Ixz, -3Iyz, -1.5 tr I)
 // The FP64 record (MpRec) holds M, COM and the moments; the particle bounding
 // box is a separate array, float for float positions and double (DS) for
 // double-single positions, where particles enter the FP64 sums as hi + lo,
@@ -56,7 +59,7 @@ template <bool DS>
 __device__ __forceinline__ void store_cell(int c, const MpRec& r, const typename BoxOf<DS>::T* bmin,
                                            const typename BoxOf<DS>::T* bmax, float inv_theta, MpRec* __restrict__ rec,
                                            typename BoxOf<DS>::T* __restrict__ box, float4* __restrict__ cell_open,
-                                           float4* __restrict__ cell_q0, float4* __restrict__ cell_q1,
+                                           float4* __restrict__ cell_stage,
                                            float4* __restrict__ cell_ls, float4* __restrict__ cell_lo) {
   rec[c] = r;
   for (int k = 0; k < 3; k++) { box[6 * (size_t)c + k] = bmin[k]; box[6 * (size_t)c + 3 + k] = bmax[k]; }
@@ -90,10 +93,15 @@ __device__ __forceinline__ void store_cell(int c, const MpRec& r, const typename
   // per-group opening angles recompute (l/theta_g + s)^2; the relative test
   // compares M l^3 (formed once here, in float) with tau ds^5
   const float mf = (float)r.m;
-  cell_ls[c] = make_float4(l, s, __fmul_rn(mf, __fmul_rn(l, __fmul_rn(l, l))), 0.0f);
   const double tr = r.ixx + r.iyy + r.izz;
-  cell_q0[c] = make_float4((float)r.m, (float)(3.0 * r.ixx), (float)(3.0 * r.iyy), (float)(3.0 * r.izz));
-  cell_q1[c] = make_float4((float)(3.0 * r.ixy), (float)(3.0 * r.ixz), (float)(3.0 * r.iyz), (float)(1.5 * tr));
+  const float t15 = (float)(1.5 * tr);
+  cell_ls[c] = make_float4(l, s, __fmul_rn(mf, __fmul_rn(l, __fmul_rn(l, l))), t15);
+  // the walk's staged record, copied to shared memory as it is (moments
+  // negated so that every difference in the interaction is one add)
+  float4* st = cell_stage + 3 * (size_t)c;
+  st[0] = make_float4(cx, cy, cz, __fmul_rn(t15, -1.0f / 3.0f));
+  st[1] = make_float4(mf, -(float)(3.0 * r.ixx), -(float)(3.0 * r.iyy), -(float)(3.0 * r.izz));
+  st[2] = make_float4(-(float)(3.0 * r.ixy), -(float)(3.0 * r.ixz), -(float)(3.0 * r.iyz), -t15);
 }
 
 // Arrival on a parent's counter: a fence publishes this child's record, a
@@ -111,7 +119,7 @@ __device__ __forceinline__ bool arrive_last(int* p, int nch) {
 template <bool DS>
 __device__ void combine_children(int p, int first, int nch, float inv_theta, MpRec* __restrict__ rec,
                                  typename BoxOf<DS>::T* __restrict__ box, float4* __restrict__ cell_open,
-                                 float4* __restrict__ cell_q0, float4* __restrict__ cell_q1,
+                                 float4* __restrict__ cell_stage,
                                  float4* __restrict__ cell_ls, float4* __restrict__ cell_lo) {
   typedef typename BoxOf<DS>::T B;
   double M = 0, X = 0, Y = 0, Z = 0;
@@ -176,7 +184,7 @@ __device__ void combine_children(int p, int first, int nch, float inv_theta, MpR
   }
   P.m = M;
   P.ixx = I[0]; P.iyy = I[1]; P.izz = I[2]; P.ixy = I[3]; P.ixz = I[4]; P.iyz = I[5];
-  store_cell<DS>(p, P, bmn, bmx, inv_theta, rec, box, cell_open, cell_q0, cell_q1, cell_ls, cell_lo);
+  store_cell<DS>(p, P, bmn, bmx, inv_theta, rec, box, cell_open, cell_stage, cell_ls, cell_lo);
 }
 
 // Combines parents bottom-up while this thread is the last child to arrive.
@@ -184,7 +192,7 @@ template <bool DS>
 __device__ void climb(int c, [[maybe_unused]] int ncells, const uint4* __restrict__ cell_data,
                       const int* __restrict__ cell_parent,
                       float inv_theta, MpRec* __restrict__ rec, typename BoxOf<DS>::T* __restrict__ box,
-                      float4* __restrict__ cell_open, float4* __restrict__ cell_q0, float4* __restrict__ cell_q1,
+                      float4* __restrict__ cell_open, float4* __restrict__ cell_stage,
                       float4* __restrict__ cell_ls, int* __restrict__ mp_count, float4* __restrict__ cell_lo) {
   while (true) {
     const int p = cell_parent[c];
@@ -194,7 +202,7 @@ __device__ void climb(int c, [[maybe_unused]] int ncells, const uint4* __restric
     const int first = (int)(y & 0x1FFFFFFFu), nch = (int)(y >> 29) + 1;
     if (!BONSAI_IN_RANGE(first + nch - 1, ncells, 0x304) || !BONSAI_IN_RANGE(c - first, nch, 0x305)) break;
     if (!arrive_last(mp_count + p, nch)) break;
-    combine_children<DS>(p, first, nch, inv_theta, rec, box, cell_open, cell_q0, cell_q1, cell_ls, cell_lo);
+    combine_children<DS>(p, first, nch, inv_theta, rec, box, cell_open, cell_stage, cell_ls, cell_lo);
     c = p;
   }
 }
@@ -205,8 +213,7 @@ template <bool DS>
 __global__ void __launch_bounds__(256) k_mp_level(int L, const TreeInfo* __restrict__ info,
                                                   const uint4* __restrict__ cell_data, float inv_theta,
                                                   MpRec* __restrict__ rec, typename BoxOf<DS>::T* __restrict__ box,
-                                                  float4* __restrict__ cell_open, float4* __restrict__ cell_q0,
-                                                  float4* __restrict__ cell_q1, float4* __restrict__ cell_ls,
+                                                  float4* __restrict__ cell_open, float4* __restrict__ cell_stage, float4* __restrict__ cell_ls,
                                                   int cell_cap, float4* __restrict__ cell_lo) {
   if (info->ncells > cell_cap) return;
   [[maybe_unused]] const int ncells = info->ncells;
@@ -216,7 +223,7 @@ __global__ void __launch_bounds__(256) k_mp_level(int L, const TreeInfo* __restr
     if (y == 0xFFFFFFFFu) continue;
     const int first = (int)(y & 0x1FFFFFFFu), nch = (int)(y >> 29) + 1;
     if (!BONSAI_IN_RANGE(first + nch - 1, ncells, 0x307)) continue;
-    combine_children<DS>(c, first, nch, inv_theta, rec, box, cell_open, cell_q0, cell_q1, cell_ls, cell_lo);
+    combine_children<DS>(c, first, nch, inv_theta, rec, box, cell_open, cell_stage, cell_ls, cell_lo);
   }
 }
 
@@ -229,8 +236,7 @@ __global__ void __launch_bounds__(256) k_multipoles(const int* __restrict__ leaf
                                                     const int* __restrict__ cell_parent,
                                                     const float4* __restrict__ jpos, float inv_theta,
                                                     MpRec* __restrict__ rec, typename BoxOf<DS>::T* __restrict__ box,
-                                                    float4* __restrict__ cell_open, float4* __restrict__ cell_q0,
-                                                    float4* __restrict__ cell_q1, float4* __restrict__ cell_ls,
+                                                    float4* __restrict__ cell_open, float4* __restrict__ cell_stage, float4* __restrict__ cell_ls,
                                                     int* __restrict__ mp_count, int cell_cap,
                                                     const float4* __restrict__ jlo, float4* __restrict__ cell_lo) {
   typedef typename BoxOf<DS>::T B;
@@ -333,43 +339,43 @@ __global__ void __launch_bounds__(256) k_multipoles(const int* __restrict__ leaf
 #endif
     r.m = m;
     r.ixx = q[0]; r.iyy = q[1]; r.izz = q[2]; r.ixy = q[3]; r.ixz = q[4]; r.iyz = q[5];
-    store_cell<DS>(c, r, mn, mx, inv_theta, rec, box, cell_open, cell_q0, cell_q1, cell_ls, cell_lo);
+    store_cell<DS>(c, r, mn, mx, inv_theta, rec, box, cell_open, cell_stage, cell_ls, cell_lo);
     if (CLIMB)
-      climb<DS>(c, ncells, cell_data, cell_parent, inv_theta, rec, box, cell_open, cell_q0, cell_q1, cell_ls, mp_count,
+      climb<DS>(c, ncells, cell_data, cell_parent, inv_theta, rec, box, cell_open, cell_stage, cell_ls, mp_count,
                 cell_lo);
   }
 }
 
 void launch_multipoles(const int* leaf_list, const TreeInfo* info, const uint4* cell_data, const int* cell_parent,
                        const float4* jpos, float inv_theta, MpRec* rec, void* box, float4* cell_open,
-                       float4* cell_q0, float4* cell_q1, float4* cell_ls, int* mp_count, int cell_cap,
+                       float4* cell_stage, float4* cell_ls, int* mp_count, int cell_cap,
                        const float4* jlo, float4* cell_lo, int nblocks, cudaStream_t s) {
 #if BONSAI_MP_CLIMB
   if (jlo)
     k_multipoles<true, true><<<nblocks, 256, 0, s>>>(leaf_list, info, cell_data, cell_parent, jpos, inv_theta, rec,
-                                                     static_cast<double*>(box), cell_open, cell_q0, cell_q1, cell_ls,
+                                                     static_cast<double*>(box), cell_open, cell_stage, cell_ls,
                                                      mp_count, cell_cap, jlo, cell_lo);
   else
     k_multipoles<false, true><<<nblocks, 256, 0, s>>>(leaf_list, info, cell_data, cell_parent, jpos, inv_theta, rec,
-                                                      static_cast<float*>(box), cell_open, cell_q0, cell_q1, cell_ls,
+                                                      static_cast<float*>(box), cell_open, cell_stage, cell_ls,
                                                       mp_count, cell_cap, nullptr, nullptr);
 #else
   // leaves, then the nodes level by level from the deepest (levels 20 .. 1)
   const int lb = nblocks;
   if (jlo) {
     k_multipoles<true, false><<<nblocks, 256, 0, s>>>(leaf_list, info, cell_data, cell_parent, jpos, inv_theta, rec,
-                                                      static_cast<double*>(box), cell_open, cell_q0, cell_q1, cell_ls,
+                                                      static_cast<double*>(box), cell_open, cell_stage, cell_ls,
                                                       mp_count, cell_cap, jlo, cell_lo);
     for (int L = kMaxLevel - 1; L >= 1; L--)
       k_mp_level<true><<<lb, 256, 0, s>>>(L, info, cell_data, inv_theta, rec, static_cast<double*>(box), cell_open,
-                                          cell_q0, cell_q1, cell_ls, cell_cap, cell_lo);
+                                          cell_stage, cell_ls, cell_cap, cell_lo);
   } else {
     k_multipoles<false, false><<<nblocks, 256, 0, s>>>(leaf_list, info, cell_data, cell_parent, jpos, inv_theta,
-                                                       rec, static_cast<float*>(box), cell_open, cell_q0, cell_q1,
+                                                       rec, static_cast<float*>(box), cell_open, cell_stage,
                                                        cell_ls, mp_count, cell_cap, nullptr, nullptr);
     for (int L = kMaxLevel - 1; L >= 1; L--)
       k_mp_level<false><<<lb, 256, 0, s>>>(L, info, cell_data, inv_theta, rec, static_cast<float*>(box), cell_open,
-                                           cell_q0, cell_q1, cell_ls, cell_cap, nullptr);
+                                           cell_stage, cell_ls, cell_cap, nullptr);
   }
 #endif
 }

@@ -69,7 +69,7 @@ struct Handle {
   unsigned* hist = nullptr;
   TreeInfo* info = nullptr;
   uint4* cell_data = nullptr;
-  float4 *cell_open = nullptr, *cell_q0 = nullptr, *cell_q1 = nullptr;
+  float4 *cell_open = nullptr, *cell_stage = nullptr;  // cell_stage: 3 per cell
   int *cell_parent = nullptr, *leaf_list = nullptr, *mp_count = nullptr;
   MpRec* rec = nullptr;
   double* cell_box = nullptr;  // 6 per cell: floats (float positions) or doubles (double-single)
@@ -250,7 +250,7 @@ struct Handle {
     n = 0;
   }
   void release_cells() {
-    dfree(&cell_data); dfree(&cell_open); dfree(&cell_q0); dfree(&cell_q1);
+    dfree(&cell_data); dfree(&cell_open); dfree(&cell_stage);
     dfree(&cell_parent); dfree(&leaf_list); dfree(&mp_count); dfree(&rec); dfree(&cell_ls);
     dfree(&cell_box);
     cap_cells = 0;
@@ -283,8 +283,7 @@ struct Handle {
     const size_t C = (size_t)cap;
     BONSAI_CUDA_TRY(dalloc(&cell_data, C));
     BONSAI_CUDA_TRY(dalloc(&cell_open, C));
-    BONSAI_CUDA_TRY(dalloc(&cell_q0, C));
-    BONSAI_CUDA_TRY(dalloc(&cell_q1, C));
+    BONSAI_CUDA_TRY(dalloc(&cell_stage, 3 * C));
     BONSAI_CUDA_TRY(dalloc(&cell_parent, C));
     BONSAI_CUDA_TRY(dalloc(&leaf_list, C));
     BONSAI_CUDA_TRY(dalloc(&mp_count, C));
@@ -491,7 +490,7 @@ struct Handle {
   }
   void enq_multipoles() {
     launch_multipoles(leaf_list, info, cell_data, cell_parent, jpos, 1.0f / prm.theta, rec, cell_box, cell_open,
-                      cell_q0, cell_q1, cell_ls, mp_count, cap_cells, precision ? jlo : nullptr,
+                      cell_stage, cell_ls, mp_count, cap_cells, precision ? jlo : nullptr,
                       precision ? cell_lo : nullptr, nsm * 8, st);
   }
   void enq_groups(int ls, int ncrit) { enq_groups_on(ls, ncrit, st, kalt, valt, sort_counts); }
@@ -563,7 +562,7 @@ struct Handle {
       rel.stats = group_stats;
       rel.part_gid = part_gid;
     }
-    launch_walk(k, walk_blocks[k], groups, info, pos[par], jpos, cell_data, cell_open, cell_q0, cell_q1, cell_ls,
+    launch_walk(k, walk_blocks[k], groups, info, pos[par], jpos, cell_data, cell_open, cell_stage, cell_ls,
                 ginv, prm.eps * prm.eps, acc, ring, kRingCap, group_counter, stats, &info->status, so(), nsys, root_beg,
                 precision ? plo[par] : nullptr, jlo, cell_lo, ginv ? group_counts : nullptr,
                 walk_list_on ? walk_list : nullptr, walk_list_on ? walk_list_n : nullptr, rel, st);

@@ -23,9 +23,12 @@
 //   * the level lists live in a per-warp pair of buffers in global memory
 //     (current level / next level, swapped per level; L1/L2 resident),
 //     bounded; overflow sets a status bit, never traps;
-//   * accepted cells and direct particles are staged by value in per-warp
-//     64-entry shared-memory rings as they are found, so the 32-wide
-//     evaluation loops read broadcast LDS.128 only;
+//   * accepted cells (their records pre-staged by the multipole kernel in
+//     cell_stage) and direct particles are copied by value with cp.async into
+//     per-warp shared-memory rings (64 quadrupoles, 128 particles) as they
+//     are found, and evaluated 32 at a time when the next 32-cell block
+//     starts, so the copies land behind the warp's own traversal and the
+//     32-wide evaluation loops read broadcast LDS.128 only;
 //   * the quadrupole kernel uses mass-weighted, pre-scaled moments
 //     (34 FP32 operations + 1 MUFU per interaction; the reference's
 //     formulation, counted as 64 flops by treecode.cu:149-158, is the same
@@ -66,6 +69,35 @@ constexpr int kWalkWarps = kWalkThreads / 32;
 struct IPart {
   float x, y, z;
 };
+
+// Staging knobs (walk at N = 2^24, theta 0.6, one B200):
+//   BONSAI_WALK_ASYNC 1: accepted cells' staged records (cell_stage, 48 B)
+//     and leaf particles are copied global -> shared by cp.async (LDGSTS,
+//     cached in L1), waited for only when their batch is evaluated; 0: loaded
+//     into registers and stored (the warp waits one L2 round trip per block);
+//   BONSAI_WALK_EVAL_EARLY 1: a 32-cell block first evaluates the full
+//     batches that earlier blocks staged, then reads its level-list entries
+//     (63.4 ms; register staging with evaluation right after staging: 63.8);
+//     0: it evaluates them while its own cell records are in flight (65.0 ms:
+//     the records held across the evaluation loop cost it registers).
+#ifndef BONSAI_WALK_ASYNC
+#define BONSAI_WALK_ASYNC 1
+#endif
+#ifndef BONSAI_WALK_EVAL_EARLY
+#define BONSAI_WALK_EVAL_EARLY 1
+#endif
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+#if BONSAI_WALK_ASYNC
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem) : "memory");
+#else
+  *static_cast<float4*>(smem) = __ldg(static_cast<const float4*>(gmem));
+#endif
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// direct-source ring per warp (a power of two, >= 64)
+constexpr int kDirRing = 128;
 
 // Interaction arithmetic over V = float (one i-particle) or V = float2 (two
 // i-particles of the lane, evaluated by the packed FFMA2/FMUL2/FADD2 of
@@ -176,8 +208,8 @@ template <int NI, bool SPLIT, bool PERGROUP, bool ENS, bool DS>
 __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
     k_walk(const int2* __restrict__ groups, const TreeInfo* __restrict__ info, const float4* __restrict__ ipos,
            const float4* __restrict__ jpos, const uint4* __restrict__ cell_data,
-           const float4* __restrict__ cell_open, const float4* __restrict__ cell_q0,
-           const float4* __restrict__ cell_q1, const float4* __restrict__ cell_ls,
+           const float4* __restrict__ cell_open, const float4* __restrict__ cell_stage,
+           const float4* __restrict__ cell_ls,
            const float* __restrict__ group_inv_theta, float eps2, float4* __restrict__ acc,
            int* __restrict__ ring_pool, int ring_cap, unsigned* __restrict__ group_counter,
            unsigned long long* __restrict__ stats, int* __restrict__ status, const int* __restrict__ sys_off,
@@ -190,7 +222,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
   __shared__ float4 s_a0[kWalkWarps][64];
   __shared__ float4 s_a1[kWalkWarps][64];
   __shared__ float4 s_a2[kWalkWarps][64];
-  __shared__ float4 s_d[kWalkWarps][64];
+  __shared__ float4 s_d[kWalkWarps][kDirRing];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int sub = SPLIT ? (lane & 15) : lane;
   const int half = SPLIT ? (lane >> 4) : 0;
@@ -282,15 +314,53 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
     unsigned n_app = 0, n_dir = 0;
     __syncwarp();
 
+    // evaluation of the staged 32-entry batches (ring order): the accepted
+    // cells' quadrupoles and the opened leaves' particles
+    auto eval_app = [&]() {
+      const float4* A0 = &s_a0[w][a_head + half];
+      const float4* A1 = &s_a1[w][a_head + half];
+      const float4* A2 = &s_a2[w][a_head + half];
+      BONSAI_UNROLL_N(BONSAI_WALK_UNROLL)
+      for (int j = 0; j < 32; j += JSTEP) {
+        const float4 a0 = A0[j], a1 = A1[j], a2 = A2[j];
+#pragma unroll
+        for (int v = 0; v < NV; v++) quad_acc(av[v], iv[v], a0, a1, a2, veps2);
+      }
+      a_head = (a_head + 32) & 63;
+      a_cnt -= 32;
+      n_app += 32;
+    };
+    auto eval_dir = [&]() {
+      const float4* D = &s_d[w][d_head + half];
+      BONSAI_UNROLL_N(BONSAI_WALK_UNROLL)
+      for (int j = 0; j < 32; j += JSTEP) {
+        const float4 pj = D[j];
+#pragma unroll
+        for (int v = 0; v < NV; v++) mono_acc(av[v], iv[v], pj, veps2);
+      }
+      d_head = (d_head + 32) & (kDirRing - 1);
+      d_cnt -= 32;
+      n_dir += 32;
+    };
+
     while (ncur > 0 && !overflow) {
       for (int blk = 0; blk < ncur; blk += 32) {
+#if BONSAI_WALK_EVAL_EARLY
+        if (a_cnt >= 32 || d_cnt >= 32) {
+          cp_async_wait_all();
+          __syncwarp();
+          if (a_cnt >= 32) eval_app();
+          while (d_cnt >= 32) eval_dir();
+          __syncwarp();
+        }
+#endif
         const int li = blk + lane;
         const bool inlist = li < ncur;
         const int cell = inlist ? lists[cb + li] : 0;
         const bool valid = inlist && BONSAI_IN_RANGE(cell, ncells, 0x404);
         uint4 cd = make_uint4(0u, 0xFFFFFFFFu, 0u, 0u);
         float4 co = make_float4(0.f, 0.f, 0.f, 0.f);
-        float mk = 0.f;  // M l^3 (relative test)
+        float4 ls = make_float4(0.f, 0.f, 0.f, 0.f);
         if (valid) {
           cd = __ldg(cell_data + cell);
           co = __ldg(cell_open + cell);
@@ -300,12 +370,25 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
             co.y = __fadd_rn(__fsub_rn(co.y, R.y), cl.y);
             co.z = __fadd_rn(__fsub_rn(co.z, R.z), cl.z);
           }
-          if (PERGROUP) {
-            const float4 ls = __ldg(cell_ls + cell);
-            const float op = __fmaf_rn(ls.x, inv_theta_g, ls.y);
-            co.w = __fmul_rn(op, op);
-            mk = ls.z;
-          }
+          if (PERGROUP) ls = __ldg(cell_ls + cell);
+        }
+#if !BONSAI_WALK_EVAL_EARLY
+        // (0) while this block's records are in flight, evaluate the full
+        // batches that earlier blocks staged (their copies have had at least
+        // one block's traversal to land)
+        if (a_cnt >= 32 || d_cnt >= 32) {
+          cp_async_wait_all();
+          __syncwarp();
+          if (a_cnt >= 32) eval_app();
+          while (d_cnt >= 32) eval_dir();
+          __syncwarp();
+        }
+#endif
+        float mk = 0.f;  // M l^3 (relative test)
+        if (PERGROUP && valid) {
+          const float op = __fmaf_rn(ls.x, inv_theta_g, ls.y);
+          co.w = __fmul_rn(op, op);
+          mk = ls.z;
         }
         const bool leaf = cd.y == 0xFFFFFFFFu;
         // the squared box-to-COM distance, shared by the geometric test (the
@@ -352,43 +435,32 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
 #endif
         nnext += tot;
 
-        // (2) accepted cells -> approximate list (staged by value)
+        // (2) accepted cells -> approximate ring, copied by value from the
+        // staged records (at most 31 + 32 entries pending)
         const bool app = valid && !split;
         const unsigned bal = __ballot_sync(kFull, app);
         if (app) {
           const int slot = (a_head + a_cnt + __popc(bal & lt)) & 63;
-          const float4 q1 = __ldg(cell_q1 + cell);
-          const float4 q0 = __ldg(cell_q0 + cell);
+          const float4* src = cell_stage + 3 * (size_t)cell;
           if (PERGROUP && rel.stats) {
+            // M from M l^3 and l; tr I from 1.5 tr I (cell_ls)
+            const float m = __fdividef(ls.z, __fmul_rn(ls.x, __fmul_rn(ls.x, ls.x)));
             const float inv = __frcp_rn(fmaxf(ds2, 1e-30f));
-            st_macc += q0.x;
-            st_mnear += near ? q0.x : 0.f;
-            st_qn += q1.w * (2.0f / 3.0f) * inv * inv;  // tr I / ds^4 = (M / ds^2) (b / ds)^2
-            st_wm += q0.x * inv;                         // the cell's force share M / ds^2
+            st_macc += m;
+            st_mnear += near ? m : 0.f;
+            st_qn += ls.w * (2.0f / 3.0f) * inv * inv;  // tr I / ds^4 = (M / ds^2) (b / ds)^2
+            st_wm += m * inv;                           // the cell's force share M / ds^2
           }
-          s_a0[w][slot] = make_float4(co.x, co.y, co.z, q1.w * (-1.0f / 3.0f));
-          s_a1[w][slot] = make_float4(q0.x, -q0.y, -q0.z, -q0.w);
-          s_a2[w][slot] = make_float4(-q1.x, -q1.y, -q1.z, -q1.w);
+          if (DS)  // the COM relative to the group's reference point
+            s_a0[w][slot] = make_float4(co.x, co.y, co.z, __ldg(&src[0].w));
+          else
+            cp_async16(&s_a0[w][slot], src);
+          cp_async16(&s_a1[w][slot], src + 1);
+          cp_async16(&s_a2[w][slot], src + 2);
         }
         a_cnt += __popc(bal);
-        if (a_cnt >= 32) {
-          __syncwarp();
-          const float4* A0 = &s_a0[w][a_head + half];
-          const float4* A1 = &s_a1[w][a_head + half];
-          const float4* A2 = &s_a2[w][a_head + half];
-          BONSAI_UNROLL_N(BONSAI_WALK_UNROLL)
-          for (int j = 0; j < 32; j += JSTEP) {
-            const float4 a0 = A0[j], a1 = A1[j], a2 = A2[j];
-#pragma unroll
-            for (int v = 0; v < NV; v++) quad_acc(av[v], iv[v], a0, a1, a2, veps2);
-          }
-          __syncwarp();
-          a_head = (a_head + 32) & 63;
-          a_cnt -= 32;
-          n_app += 32;
-        }
 
-        // (3) particles of opened leaves -> direct list
+        // (3) particles of opened leaves -> direct ring
         const int nb = (split && leaf) ? (int)(cd.w - cd.z) : 0;
         const int incl2 = warp_incl_scan(nb);
         const int tot2 = __shfl_sync(kFull, incl2, 31);
@@ -399,32 +471,27 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
           const int f = __shfl_sync(kFull, pb, src);
           const int e = __shfl_sync(kFull, incl2 - nb, src);
           const int cnt = min(32, tot2 - base);
+          if (d_cnt + cnt > kDirRing) {  // no room: evaluate one batch now
+            cp_async_wait_all();
+            __syncwarp();
+            eval_dir();
+            __syncwarp();
+          }
           if (lane < cnt) {
             const int jj = BONSAI_IN_RANGE(f + (s - e), npart, 0x406) ? f + (s - e) : 0;
-            float4 pj = __ldg(jpos + jj);
+            float4* dst = &s_d[w][(d_head + d_cnt + lane) & (kDirRing - 1)];
             if (DS) {
+              float4 pj = __ldg(jpos + jj);
               const float4 lo = __ldg(jpos_lo + jj);
               pj.x = __fadd_rn(__fsub_rn(pj.x, R.x), lo.x);
               pj.y = __fadd_rn(__fsub_rn(pj.y, R.y), lo.y);
               pj.z = __fadd_rn(__fsub_rn(pj.z, R.z), lo.z);
+              *dst = pj;
+            } else {
+              cp_async16(dst, jpos + jj);
             }
-            s_d[w][(d_head + d_cnt + lane) & 63] = pj;
           }
           d_cnt += cnt;
-          if (d_cnt >= 32) {
-            __syncwarp();
-            const float4* D = &s_d[w][d_head + half];
-            BONSAI_UNROLL_N(BONSAI_WALK_UNROLL)
-            for (int j = 0; j < 32; j += JSTEP) {
-              const float4 pj = D[j];
-#pragma unroll
-              for (int v = 0; v < NV; v++) mono_acc(av[v], iv[v], pj, veps2);
-            }
-            __syncwarp();
-            d_head = (d_head + 32) & 63;
-            d_cnt -= 32;
-            n_dir += 32;
-          }
         }
       }
       cb ^= half_cap;
@@ -433,7 +500,8 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
       __syncwarp();
     }
 
-    // flush the partial batches
+    // the remaining batches, full and partial
+    cp_async_wait_all();
     __syncwarp();
     for (int j = half; j < a_cnt; j += JSTEP) {
       const int sl = (a_head + j) & 63;
@@ -443,7 +511,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
     }
     n_app += a_cnt;
     for (int j = half; j < d_cnt; j += JSTEP) {
-      const float4 pj = s_d[w][(d_head + j) & 63];
+      const float4 pj = s_d[w][(d_head + j) & (kDirRing - 1)];
 #pragma unroll
       for (int v = 0; v < NV; v++) mono_acc(av[v], iv[v], pj, veps2);
     }
@@ -555,14 +623,14 @@ int walk_blocks_per_sm(int variant) {
 }
 
 void launch_walk(int variant, int nblocks, const int2* groups, const TreeInfo* info, const float4* ipos,
-                 const float4* jpos, const uint4* cell_data, const float4* cell_open, const float4* cell_q0,
-                 const float4* cell_q1, const float4* cell_ls, const float* group_inv_theta, float eps2,
+                 const float4* jpos, const uint4* cell_data, const float4* cell_open, const float4* cell_stage,
+                 const float4* cell_ls, const float* group_inv_theta, float eps2,
                  float4* acc, int* ring_pool, int ring_cap, unsigned* group_counter, unsigned long long* stats,
                  int* status, const int* sys_off, int nsys, const int* root_beg, const float4* ipos_lo,
                  const float4* jpos_lo, const float4* cell_lo, uint2* group_counts, const int* group_list,
                  const unsigned* group_list_n, const RelativeArgs& rel, cudaStream_t s) {
 #define BONSAI_WALK_ARGS                                                                                          \
-  groups, info, ipos, jpos, cell_data, cell_open, cell_q0, cell_q1, cell_ls, group_inv_theta, eps2, acc, ring_pool, \
+  groups, info, ipos, jpos, cell_data, cell_open, cell_stage, cell_ls, group_inv_theta, eps2, acc, ring_pool, \
       ring_cap, group_counter, stats, status, sys_off, nsys, root_beg, ipos_lo, jpos_lo, cell_lo, group_counts,  \
       group_list, group_list_n, rel
 #define BONSAI_WALK(NI, SP)                                                                \
