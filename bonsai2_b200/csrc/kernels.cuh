@@ -15,6 +15,10 @@ constexpr int kMlpWeights = kMlpHidden * kMlpFeatures + kMlpHidden + kMlpHidden 
 constexpr int kWalkMinBlocks = BONSAI_WALK_MINB;
 
 // keys.cu
+// PH state tables: one level per lookup (48 states x 8 octants), then two
+// levels per lookup (48 x 64)
+constexpr int kPhTable1 = 48 * 8;
+constexpr int kPhTableSize = kPhTable1 + 48 * 64;
 void build_ph_table(uint16_t* tab);
 __global__ void k_box(const float4* __restrict__ pos, int n, float* __restrict__ partial, unsigned* __restrict__ ticket,
                       Box* __restrict__ box, int* __restrict__ status);
