@@ -161,67 +161,67 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_chains(const unsigned lon
 
 // One block: exclusive scan of each histogram row across tiles, rows chained
 // so that offsets are global (cells level-major; leaves ordered likewise).
+// The rows are independent once their totals are known: each warp sums its
+// rows, one thread chains the row totals into row bases (and fills the tree
+// info), then each warp scans its rows, four entries per lane per step.
 __global__ void __launch_bounds__(1024) k_tree_scan(unsigned* __restrict__ hist, int nb, int cell_cap,
                                                     int leaf_cap, int n, TreeInfo* __restrict__ info) {
-  __shared__ unsigned sh[32];
-  __shared__ unsigned carry;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  unsigned tot_cells = 0, tot_leaves = 0;
-  int nlevels = 0;
-  for (int row = 0; row < 2 * kNL; row++) {
-    const int L = row % kNL;
-    if (threadIdx.x == 0) {
-      carry = (row < kNL) ? tot_cells : tot_leaves;
-      if (row < kNL) info->level_beg[L] = (int)carry;
-    }
-    __syncthreads();
-    unsigned* h = hist + row * nb;
-    for (int b0 = 0; b0 < nb; b0 += 1024) {
-      const int b = b0 + threadIdx.x;
-      const unsigned v = (b < nb && L > 0) ? h[b] : 0u;
-      unsigned x = v;
+  __shared__ unsigned rowtot[2 * kNL], rowbase[2 * kNL];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int row = w; row < 2 * kNL; row += nw) {
+    const unsigned* h = hist + (size_t)row * nb;
+    unsigned sum = 0;
+    if (row % kNL > 0)
+      for (int b = lane; b < nb; b += 32) sum += h[b];
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const unsigned t = __shfl_up_sync(kFull, x, o);
-        if (lane >= o) x += t;
-      }
-      if (lane == 31) sh[w] = x;
-      __syncthreads();
-      if (w == 0) {
-        unsigned y = sh[lane];
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const unsigned t = __shfl_up_sync(kFull, y, o);
-          if (lane >= o) y += t;
-        }
-        sh[lane] = y;
-      }
-      __syncthreads();
-      const unsigned excl = (w ? sh[w - 1] : 0u) + x - v;
-      if (b < nb) h[b] = carry + excl;
-      __syncthreads();
-      if (threadIdx.x == 0) carry += sh[31];
-      __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-      if (row < kNL) {
-        if (L > 0 && carry > tot_cells) nlevels = L;
-        tot_cells = carry;
-        info->level_end[L] = (int)carry;
-      } else {
-        tot_leaves = carry;
-      }
-    }
-    __syncthreads();
+    for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
+    if (lane == 0) rowtot[row] = sum;
   }
+  __syncthreads();
   if (threadIdx.x == 0) {
-    for (int L = kNL; L < kLevels; L++) info->level_beg[L] = info->level_end[L] = (int)tot_cells;
-    info->ncells = (int)tot_cells;
-    info->nleaves = (int)tot_leaves;
-    info->nnodes = (int)(tot_cells - tot_leaves);
+    unsigned tc = 0, tl = 0;
+    int nlevels = 0;
+    for (int L = 0; L < kNL; L++) {
+      rowbase[L] = tc;
+      info->level_beg[L] = (int)tc;
+      if (L > 0 && rowtot[L] > 0) nlevels = L;
+      tc += rowtot[L];
+      info->level_end[L] = (int)tc;
+    }
+    for (int L = 0; L < kNL; L++) {
+      rowbase[kNL + L] = tl;
+      tl += rowtot[kNL + L];
+    }
+    for (int L = kNL; L < kLevels; L++) info->level_beg[L] = info->level_end[L] = (int)tc;
+    info->ncells = (int)tc;
+    info->nleaves = (int)tl;
+    info->nnodes = (int)(tc - tl);
     info->nlevels = nlevels;
     info->npart = n;
-    if ((int)tot_cells > cell_cap || (int)tot_leaves > leaf_cap) set_status(&info->status, kStatusCellCapacity);
+    if ((int)tc > cell_cap || (int)tl > leaf_cap) set_status(&info->status, kStatusCellCapacity);
+  }
+  __syncthreads();
+  for (int row = w; row < 2 * kNL; row += nw) {
+    unsigned* h = hist + (size_t)row * nb;
+    const bool live = row % kNL > 0;
+    unsigned carry = rowbase[row];
+    for (int b0 = 0; b0 < nb; b0 += 128) {
+      const int b = b0 + 4 * lane;
+      unsigned v[4], s = 0;
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        v[q] = (live && b + q < nb) ? h[b + q] : 0u;
+        s += v[q];
+      }
+      const unsigned incl = (unsigned)warp_incl_scan((int)s);
+      unsigned run = carry + incl - s;
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        if (b + q < nb) h[b + q] = run;
+        run += v[q];
+      }
+      carry += __shfl_sync(kFull, incl, 31);
+    }
   }
 }
 
