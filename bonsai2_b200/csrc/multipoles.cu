@@ -114,9 +114,54 @@ __device__ __forceinline__ bool arrive_last(int* p, int nch) {
   return true;
 }
 
+// A child's record fields.  CACHED (the level passes, whose children were
+// written by earlier launches): 16-byte vector loads through L1, so a record
+// costs 5 load instructions and its second read hits L1; otherwise (the
+// arrival-counter climb, whose siblings wrote them in this launch) 8-byte
+// loads from L2.
+template <bool CACHED>
+__device__ __forceinline__ void load_mass_com(const MpRec* r, double& m, double& x, double& y, double& z) {
+  if (CACHED) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(r)), b = __ldg(reinterpret_cast<const double2*>(r) + 1);
+    m = a.x; x = a.y; y = b.x; z = b.y;
+  } else {
+    m = __ldcg(&r->m); x = __ldcg(&r->cx); y = __ldcg(&r->cy); z = __ldcg(&r->cz);
+  }
+}
+template <bool CACHED>
+__device__ __forceinline__ MpRec load_rec(const MpRec* r) {
+  MpRec o;
+  if (CACHED) {
+    const double2* q = reinterpret_cast<const double2*>(r);
+    const double2 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3), e = __ldg(q + 4);
+    o.m = a.x; o.cx = a.y; o.cy = b.x; o.cz = b.y;
+    o.ixx = c.x; o.iyy = c.y; o.izz = d.x; o.ixy = d.y; o.ixz = e.x; o.iyz = e.y;
+  } else {
+    o.m = __ldcg(&r->m); o.cx = __ldcg(&r->cx); o.cy = __ldcg(&r->cy); o.cz = __ldcg(&r->cz);
+    o.ixx = __ldcg(&r->ixx); o.iyy = __ldcg(&r->iyy); o.izz = __ldcg(&r->izz);
+    o.ixy = __ldcg(&r->ixy); o.ixz = __ldcg(&r->ixz); o.iyz = __ldcg(&r->iyz);
+  }
+  return o;
+}
+template <bool CACHED, class B>
+__device__ __forceinline__ void load_box(const B* bk, B lo[3], B hi[3]) {
+  if (CACHED && sizeof(B) == 4) {
+    const float2* q = reinterpret_cast<const float2*>(bk);  // 24 B per cell: 8-byte aligned
+    const float2 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+    lo[0] = (B)a.x; lo[1] = (B)a.y; lo[2] = (B)b.x; hi[0] = (B)b.y; hi[1] = (B)c.x; hi[2] = (B)c.y;
+  } else if (CACHED) {
+    const double2* q = reinterpret_cast<const double2*>(bk);  // 48 B per cell: 16-byte aligned
+    const double2 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+    lo[0] = (B)a.x; lo[1] = (B)a.y; lo[2] = (B)b.x; hi[0] = (B)b.y; hi[1] = (B)c.x; hi[2] = (B)c.y;
+  } else {
+#pragma unroll
+    for (int a = 0; a < 3; a++) { lo[a] = __ldcg(bk + a); hi[a] = __ldcg(bk + 3 + a); }
+  }
+}
+
 // A parent's moments from its nch contiguous children (parallel-axis
 // theorem, FP64), the children taken in index order.
-template <bool DS>
+template <bool DS, bool CACHED>
 __device__ void combine_children(int p, int first, int nch, float inv_theta, MpRec* __restrict__ rec,
                                  typename BoxOf<DS>::T* __restrict__ box, float4* __restrict__ cell_open,
                                  float4* __restrict__ cell_stage,
@@ -133,11 +178,8 @@ __device__ void combine_children(int p, int first, int nch, float inv_theta, MpR
 #pragma unroll
     for (int u = 0; u < kB; u++) {
       const int k = min(k0 + u, nch - 1);
-      const MpRec* ck = rec + first + k;
-      mb[u] = __ldcg(&ck->m); xb[u] = __ldcg(&ck->cx); yb[u] = __ldcg(&ck->cy); zb[u] = __ldcg(&ck->cz);
-      const B* bk = box + 6 * (size_t)(first + k);
-#pragma unroll
-      for (int a = 0; a < 3; a++) { lo[u][a] = __ldcg(bk + a); hi[u][a] = __ldcg(bk + 3 + a); }
+      load_mass_com<CACHED>(rec + first + k, mb[u], xb[u], yb[u], zb[u]);
+      load_box<CACHED>(box + 6 * (size_t)(first + k), lo[u], hi[u]);
     }
 #pragma unroll
     for (int u = 0; u < kB; u++) {
@@ -164,10 +206,7 @@ __device__ void combine_children(int p, int first, int nch, float inv_theta, MpR
     MpRec cb[kB2];
 #pragma unroll
     for (int u = 0; u < kB2; u++) {
-      const MpRec* ck = rec + first + min(k0 + u, nch - 1);
-      cb[u].m = __ldcg(&ck->m); cb[u].cx = __ldcg(&ck->cx); cb[u].cy = __ldcg(&ck->cy); cb[u].cz = __ldcg(&ck->cz);
-      cb[u].ixx = __ldcg(&ck->ixx); cb[u].iyy = __ldcg(&ck->iyy); cb[u].izz = __ldcg(&ck->izz);
-      cb[u].ixy = __ldcg(&ck->ixy); cb[u].ixz = __ldcg(&ck->ixz); cb[u].iyz = __ldcg(&ck->iyz);
+      cb[u] = load_rec<CACHED>(rec + first + min(k0 + u, nch - 1));
     }
 #pragma unroll
     for (int u = 0; u < kB2; u++) {
@@ -202,7 +241,7 @@ __device__ void climb(int c, [[maybe_unused]] int ncells, const uint4* __restric
     const int first = (int)(y & 0x1FFFFFFFu), nch = (int)(y >> 29) + 1;
     if (!BONSAI_IN_RANGE(first + nch - 1, ncells, 0x304) || !BONSAI_IN_RANGE(c - first, nch, 0x305)) break;
     if (!arrive_last(mp_count + p, nch)) break;
-    combine_children<DS>(p, first, nch, inv_theta, rec, box, cell_open, cell_stage, cell_ls, cell_lo);
+    combine_children<DS, false>(p, first, nch, inv_theta, rec, box, cell_open, cell_stage, cell_ls, cell_lo);
     c = p;
   }
 }
@@ -223,7 +262,7 @@ __global__ void __launch_bounds__(256) k_mp_level(int L, const TreeInfo* __restr
     if (y == 0xFFFFFFFFu) continue;
     const int first = (int)(y & 0x1FFFFFFFu), nch = (int)(y >> 29) + 1;
     if (!BONSAI_IN_RANGE(first + nch - 1, ncells, 0x307)) continue;
-    combine_children<DS>(c, first, nch, inv_theta, rec, box, cell_open, cell_stage, cell_ls, cell_lo);
+    combine_children<DS, true>(c, first, nch, inv_theta, rec, box, cell_open, cell_stage, cell_ls, cell_lo);
   }
 }
 
