@@ -43,16 +43,23 @@ struct Chain {
   int a, b;  // levels [a, b]; a == 0: no cell starts here
 };
 
-// sd[loc + j] = d(i + j) for j in [-kHalo, kHalo] (0 past n); wm[x] = min of sd
-// over [x, x + wp), wp the largest power of two <= nleaf, so that
-// m(i) = min d(i+1 .. i+nleaf) = min(wm[loc + 1], wm[loc + 1 + nleaf - wp])
-__device__ __forceinline__ Chain make_chain(const uint8_t* sd, const uint8_t* wm, int wp, int loc, int i, int n,
+constexpr int kLen = kTreeTile + 2 * kHalo;  // positions of a tile with its halo
+
+// sd[loc + j] = d(i + j) for j in [-kHalo, kHalo] (0 past n); W[k - 1][x] =
+// min of sd over [x, x + 2^k) for 2^k <= wp, wp the largest power of two <=
+// nleaf (0 where the window leaves the tile), so that
+// m(i) = min d(i+1 .. i+nleaf) = min(W[K][loc + 1], W[K][loc + 1 + nleaf - wp]).
+__device__ __forceinline__ uint8_t wmin(const uint8_t* sd, const uint8_t* W, int k, int x) {
+  return k == 0 ? sd[x] : W[(k - 1) * kLen + x];
+}
+__device__ __forceinline__ Chain make_chain(const uint8_t* sd, const uint8_t* W, int K, int wp, int loc, int i, int n,
                                             int nleaf, bool* fat) {
   Chain c{0, 0};
   const int di = (i == 0) ? 0 : (int)sd[loc];
   const int ls = max(di, 1);
   if (ls > kMaxLevel) return c;
-  const int m = min((int)wm[loc + 1], (int)wm[loc + 1 + nleaf - wp]);
+  const int m = K == 0 ? min((int)sd[loc + 1], (int)sd[loc + 1 + nleaf - wp])
+                       : min((int)W[(K - 1) * kLen + loc + 1], (int)W[(K - 1) * kLen + loc + 1 + nleaf - wp]);
   if (ls < m) {
     c.a = ls;
     c.b = min(m, kMaxLevel);
@@ -63,19 +70,26 @@ __device__ __forceinline__ Chain make_chain(const uint8_t* sd, const uint8_t* wm
     c.a = c.b = 1;
     return c;
   }
-  // parent run at level ls-1 containing i: [p, e)
-  int p = -1, e = -1;
-  for (int j = 1; j <= nleaf; j++) {
-    const int q = i - j;
-    if (q <= 0) { p = 0; break; }
-    if ((int)sd[loc - j] <= ls - 1) { p = q; break; }
+  // the parent run at level ls-1 containing i is [p, e): p the nearest
+  // position <= i - 1 with d <= ls-1 (d = 0 at and before position 0), e the
+  // nearest position >= i + 1 with d <= ls-1 (d = 0 at and past n), each
+  // looked for within nleaf positions by binary lifting over the window
+  // minima; the small run starting here is a leaf iff the parent holds more
+  // than nleaf particles (or a bound is not found within nleaf)
+  const int l1 = ls - 1;
+  int xb = loc;  // [xb, loc - 1] all > l1
+  for (int k = K; k >= 0; k--) {
+    const int st = 1 << k;
+    if (xb - st >= loc - nleaf && (int)wmin(sd, W, k, xb - st) > l1) xb -= st;
   }
-  for (int j = 1; j <= nleaf; j++) {
-    const int q = i + j;
-    if (q >= n) { e = n; break; }
-    if ((int)sd[loc + j] <= ls - 1) { e = q; break; }
+  int xf = loc + 1;  // [loc + 1, xf - 1] all > l1
+  for (int k = K; k >= 0; k--) {
+    const int st = 1 << k;
+    if (xf + st - 1 <= loc + nleaf && (int)wmin(sd, W, k, xf) > l1) xf += st;
   }
-  if (p < 0 || e < 0 || e - p > nleaf) c.a = c.b = ls;
+  const bool found = xb > loc - nleaf && xf <= loc + nleaf;
+  // p = i - (loc - xb + 1), e = i + (xf - loc): e - p = xf - xb + 1
+  if (!found || xf - xb + 1 > nleaf) c.a = c.b = ls;
   return c;
 }
 
@@ -124,17 +138,15 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_chains(const unsigned lon
   load_d_from_keys(keys, n, t0, sd, sk, sys_off, nsys);
   for (int j = threadIdx.x; j < kTreeTile; j += blockDim.x)
     if (t0 + j < n) dlev[t0 + j] = sd[kHalo + j];
-  // window minima of d by doubling, in the key buffer's space (no longer read)
-  constexpr int kLen = kTreeTile + 2 * kHalo;
-  uint8_t* cur = reinterpret_cast<uint8_t*>(sk);
-  uint8_t* nxt = cur + kLen;
-  for (int j = threadIdx.x; j < kLen; j += blockDim.x) cur[j] = sd[j];
-  __syncthreads();
-  int wp = 1;
-  for (; 2 * wp <= nleaf; wp *= 2) {
-    for (int j = threadIdx.x; j < kLen; j += blockDim.x) nxt[j] = min(cur[j], j + wp < kLen ? cur[j + wp] : (uint8_t)0);
+  // window minima of d by doubling, every level kept (W[k-1]: windows of
+  // 2^k), in the key buffer's space (no longer read)
+  uint8_t* W = reinterpret_cast<uint8_t*>(sk);
+  int wp = 1, K = 0;
+  for (; 2 * wp <= nleaf; wp *= 2, K++) {
+    const uint8_t* prev = K == 0 ? sd : W + (K - 1) * kLen;
+    uint8_t* out = W + K * kLen;
+    for (int j = threadIdx.x; j < kLen; j += blockDim.x) out[j] = min(prev[j], j + wp < kLen ? prev[j + wp] : (uint8_t)0);
     __syncthreads();
-    uint8_t* t = cur; cur = nxt; nxt = t;
   }
   bool anyfat = false;
   const int i0 = t0 + threadIdx.x * kTreeItems;
@@ -143,7 +155,7 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_chains(const unsigned lon
     const int i = i0 + k;
     if (i >= n) break;
     bool fat = false;
-    const Chain c = make_chain(sd, cur, wp, kHalo + (i - t0), i, n, nleaf, &fat);
+    const Chain c = make_chain(sd, W, K, wp, kHalo + (i - t0), i, n, nleaf, &fat);
     anyfat |= fat;
     chain[i] = (uint16_t)(c.a | (c.b << 8));
     if (c.a) {
@@ -248,24 +260,19 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_cells(
     boff[1][threadIdx.x] = hist[(kNL + threadIdx.x) * nb + blockIdx.x];
   }
   const int i0 = t0 + threadIdx.x * kTreeItems;
-  int ca[kTreeItems], cb[kTreeItems];
-#pragma unroll
+  // per-thread totals per level (cells of the thread's chains; leaves)
+  for (int L = 0; L < kNL; L++) {
+    cpre[L][threadIdx.x] = 0;
+    lpre[L][threadIdx.x] = 0;
+  }
+#pragma unroll 4
   for (int k = 0; k < kTreeItems; k++) {
     const int i = i0 + k;
     const unsigned c = (i < n) ? (unsigned)chain[i] : 0u;
-    ca[k] = (int)(c & 255u);
-    cb[k] = (int)(c >> 8);
-  }
-  // per-thread totals per level
-  for (int L = 0; L < kNL; L++) {
-    unsigned cc = 0, lc = 0;
-#pragma unroll
-    for (int k = 0; k < kTreeItems; k++) {
-      cc += (ca[k] && ca[k] <= L && L <= cb[k]);
-      lc += (ca[k] && cb[k] == L);
-    }
-    cpre[L][threadIdx.x] = (uint16_t)cc;
-    lpre[L][threadIdx.x] = (uint16_t)lc;
+    const int a = (int)(c & 255u), b = (int)(c >> 8);
+    if (!a) continue;
+    for (int L = a; L <= b; L++) cpre[L][threadIdx.x]++;
+    lpre[b][threadIdx.x]++;
   }
   __syncthreads();
   // exclusive scans of the 2*kNL rows over the 256 threads (one warp per row)
@@ -283,31 +290,23 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_cells(
     }
   }
   __syncthreads();
+  // cpre[L][t] / lpre[L][t] now hold the thread's first cell / leaf slot at
+  // level L (relative to the level's block offset) and advance as its items
+  // are written: an item's cells and links read them before it adds its own
 #pragma unroll 1
   for (int k = 0; k < kTreeItems; k++) {
     const int i = i0 + k;
     if (i >= n) break;
-    const int a = ca[k], b = cb[k];
+    const unsigned c = (unsigned)chain[i];  // (the thread's 32 bytes of chain words, cached)
+    const int a = (int)(c & 255u), b = (int)(c >> 8);
     if (!a) continue;
     const int loc = kHalo + (i - t0);
-    // leaf index
     {
-      int lk = 0;
-      for (int q = 0; q < k; q++) lk += (ca[q] && cb[q] == b);
-      const int leaf_idx = (int)(boff[1][b] + lpre[b][threadIdx.x]) + lk;
-      int lc = 0;
-      for (int q = 0; q < k; q++) lc += (ca[q] && ca[q] <= b && b <= cb[q]);
-      if (BONSAI_IN_RANGE(leaf_idx, nleaves, 0x101)) leaf_list[leaf_idx] = (int)(boff[0][b] + cpre[b][threadIdx.x]) + lc;
+      const int leaf_idx = (int)(boff[1][b] + lpre[b][threadIdx.x]);
+      if (BONSAI_IN_RANGE(leaf_idx, nleaves, 0x101)) leaf_list[leaf_idx] = (int)(boff[0][b] + cpre[b][threadIdx.x]);
     }
     for (int L = a; L <= b; L++) {
-      int lc = 0, lcp = 0, lc1 = 0;
-      for (int q = 0; q < k; q++) {
-        const bool any = ca[q] != 0;
-        lc += (any && ca[q] <= L && L <= cb[q]);
-        lcp += (any && ca[q] <= L - 1 && L - 1 <= cb[q]);
-        lc1 += (any && ca[q] <= L + 1 && L + 1 <= cb[q]);
-      }
-      const int cidx = (int)(boff[0][L] + cpre[L][threadIdx.x]) + lc;
+      const int cidx = (int)(boff[0][L] + cpre[L][threadIdx.x]);
       if (!BONSAI_IN_RANGE(cidx, ncells, 0x102)) continue;
       const bool leaf = (L == b);
       uint4 cd;
@@ -320,18 +319,20 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_cells(
         // the parent is the last level-(L-1) cell starting at or before i:
         // the one starting at i when the chain here covers level L-1, else
         // the one before the first level-(L-1) cell that starts after i
-        parent = (int)(boff[0][L - 1] + cpre[L - 1][threadIdx.x]) + lcp - (a <= L - 1 ? 0 : 1);
+        parent = (int)(boff[0][L - 1] + cpre[L - 1][threadIdx.x]) - (a <= L - 1 ? 0 : 1);
         cd.x = (unsigned)parent | ((unsigned)L << 27);
       }
       // nodes: the first child (children are contiguous at level L + 1); the
       // child count and every cell's run end follow in the level passes
-      cd.y = leaf ? 0xFFFFFFFFu : (unsigned)((int)(boff[0][L + 1] + cpre[L + 1][threadIdx.x]) + lc1);
+      cd.y = leaf ? 0xFFFFFFFFu : (unsigned)((int)(boff[0][L + 1] + cpre[L + 1][threadIdx.x]));
       cd.z = (unsigned)i;
       cd.w = (unsigned)i;
       cell_data[cidx] = cd;
       cell_parent[cidx] = parent;
       mp_count[cidx] = 0;
     }
+    for (int L = a; L <= b; L++) cpre[L][threadIdx.x]++;
+    lpre[b][threadIdx.x]++;
   }
 }
 
