@@ -53,7 +53,10 @@ struct BoxOf<true> {
   typedef double T;
 };
 
-constexpr int kMpBatch = 4;  // leaf particles loaded ahead of their sums
+#ifndef BONSAI_MP_BATCH
+#define BONSAI_MP_BATCH 4
+#endif
+constexpr int kMpBatch = BONSAI_MP_BATCH;  // leaf particles loaded ahead of their sums
 
 template <bool DS>
 __device__ __forceinline__ void store_cell(int c, const MpRec& r, const typename BoxOf<DS>::T* bmin,

@@ -83,6 +83,9 @@ struct IPart {
 #ifndef BONSAI_WALK_ASYNC
 #define BONSAI_WALK_ASYNC 1
 #endif
+#ifndef BONSAI_WALK_LIST_AHEAD
+#define BONSAI_WALK_LIST_AHEAD 1
+#endif
 #ifndef BONSAI_WALK_EVAL_EARLY
 #define BONSAI_WALK_EVAL_EARLY 1
 #endif
@@ -344,7 +347,15 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
     };
 
     while (ncur > 0 && !overflow) {
+#if BONSAI_WALK_LIST_AHEAD
+      // the level's list entries are read one 32-cell block ahead
+      int cell_ahead = lane < ncur ? lists[cb + lane] : 0;
+#endif
       for (int blk = 0; blk < ncur; blk += 32) {
+#if BONSAI_WALK_LIST_AHEAD
+        const int cell_here = cell_ahead;
+        if (blk + 32 < ncur) cell_ahead = blk + 32 + lane < ncur ? lists[cb + blk + 32 + lane] : 0;
+#endif
 #if BONSAI_WALK_EVAL_EARLY
         if (a_cnt >= 32 || d_cnt >= 32) {
           cp_async_wait_all();
@@ -356,7 +367,11 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
 #endif
         const int li = blk + lane;
         const bool inlist = li < ncur;
+#if BONSAI_WALK_LIST_AHEAD
+        const int cell = inlist ? cell_here : 0;
+#else
         const int cell = inlist ? lists[cb + li] : 0;
+#endif
         const bool valid = inlist && BONSAI_IN_RANGE(cell, ncells, 0x404);
         uint4 cd = make_uint4(0u, 0xFFFFFFFFu, 0u, 0u);
         float4 co = make_float4(0.f, 0.f, 0.f, 0.f);
