@@ -123,6 +123,28 @@ void exclusive_scan(const unsigned* in, unsigned* out, int m, unsigned* bsum, un
 // pass.
 // ---------------------------------------------------------------------------
 constexpr unsigned kFlagAgg = 1u << 30, kFlagInc = 2u << 30, kValMask = (1u << 30) - 1u;
+
+// The lanes holding the same digit (0..256, 256 = no key): the intersection
+// of nine bit ballots (BONSAI_SORT_BALLOT_MATCH, the default), or
+// __match_any_sync, which was slower on the B200 (PH sort + group formation at
+// N = 2^24: 1.82 against 1.93 ms).  Issuing all items' ballots before the
+// chain through the warp's counters was measured no faster.
+#ifndef BONSAI_SORT_BALLOT_MATCH
+#define BONSAI_SORT_BALLOT_MATCH 1
+#endif
+__device__ __forceinline__ unsigned digit_peers(unsigned d) {
+#if BONSAI_SORT_BALLOT_MATCH
+  unsigned m = kFull;
+#pragma unroll
+  for (int b = 0; b < 9; b++) {
+    const unsigned bal = __ballot_sync(kFull, (d >> b) & 1u);
+    m &= ((d >> b) & 1u) ? bal : ~bal;
+  }
+  return m;
+#else
+  return __match_any_sync(kFull, d);
+#endif
+}
 constexpr int kLookbackSpin = 1 << 22;
 
 __global__ void __launch_bounds__(kSortThreads) k_sort_hist8(const unsigned long long* __restrict__ keys, int n,
@@ -190,7 +212,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_sort_onesweep(
     }
     if ((k & 3) == 0) dpack[k >> 2] = 0u;
     dpack[k >> 2] |= (d & 255u) << (8 * (k & 3));
-    const unsigned peers = __match_any_sync(kFull, d);
+    const unsigned peers = digit_peers(d);
     const unsigned before = (unsigned)__popc(peers & lanemask_lt());
     const unsigned cur = ok ? wcnt[w][d] : 0u;
     rank[k] = cur + before;
