@@ -97,7 +97,8 @@ def parse():
     ap.add_argument("--level-split", type=int, default=5)
     ap.add_argument("--dt", type=float, default=1.0 / 128)
     ap.add_argument("--seed", type=int, default=19810614)
-    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--e2e-steps", type=int, default=20,
+                    help="pipelined end-to-end steps (the first upload and the last download are not overlapped)")
     ap.add_argument("--error-samples", type=int, default=4096)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-group-fraction", type=float, default=1.0 / 512)
