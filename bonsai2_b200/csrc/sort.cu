@@ -9,8 +9,8 @@
 // memory, tile offsets come from a decoupled look-back, and tiles are written
 // out through shared memory in contiguous digit runs.  A thread keeps only the
 // 16 ranks and packed digits of its keys across the look-back (the keys are
-// re-read from L2 for staging): 80 registers, 3 blocks per SM (keeping the
-// keys, 127 registers and 2 blocks per SM, was 16 % slower per sort).
+// re-read from L2 for staging): 4 blocks per SM (keeping the keys, 127
+// registers and 2 blocks per SM, was 16 % slower per sort than 3 blocks).
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -122,6 +122,12 @@ void exclusive_scan(const unsigned* in, unsigned* out, int m, unsigned* bsum, un
 // writes it out in contiguous runs.  One read and one write of the pairs per
 // pass.
 // ---------------------------------------------------------------------------
+// blocks per SM of the one-sweep pass: the pass is latency-bound, and 4 blocks
+// (64 registers, a 40-byte spill) beat 3 (80 registers): build phase at
+// N = 2^24 4.49 against 4.71 ms
+#ifndef BONSAI_SORT_MINB
+#define BONSAI_SORT_MINB 4
+#endif
 constexpr unsigned kFlagAgg = 1u << 30, kFlagInc = 2u << 30, kValMask = (1u << 30) - 1u;
 
 // The lanes holding the same digit (0..256, 256 = no key): the intersection
@@ -180,7 +186,7 @@ __global__ void __launch_bounds__(256) k_sort_hist_scan(unsigned* __restrict__ g
 // value, the element's position in the sort's input order), not of its key:
 // the passes that make an ensemble sort stable-partition by system last.
 template <bool SYSD>
-__global__ void __launch_bounds__(kSortThreads, 3) k_sort_onesweep(
+__global__ void __launch_bounds__(kSortThreads, BONSAI_SORT_MINB) k_sort_onesweep(
     const unsigned long long* __restrict__ keys_in, const int* __restrict__ vals_in, int n, int shift,
     const unsigned* __restrict__ gbase, unsigned* __restrict__ status, unsigned* __restrict__ tile_counter,
     unsigned long long* __restrict__ keys_out, int* __restrict__ vals_out, int* __restrict__ err,
