@@ -53,6 +53,12 @@ struct BoxOf<true> {
   typedef double T;
 };
 
+// minimum blocks per SM of the leaf and level passes (1: no bound; 5 or 6
+// blocks spill the FP64 sums and were slower: build phase 4.59 / 4.84 ms
+// against 4.50 at N = 2^24)
+#ifndef BONSAI_MP_MINB
+#define BONSAI_MP_MINB 1
+#endif
 #ifndef BONSAI_MP_BATCH
 #define BONSAI_MP_BATCH 4
 #endif
@@ -252,7 +258,7 @@ __device__ void climb(int c, [[maybe_unused]] int ncells, const uint4* __restric
 // The nodes of one level from their children, one thread per cell (leaves
 // were done by the leaf pass): the level-by-level form of the climb.
 template <bool DS>
-__global__ void __launch_bounds__(256) k_mp_level(int L, const TreeInfo* __restrict__ info,
+__global__ void __launch_bounds__(256, BONSAI_MP_MINB) k_mp_level(int L, const TreeInfo* __restrict__ info,
                                                   const uint4* __restrict__ cell_data, float inv_theta,
                                                   MpRec* __restrict__ rec, typename BoxOf<DS>::T* __restrict__ box,
                                                   float4* __restrict__ cell_open, float4* __restrict__ cell_stage, float4* __restrict__ cell_ls,
@@ -273,7 +279,7 @@ __global__ void __launch_bounds__(256) k_mp_level(int L, const TreeInfo* __restr
 // bottom-up climb.  (Half-warp-cooperative leaves
 // with shuffle reductions were measured 13x slower on the B200.)
 template <bool DS, bool CLIMB>
-__global__ void __launch_bounds__(256) k_multipoles(const int* __restrict__ leaf_list, const TreeInfo* __restrict__ info,
+__global__ void __launch_bounds__(256, BONSAI_MP_MINB) k_multipoles(const int* __restrict__ leaf_list, const TreeInfo* __restrict__ info,
                                                     const uint4* __restrict__ cell_data,
                                                     const int* __restrict__ cell_parent,
                                                     const float4* __restrict__ jpos, float inv_theta,
