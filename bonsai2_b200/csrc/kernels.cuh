@@ -81,7 +81,8 @@ struct RelativeArgs {
   float4* stats = nullptr;     // per-group statistics written by the walk (null: none)
   int* part_gid = nullptr;     // group of each particle, written with the statistics
   int* acc_valid = nullptr;    // [0] set to 1 by the walk once acc holds this evaluation's
-                               // accelerations, [1] to whether it wrote the statistics too
+                               // accelerations, [1] to where its statistics came from: 0 none,
+                               // 1 a walk without the relative test (the fallback), 2 a relative walk
 };
 
 // What the learned features read of the previous evaluation.
@@ -89,6 +90,7 @@ struct PrevEval {
   const float4* acc = nullptr;    // its accelerations, in its particle order
   const int* perm = nullptr;      // current position -> index in that order (null: the same order)
   const int* acc_valid = nullptr; // device flags: [0] acc is valid, [1] stats and part_gid came with it
+                                  // (1: from the fixed-angle fallback, 2: from a relative walk)
   const int* part_gid = nullptr;  // group of each particle in that evaluation (its order)
   const float4* stats = nullptr;  // its per-group statistics
   int stats_cap = 0;              // capacity of stats
@@ -187,9 +189,11 @@ void launch_group_features(const int2* groups, const TreeInfo* info, const float
 // the network's output y in [lo, hi] per group: tau = amag 10^y, 1/theta =
 // inv_bound; without previous accelerations the fixed angle (tau = 0,
 // 1/theta = inv_fixed)
+// start_alpha: the bound tau = start_alpha amag used instead of the network
+// when the previous statistics came from the fixed-angle fallback
 void launch_mlp_infer(const float* feat, const void* wh, const TreeInfo* info, float lo, float hi, const float* amag,
-                      const int* acc_valid, float inv_bound, float inv_fixed, float* inv, float* tau, int nblocks,
-                      cudaStream_t st);
+                      const int* acc_valid, float inv_bound, float inv_fixed, float start_alpha, float* inv, float* tau,
+                      int nblocks, cudaStream_t st);
 // relative mode with one accuracy parameter: tau = alpha amag (fallback as above)
 void launch_relative_tau(const TreeInfo* info, const float* amag, const int* acc_valid, float alpha, float inv_bound,
                          float inv_fixed, float* inv, float* tau, int nblocks, cudaStream_t st);

@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(256) k_group_features(const int2* __restrict__
 __global__ void __launch_bounds__(256) k_mlp_infer(const float* __restrict__ feat, const __half* __restrict__ wh,
                                                    const TreeInfo* __restrict__ info, float lo, float hi,
                                                    const float* __restrict__ amag, const int* __restrict__ acc_valid,
-                                                   float inv_bound, float inv_fixed,
+                                                   float inv_bound, float inv_fixed, float start_alpha,
                                                    float* __restrict__ group_inv_theta, float* __restrict__ group_tau) {
   __shared__ __half sw[kMlpWeights + 1];
   __shared__ float sh[8][kH];
@@ -206,7 +206,15 @@ __global__ void __launch_bounds__(256) k_mlp_infer(const float* __restrict__ fea
     for (int o = 16; o; o >>= 1) z += __shfl_xor_sync(kFull, z, o);
     z += __half2float(sw[oB3]);
     if (lane == 0) {
-      if (*acc_valid) {
+      if (acc_valid[0] && acc_valid[1] == 1) {
+        // the previous walk was the fixed-angle fallback, whose statistics
+        // the network never saw in training: one evaluation with the
+        // single-parameter bound, the relative walk the training tables were
+        // recorded after (the network's bounds overshot the error target by
+        // ~2x in this evaluation)
+        group_tau[g] = start_alpha * amag[g];
+        group_inv_theta[g] = inv_bound;
+      } else if (acc_valid[0]) {
         const float y = lo + (hi - lo) / (1.0f + expf(-z));
         group_tau[g] = amag[g] * exp10f(y);
         group_inv_theta[g] = inv_bound;
@@ -447,10 +455,10 @@ void launch_group_features(const int2* groups, const TreeInfo* info, const float
 }
 
 void launch_mlp_infer(const float* feat, const void* wh, const TreeInfo* info, float lo, float hi, const float* amag,
-                      const int* acc_valid, float inv_bound, float inv_fixed, float* inv, float* tau, int nblocks,
-                      cudaStream_t st) {
+                      const int* acc_valid, float inv_bound, float inv_fixed, float start_alpha, float* inv, float* tau,
+                      int nblocks, cudaStream_t st) {
   k_mlp_infer<<<nblocks, 256, 0, st>>>(feat, static_cast<const __half*>(wh), info, lo, hi, amag, acc_valid,
-                                       inv_bound, inv_fixed, inv, tau);
+                                       inv_bound, inv_fixed, start_alpha, inv, tau);
 }
 
 void launch_relative_tau(const TreeInfo* info, const float* amag, const int* acc_valid, float alpha, float inv_bound,

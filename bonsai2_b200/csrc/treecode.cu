@@ -26,6 +26,10 @@ using namespace bonsai;
 
 namespace {
 
+// the learned form's bound tau = kStartAlpha A_g in the one evaluation after
+// the fixed-angle fallback (the single-parameter relative walk the training
+// tables are recorded after, bonsai2_b200/learned.py ALPHA0)
+constexpr float kStartAlpha = 1e-2f;
 constexpr int kRingCap = 16384;  // per-warp level lists of the walk (ints): two halves of 8192
 constexpr int kMaxLevelSplit = 7;
 
@@ -550,7 +554,7 @@ struct Handle {
                             group_feat, so(), nsys, root_beg, prev, group_amag, nsm * 8, st);
       if (theta_mode == 1)
         launch_mlp_infer(group_feat, mlp_wh, info, theta_lo, theta_hi, group_amag, acc_valid, 1.0f / theta_bound,
-                         1.0f / prm.theta, group_inv, group_tau, nsm * 4, st);
+                         1.0f / prm.theta, kStartAlpha, group_inv, group_tau, nsm * 4, st);
       else
         launch_relative_tau(info, group_amag, acc_valid, rel_alpha, 1.0f / theta_bound, 1.0f / prm.theta,
                             group_inv, group_tau, nsm * 4, st);

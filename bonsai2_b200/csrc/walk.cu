@@ -241,6 +241,11 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
   const unsigned lt = lanemask_lt();
   unsigned long long sum_app = 0, sum_dir = 0;
   unsigned max_app = 0, max_dir = 0;
+  // whether this evaluation is the fixed-angle fallback (no previous
+  // accelerations when it starts): its statistics are then flagged as those
+  // of a walk without the relative test
+  bool start_fallback = false;
+  if (rel.acc_valid && blockIdx.x == 0 && threadIdx.x == 0) start_fallback = rel.acc_valid[0] == 0;
 
   while (true) {
     int g = 0;
@@ -582,7 +587,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
   // the accelerations just written are the previous ones of the next evaluation
   if (rel.acc_valid && blockIdx.x == 0 && threadIdx.x == 0) {
     rel.acc_valid[0] = 1;
-    rel.acc_valid[1] = rel.stats != nullptr;
+    rel.acc_valid[1] = rel.stats == nullptr ? 0 : (start_fallback ? 1 : 2);
   }
   if (lane == 0) {
     atomicAdd(stats + 0, sum_app);

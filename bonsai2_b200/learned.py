@@ -280,13 +280,24 @@ def allocation_labels(E, C, sizes, thetas, target, fraction=0.9):
 # ---------------------------------------------------------------------------
 # the learned form: relative accuracy mode
 # ---------------------------------------------------------------------------
-def _prepare_relative(t: Treecode, nleaf, ncrit, level_split, alpha0, theta_bound):
+def _prepare_relative(t: Treecode, nleaf, ncrit, level_split, alpha0, theta_bound, learned=None):
     """A relative walk at alpha0 (theta mode 2 with host bounds alpha0 A_g,
     after the fixed-angle first evaluation that gives A_g) so that acc and the
     walk statistics are those of a relative walk, then the tree rebuilt from
     the same positions (same groups, identity permutation): the state the
-    learned features see inside a run."""
+    learned features see inside a run.  learned = (weights, lo, hi): instead,
+    the learned walk itself at its steady state (the fallback, then six
+    evaluations), so that the features are those the network sees in a run."""
     set_relative_bound(t, theta_bound)
+    if learned is not None:
+        w, lo, hi = learned
+        set_weights(t, w)
+        set_theta_mode(t, 1, lo, hi)
+        run_relative(t, nleaf, ncrit, level_split, evaluations=7)
+        t.buildTree(nleaf)
+        t.computeMultipoles()
+        t.makeGroups(level_split, ncrit)
+        return
     set_theta_mode(t, 0)
     t.buildTree(nleaf)
     t.computeMultipoles()
@@ -308,7 +319,7 @@ def _prepare_relative(t: Treecode, nleaf, ncrit, level_split, alpha0, theta_boun
 
 
 def relative_tables(pos, vel, eps, ys=Y_GRID, samples_per_group=8, max_groups=8192, seed=0, nleaf=16, ncrit=64,
-                    level_split=5, alpha0=ALPHA0, theta_bound=THETA_BOUND, device=0):
+                    level_split=5, alpha0=ALPHA0, theta_bound=THETA_BOUND, device=0, learned=None):
     """For a random subset of groups: features F (g, 16) as the learned walk
     sees them; the group scale A (g,); error table E (g, k) = geometric mean
     over the group's sampled particles of |da|/|a| against the FP64 direct sum
@@ -321,7 +332,7 @@ def relative_tables(pos, vel, eps, ys=Y_GRID, samples_per_group=8, max_groups=81
         t.h_ptclPos[:] = pos
         t.h_ptclVel[:] = vel
         t.ptcl_h2d()
-        _prepare_relative(t, nleaf, ncrit, level_split, alpha0, theta_bound)
+        _prepare_relative(t, nleaf, ncrit, level_split, alpha0, theta_bound, learned)
         F = group_features(t)
         A = group_scale(t).astype(np.float64)
         groups = t.groups()
@@ -405,7 +416,7 @@ def calibrate_relative(pos, vel, w, eps, target, fraction=0.9, samples=2048, ite
 
         def median_err(c):
             set_theta_mode(t, 1, YLO + c, YHI + c)
-            run_relative(t, nleaf, ncrit, level_split, evaluations=2)
+            run_relative(t, nleaf, ncrit, level_split, evaluations=4)
             acc = t.get_acc()[samp].astype(np.float64)
             return float(np.median(np.linalg.norm(acc[:, :3] - ref[:, :3], axis=1) / refn))
 

@@ -204,7 +204,7 @@ def test_learned_form_gains_at_equal_median(oracle, lib):
         if learned:
             Lr.set_weights(t, w)
             Lr.set_theta_mode(t, 1, lo, hi)
-        for _ in range(3 if learned else 1):
+        for _ in range(7 if learned else 1):  # the learned bounds' steady state
             s = _evaluate(t)
         acc = t.get_acc().astype(np.float64)
         t.close()
