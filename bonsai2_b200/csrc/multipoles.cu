@@ -104,7 +104,10 @@ __device__ __forceinline__ void store_cell(int c, const MpRec& r, const typename
   const float mf = (float)r.m;
   const double tr = r.ixx + r.iyy + r.izz;
   const float t15 = (float)(1.5 * tr);
-  cell_ls[c] = make_float4(l, s, __fmul_rn(mf, __fmul_rn(l, __fmul_rn(l, l))), t15);
+  // (the relative test's size is the box's l: the mass-weighted rms radius
+  // sqrt(tr I / M) in its place ran 3-4 % slower at equal median error)
+  const float mk = __fmul_rn(mf, __fmul_rn(l, __fmul_rn(l, l)));
+  cell_ls[c] = make_float4(l, s, mk, t15);
   // the walk's staged record, copied to shared memory as it is (moments
   // negated so that every difference in the interaction is one add)
   float4* st = cell_stage + 3 * (size_t)c;
