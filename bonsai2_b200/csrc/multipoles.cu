@@ -75,7 +75,12 @@ __device__ __forceinline__ void store_cell(int c, const MpRec& r, const typename
   const float cx = (float)r.cx, cy = (float)r.cy, cz = (float)r.cz;
   float s, l;
   if (DS) {
-    cell_lo[c] = make_float4((float)(r.cx - (double)cx), (float)(r.cy - (double)cy), (float)(r.cz - (double)cz), 0.f);
+    // w: the staged record's -0.5 tr I (cell_stage[3c].w), so that the
+    // double-single walk, which loads cell_lo for every visited cell, stages
+    // an accepted cell without another load
+    const float t15d = (float)(1.5 * (r.ixx + r.iyy + r.izz));
+    cell_lo[c] = make_float4((float)(r.cx - (double)cx), (float)(r.cy - (double)cy), (float)(r.cz - (double)cz),
+                             __fmul_rn(t15d, -1.0f / 3.0f));
     // extents and centre offsets from the exact box and COM
     double hm = 0.0, d2 = 0.0;
     const double com[3] = {r.cx, r.cy, r.cz};

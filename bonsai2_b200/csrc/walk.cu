@@ -381,6 +381,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
         uint4 cd = make_uint4(0u, 0xFFFFFFFFu, 0u, 0u);
         float4 co = make_float4(0.f, 0.f, 0.f, 0.f);
         float4 ls = make_float4(0.f, 0.f, 0.f, 0.f);
+        [[maybe_unused]] float a0w = 0.f;  // DS: the staged -0.5 tr I, carried by cell_lo.w
         if (valid) {
           cd = __ldg(cell_data + cell);
           co = __ldg(cell_open + cell);
@@ -389,6 +390,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
             co.x = __fadd_rn(__fsub_rn(co.x, R.x), cl.x);
             co.y = __fadd_rn(__fsub_rn(co.y, R.y), cl.y);
             co.z = __fadd_rn(__fsub_rn(co.z, R.z), cl.z);
+            a0w = cl.w;
           }
           if (PERGROUP) ls = __ldg(cell_ls + cell);
         }
@@ -472,7 +474,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
             st_wm += m * inv;                           // the cell's force share M / ds^2
           }
           if (DS)  // the COM relative to the group's reference point
-            s_a0[w][slot] = make_float4(co.x, co.y, co.z, __ldg(&src[0].w));
+            s_a0[w][slot] = make_float4(co.x, co.y, co.z, a0w);
           else
             cp_async16(&s_a0[w][slot], src);
           cp_async16(&s_a1[w][slot], src + 1);
