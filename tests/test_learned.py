@@ -155,6 +155,36 @@ def test_relative_modes_fall_back_to_fixed_angle(oracle, lib):
 
 
 @pytest.mark.gpu
+def test_learned_form_starts_with_the_single_alpha_bound(oracle, lib):
+    """The evaluation after the fixed-angle fallback reads statistics of a
+    walk without the relative test, which the network never saw in training:
+    it takes the single-parameter bound tau = 1e-2 A_g instead (the state the
+    training tables are recorded after), so its accelerations equal theta
+    mode 3's at alpha 1e-2 bit for bit, whatever the weights; the evaluation
+    after it uses the network."""
+    import bonsai2_b200 as B
+    from bonsai2_b200 import learned as Lr
+    pos, vel = oracle.plummer_float4(30000, 7)
+    accs = {}
+    for mode in (1, 3):
+        t = _load(B, pos, vel)
+        Lr.set_relative_bound(t, Lr.THETA_BOUND)
+        if mode == 1:
+            Lr.set_weights(t, Lr.init_weights(5))
+            Lr.set_theta_mode(t, 1, Lr.YLO, Lr.YHI)
+        else:
+            Lr.set_theta_mode(t, 3, Lr.ALPHA0, Lr.ALPHA0)
+        _evaluate(t)   # fixed-angle fallback
+        s2 = _evaluate(t)
+        a2 = t.get_acc()
+        s3 = _evaluate(t)
+        accs[mode] = (a2, s2, s3)
+        t.close()
+    assert np.array_equal(accs[1][0], accs[3][0]) and np.array_equal(accs[1][1], accs[3][1])
+    assert not np.array_equal(accs[1][2], accs[3][2])   # then the network's own bounds
+
+
+@pytest.mark.gpu
 def test_relative_mode_fp64_checker_takes_the_same_lists(oracle, lib):
     import bonsai2_b200 as B
     from bonsai2_b200 import learned as Lr
