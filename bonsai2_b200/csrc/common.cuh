@@ -7,8 +7,10 @@
 //   CellData    uint4  (parent | level<<27, first | (n-1)<<29 or ~0 for a
 //                       leaf, pbeg, pend)      -- Treecode.h:45-89
 //   cell_open   float4 (com x,y,z, cellOp^2)   -- d_cellSize, computeMultipoles.cu:180
-//   cell_q0     float4 (M, Ixx, Iyy, Izz)      -- mass-weighted central moments
-//   cell_q1     float4 (Ixy, Ixz, Iyz, 1.5*trace I)
+//   cell_stage  3 x float4 per cell, the walk's staged quadrupole record:
+//               (COM, -0.5 tr I), (M, -3Ixx, -3Iyy, -3Izz),
+//               (-3Ixy, -3Ixz, -3Iyz, -1.5 tr I), I the mass-weighted
+//               central second moments (multipoles.cu)
 //   GroupData   int2   (pbeg, np)              -- Treecode.h:29-43
 #pragma once
 #include <cstdint>

@@ -5,8 +5,8 @@
 // makeGroups.cu:270-277, buildTree.cu:940-944): a stable radix sort, ties in
 // input order.  This is a hand-written replacement with the same semantics:
 // 8 passes of 8 bits, one-sweep (below): keys are ranked stably inside each
-// 4096-key tile with warp match_any and per-warp digit counters in shared
-// memory, tile offsets come from a decoupled look-back, and tiles are written
+// 4096-key tile (the lanes of equal digit from bit ballots) with per-warp
+// digit counters in shared memory, tile offsets come from a decoupled look-back, and tiles are written
 // out through shared memory in contiguous digit runs.  A thread keeps only the
 // 16 ranks and packed digits of its keys across the look-back (the keys are
 // re-read from L2 for staging): 4 blocks per SM (keeping the keys, 127
