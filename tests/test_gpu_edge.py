@@ -177,7 +177,7 @@ def test_leapfrog_time_reversible(precision):
 
 
 def test_full_size_properties(lib):
-    # BASELINE's large configuration: N = 2^24 Plummer, theta 0.4, eps 0.005
+    # the large benchmark configuration: N = 2^24 Plummer, theta 0.4, eps 0.005
     import bonsai2_b200 as B
     n = 1 << 24
     pos, vel = B.plummer(n, 19810614)
