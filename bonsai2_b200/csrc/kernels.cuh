@@ -190,7 +190,8 @@ void launch_group_features(const int2* groups, const TreeInfo* info, const float
 // inv_bound; without previous accelerations the fixed angle (tau = 0,
 // 1/theta = inv_fixed)
 // start_alpha: the bound tau = start_alpha amag used instead of the network
-// when the previous statistics came from the fixed-angle fallback
+// when the previous walk recorded no relative-walk statistics (acc_valid[1]
+// != 2: the fixed-angle fallback, or a walk in another theta mode)
 void launch_mlp_infer(const float* feat, const void* wh, const TreeInfo* info, float lo, float hi, const float* amag,
                       const int* acc_valid, float inv_bound, float inv_fixed, float start_alpha, float* inv, float* tau,
                       int nblocks, cudaStream_t st);

@@ -206,12 +206,13 @@ __global__ void __launch_bounds__(256) k_mlp_infer(const float* __restrict__ fea
     for (int o = 16; o; o >>= 1) z += __shfl_xor_sync(kFull, z, o);
     z += __half2float(sw[oB3]);
     if (lane == 0) {
-      if (acc_valid[0] && acc_valid[1] == 1) {
-        // the previous walk was the fixed-angle fallback, whose statistics
-        // the network never saw in training: one evaluation with the
+      if (acc_valid[0] && acc_valid[1] != 2) {
+        // the previous walk was not a relative walk with statistics (the
+        // fixed-angle fallback, or another theta mode): the network never
+        // saw such statistics in training, so one evaluation takes the
         // single-parameter bound, the relative walk the training tables were
-        // recorded after (the network's bounds overshot the error target by
-        // ~2x in this evaluation)
+        // recorded after (after the fallback, the network's own bounds
+        // overshot the error target by ~2x in this evaluation)
         group_tau[g] = start_alpha * amag[g];
         group_inv_theta[g] = inv_bound;
       } else if (acc_valid[0]) {
