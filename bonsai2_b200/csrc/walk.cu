@@ -101,6 +101,14 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // direct-source ring per warp (a power of two, >= 64)
 constexpr int kDirRing = 128;
+// double-single positions: the leaf particles' hi and lo parts are copied by
+// cp.async into two rings (64 entries each, to stay within static shared
+// memory) and combined into (hi - R) + lo in shared memory right before the
+// batch is evaluated, one lane per entry; 0: loaded into registers and
+// combined at staging (the warp waits a round trip per 32 particles)
+#ifndef BONSAI_WALK_DS_ASYNC
+#define BONSAI_WALK_DS_ASYNC 1
+#endif
 
 // Interaction arithmetic over V = float (one i-particle) or V = float2 (two
 // i-particles of the lane, evaluated by the packed FFMA2/FMUL2/FADD2 of
@@ -225,7 +233,10 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
   __shared__ float4 s_a0[kWalkWarps][64];
   __shared__ float4 s_a1[kWalkWarps][64];
   __shared__ float4 s_a2[kWalkWarps][64];
-  __shared__ float4 s_d[kWalkWarps][kDirRing];
+  constexpr bool DSA = DS && BONSAI_WALK_DS_ASYNC;
+  constexpr int DRING = DSA ? 64 : kDirRing;
+  __shared__ float4 s_d[kWalkWarps][DRING];
+  __shared__ float4 s_dlo[kWalkWarps][DSA ? DRING : 1];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int sub = SPLIT ? (lane & 15) : lane;
   const int half = SPLIT ? (lane >> 4) : 0;
@@ -338,7 +349,22 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
       a_cnt -= 32;
       n_app += 32;
     };
+    // DSA: the entries [d_head + first, + count) become (hi - R) + lo (their
+    // copies have landed: called after cp_async_wait_all and __syncwarp)
+    [[maybe_unused]] auto combine_dir = [&](int first, int count) {
+      for (int k = lane; k < count; k += 32) {
+        const int sl = (d_head + first + k) & (DRING - 1);
+        float4 pj = s_d[w][sl];
+        const float4 lo = s_dlo[w][sl];
+        pj.x = __fadd_rn(__fsub_rn(pj.x, R.x), lo.x);
+        pj.y = __fadd_rn(__fsub_rn(pj.y, R.y), lo.y);
+        pj.z = __fadd_rn(__fsub_rn(pj.z, R.z), lo.z);
+        s_d[w][sl] = pj;
+      }
+      __syncwarp();
+    };
     auto eval_dir = [&]() {
+      if (DSA) combine_dir(0, 32);
       const float4* D = &s_d[w][d_head + half];
       BONSAI_UNROLL_N(BONSAI_WALK_UNROLL)
       for (int j = 0; j < 32; j += JSTEP) {
@@ -346,7 +372,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
 #pragma unroll
         for (int v = 0; v < NV; v++) mono_acc(av[v], iv[v], pj, veps2);
       }
-      d_head = (d_head + 32) & (kDirRing - 1);
+      d_head = (d_head + 32) & (DRING - 1);
       d_cnt -= 32;
       n_dir += 32;
     };
@@ -493,7 +519,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
           const int f = __shfl_sync(kFull, pb, src);
           const int e = __shfl_sync(kFull, incl2 - nb, src);
           const int cnt = min(32, tot2 - base);
-          if (d_cnt + cnt > kDirRing) {  // no room: evaluate one batch now
+          if (d_cnt + cnt > DRING) {  // no room: evaluate one batch now
             cp_async_wait_all();
             __syncwarp();
             eval_dir();
@@ -501,8 +527,12 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
           }
           if (lane < cnt) {
             const int jj = BONSAI_IN_RANGE(f + (s - e), npart, 0x406) ? f + (s - e) : 0;
-            float4* dst = &s_d[w][(d_head + d_cnt + lane) & (kDirRing - 1)];
-            if (DS) {
+            const int dsl = (d_head + d_cnt + lane) & (DRING - 1);
+            float4* dst = &s_d[w][dsl];
+            if (DSA) {
+              cp_async16(dst, jpos + jj);
+              cp_async16(&s_dlo[w][dsl], jpos_lo + jj);
+            } else if (DS) {
               float4 pj = __ldg(jpos + jj);
               const float4 lo = __ldg(jpos_lo + jj);
               pj.x = __fadd_rn(__fsub_rn(pj.x, R.x), lo.x);
@@ -532,8 +562,9 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks)
       for (int v = 0; v < NV; v++) quad_acc(av[v], iv[v], a0, a1, a2, veps2);
     }
     n_app += a_cnt;
+    if (DSA) combine_dir(0, d_cnt);
     for (int j = half; j < d_cnt; j += JSTEP) {
-      const float4 pj = s_d[w][(d_head + j) & (kDirRing - 1)];
+      const float4 pj = s_d[w][(d_head + j) & (DRING - 1)];
 #pragma unroll
       for (int v = 0; v < NV; v++) mono_acc(av[v], iv[v], pj, veps2);
     }
