@@ -158,6 +158,7 @@ class Dist:
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.backend = backend
         if self.world > 1:
             import datetime
             import torch.distributed as dist
@@ -167,7 +168,10 @@ class Dist:
 
     def barrier(self):
         if self.pg:
-            self.pg.barrier()
+            if self.backend == "nccl":  # the rank's own GPU, not one NCCL infers
+                self.pg.barrier(device_ids=[self.local])
+            else:
+                self.pg.barrier()
 
     def max(self, x: float) -> float:
         if not self.pg:
