@@ -243,7 +243,11 @@ int bonsai_direct_fp64_noalloc(const float *d_pos4, int n, const int *d_sample, 
 #define BONSAI_MLP_WEIGHTS 5313 /* W1[64][16], b1[64], W2[64][64], b2[64], w3[64], b3 */
 /* mode 0: fixed theta (params);
  * 1 (learned): tau_g = A_g 10^y_g, y_g = lo + (hi-lo)*sigmoid(MLP(features_g))
- *   from the weights of bonsai_set_mlp_weights;
+ *   from the weights of bonsai_set_mlp_weights; the features include
+ *   statistics of the previous walk, and when that walk left none of a
+ *   relative walk (the fixed-angle evaluation after a load, or a walk in
+ *   another mode) the evaluation takes tau_g = 1e-2 A_g instead of the
+ *   network, the relative walk the training tables are recorded after;
  * 2: theta_g from bonsai_set_group_theta, tau_g from bonsai_set_group_tau;
  * 3 (relative, one parameter): tau_g = lo * A_g (lo = alpha > 0; hi >= lo).
  * Features are clamped to [-10, 10] (degenerate groups, e.g. of a one-particle
